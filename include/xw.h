@@ -1,0 +1,237 @@
+/* xw.h -- C ABI of the B200-native weighing-matrix population annealer.
+ *
+ * Drop-in boundary for the xweigh_cuda path of flinty-mathematics/xtax.
+ * Every entry point names the reference interface it replaces
+ * (src/xweigh_cuda.hpp, src/xweigh_cuda.cu, src/xweigh_anneal.hpp,
+ * src/xweigh_cuda_main.cpp).  Plain C types only; no exceptions cross the
+ * ABI.  Each call returns an xw status code; on failure xw_last_error()
+ * gives the message (thread-local), worded like the reference's exception
+ * text where one exists.
+ *
+ * Matrices are n*n int8 arrays in the reference's column-major order:
+ * entry (row r, column c) at [c*n + r] (xweigh_anneal.hpp:290-296), except
+ * the batched rescoring input, which is row-major (see xw_rescore).
+ */
+#ifndef XW_H
+#define XW_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define XW_OK 0
+#define XW_ERR_INVALID 1   /* an argument or parameter is out of range */
+#define XW_ERR_CUDA 2      /* a CUDA runtime call failed */
+#define XW_ERR_CAPACITY 3  /* shared memory, device memory or a size limit */
+#define XW_ERR_INTERNAL 4  /* an invariant failed (score mismatch, ...) */
+#define XW_ERR_NOT_FOUND 5 /* unknown request id */
+#define XW_ERR_TIMEOUT 6   /* a wait ended before the request finished */
+#define XW_ERR_IO 7        /* file read or write failed */
+
+#define XW_MAX_ORDER_CUDA 128       /* largest n the device path anneals */
+#define XW_MAX_CANDIDATE_SAMPLES 32 /* xweigh_cuda.hpp:11 */
+#define XW_MAX_TARGET_SAMPLES 64    /* xweigh_cuda.hpp:12 */
+
+/* Mirrors xweigh_cuda::Params (xweigh_cuda.hpp:14-44) field for field, in
+ * the same order, followed by the extensions of this implementation. */
+typedef struct xw_params {
+    int32_t device;
+    int32_t replicas;             /* 0 = occupancy-based */
+    int32_t moves_per_launch;     /* iterations per replica between host checks */
+    uint64_t seed;                /* 0 = random_device */
+    double max_seconds;
+    double save_interval;
+    double sign_fraction;
+    double double_sign_fraction;
+    double switch_sign_fraction;
+    double squared_objective_fraction;
+    double parity_objective_fraction;
+    double greedy_fraction;
+    int32_t candidate_samples;
+    double target_fraction;
+    int32_t target_samples;
+    double t_init;
+    double t_min;
+    double cooling;
+    int32_t moves_per_cool;
+    int32_t stuck_threshold;
+    double reheat;
+    double restart_interval;      /* accepted and validated; elite restarts are not run */
+    double restart_fraction;
+    int32_t restart_kick_min;
+    int32_t restart_kick_max;
+    /* ---- extensions ---- */
+    uint64_t max_moves;           /* total move budget over all replicas, 0 = none */
+    int32_t tempering;            /* 1: replicas form a parallel-tempering ladder t_min..t_init */
+    int32_t exchange_interval;    /* iterations between exchanges when tempering */
+    int32_t objective;            /* -1 reference per-replica mix, 0 L1, 1 squared, 2 parity */
+    int32_t move_set;             /* 0 flip/switch/double flip, 1 flip/within-row swap */
+    int32_t start_kind;           /* 0 regular random start, 1 row-only random start */
+    int32_t stop_on_solve;        /* 1: stop every replica once one solves */
+    int32_t warps_per_block;      /* 0 = autotuned */
+    int32_t reserved;
+} xw_params;
+
+/* xweigh_cuda::DeviceInfo (xweigh_cuda.hpp:46-54) */
+typedef struct xw_device_info {
+    char name[256];
+    int32_t ordinal;
+    int32_t compute_major;
+    int32_t compute_minor;
+    int32_t multiprocessors;
+    uint64_t global_memory;
+    uint64_t max_shared_memory_per_block;
+} xw_device_info;
+
+/* xweigh_cuda::RunResult (xweigh_cuda.hpp:56-65) plus the best state's
+ * scores, solve time and exact verification */
+typedef struct xw_result {
+    int64_t score;
+    int64_t conflicts;
+    int32_t replicas;
+    int32_t solved;               /* best score is 0 */
+    int32_t verified;             /* W W^T = wI checked exactly in int64 */
+    int32_t best_replica;
+    uint64_t moves;
+    uint64_t candidate_evaluations;
+    uint64_t restarted_replicas;
+    uint64_t iterations;          /* per-replica iterations of the longest replica */
+    double initialization_seconds;
+    double search_seconds;
+    double time_to_solution_seconds; /* -1 when unsolved */
+    xw_device_info device;
+} xw_result;
+
+typedef void (*xw_log_fn)(const char* line, void* user);
+typedef void (*xw_checkpoint_fn)(const int8_t* best_colmajor, int32_t n, void* user);
+
+/* Reference defaults (xweigh_cuda.hpp:14-44) and extension defaults. */
+void xw_params_default(xw_params* p);
+
+/* Thread-local message of the last failed call on this thread. */
+const char* xw_last_error(void);
+
+/* validate_params (xweigh_cuda.cu:1160-1241): XW_OK or XW_ERR_INVALID with
+ * the reference's message. */
+int32_t xw_validate_params(int32_t n, int32_t w, const xw_params* p);
+
+/* xweigh_cuda::query_device (xweigh_cuda.cu:1382-1417) */
+int32_t xw_query_device(int32_t ordinal, xw_device_info* out);
+
+/* xweigh_cuda::run_annealer (xweigh_cuda.cu:1419-2436).  start_colmajor
+ * (nullable, n*n) starts every replica from one validated state, as
+ * initial_state does.  best_colmajor (caller-owned, n*n) receives the best
+ * state.  log receives the reference's progress lines; checkpoint receives
+ * the best state at most every save_interval seconds.  Stops on
+ * xw_request_stop(), max_seconds, max_moves or a solve. */
+int32_t xw_run(int32_t n, int32_t w, const xw_params* p, const int8_t* start_colmajor,
+               xw_log_fn log, xw_checkpoint_fn checkpoint, void* user,
+               xw_result* out, int8_t* best_colmajor);
+
+/* The stop flag (g_stop, stop_signal.hpp:44).  Async-signal-safe. */
+void xw_request_stop(void);
+void xw_clear_stop(void);
+
+/* ---- host-side helpers of the drop-in ------------------------------- */
+/* State::random_start (xweigh_anneal.hpp:117-131) */
+int32_t xw_random_start(int32_t n, int32_t w, uint32_t seed, int8_t* out_colmajor);
+/* row-only start: w nonzeros per row at uniform positions, uniform signs */
+int32_t xw_row_start(int32_t n, int32_t w, uint64_t seed, uint32_t replica, int8_t* out_colmajor);
+/* State::sylvester_blocks (xweigh_anneal.hpp:133-149) */
+int32_t xw_sylvester(int32_t n, int32_t w, int8_t* out_colmajor);
+/* full recompute: stats = {L1 score, conflicts, squared, parity} over i<j */
+int32_t xw_score(int32_t n, int32_t w, const int8_t* W_colmajor, int64_t stats[4]);
+/* verify_support / verify_weighing (xweigh_anneal.hpp:221-264):
+ * bit0 support, bit1 W W^T = wI */
+int32_t xw_verify(int32_t n, int32_t w, const int8_t* W_colmajor);
+/* read_state_csv (xweigh_anneal.hpp:669-756) */
+int32_t xw_read_csv(const char* path, int32_t n, int32_t w, int8_t* out_colmajor);
+/* write_entries_csv (xweigh_anneal.hpp:758-797), atomic temp + rename */
+int32_t xw_write_csv(const char* path, int32_t n, const int8_t* W_colmajor);
+/* impossibility_reason (xweigh_cuda_main.cpp:32-52); "" when none */
+const char* xw_impossibility_reason(int32_t n, int32_t w);
+/* calibrate_temperature (xweigh_anneal.hpp:881-899) on State s with seed */
+double xw_calibrate(int32_t n, int32_t w, const int8_t* W_colmajor, const xw_params* p, uint32_t seed);
+
+/* ---- batched populations (many independent searches, one device) ---- */
+/* One search W(n,w): `replicas` replicas with starts derived from `seed`
+ * (regular start of replica r: State::random_start(n, w, seed + r*0x9e3779b9)). */
+typedef struct xw_job_spec {
+    int32_t n, w;
+    uint64_t seed;
+    int32_t replicas;
+    int32_t reserved;
+    uint64_t max_moves;           /* per-job total move budget, 0 = the params' */
+} xw_job_spec;
+
+typedef struct xw_job_result {
+    int64_t score, conflicts;     /* best over the job's replicas */
+    int32_t best_replica;
+    int32_t solved;
+    int32_t verified;
+    int32_t error;                /* nonzero: a replica failed a device self-check */
+    uint64_t moves;
+    uint64_t candidate_evaluations;
+    uint64_t iterations;          /* max over replicas */
+    uint64_t solved_iteration;    /* iteration of the first solve */
+    double time_to_solution_seconds; /* device clock, from the first launch */
+} xw_job_result;
+
+typedef struct xw_batch xw_batch;
+
+/* Build the jobs' start states (or copy `starts`, sum of R*n*n bytes in job
+ * order, nullable) and upload them.  Tempering jobs form one ladder each. */
+int32_t xw_batch_create(const xw_job_spec* jobs, int32_t njobs, const xw_params* p,
+                        const int8_t* starts, xw_batch** out);
+/* Bind the batch's work to a CUDA stream (cudaStream_t; NULL = its own). */
+int32_t xw_batch_set_stream(xw_batch* b, void* cuda_stream);
+/* Restore the uploaded start states on the device (no host transfer). */
+int32_t xw_batch_reset(xw_batch* b);
+/* Enqueue `iters` iterations per replica: rounds of exchange_interval (or
+ * moves_per_launch) iterations, each one persistent launch (plus an
+ * exchange launch when tempering), as one captured CUDA graph.  Returns
+ * without waiting. */
+int32_t xw_batch_run(xw_batch* b, uint64_t iters);
+int32_t xw_batch_synchronize(xw_batch* b);
+/* Device milliseconds of each anneal launch of the last xw_batch_run. */
+int32_t xw_batch_launch_times(xw_batch* b, float* ms, int32_t cap, int32_t* count);
+/* Results per job; best (nullable) receives each job's best W in job order. */
+int32_t xw_batch_results(xw_batch* b, xw_job_result* results, int8_t* best);
+/* Snapshot of one replica (the per-replica state of DeviceStorage,
+ * xweigh_cuda.cu:197-215, plus this implementation's Philox position). */
+typedef struct xw_replica_state {
+    uint64_t iterations;          /* Philox iteration counter */
+    uint64_t moves;
+    uint64_t candidate_evaluations;
+    int64_t score, conflicts;
+    int64_t best_score, best_conflicts;
+    int64_t objective_total;
+    double temperature, reheat_temperature;
+    int32_t moves_since_improvement, cooling_counter, rung, objective_kind;
+    uint32_t status, error;
+} xw_replica_state;
+
+/* Read replica `replica` of job `job`: state, current W, best W (n*n each,
+ * nullable) and the minority lists (n*min(w,n-w) bytes, nullable). */
+int32_t xw_batch_read_replica(xw_batch* b, int32_t job, int32_t replica, xw_replica_state* st,
+                              int8_t* W, int8_t* best_W, uint8_t* minority);
+
+/* Launch shape of the batch: warps per block, blocks, shared bytes per warp. */
+int32_t xw_batch_shape(xw_batch* b, int32_t* warps_per_block, int32_t* blocks, int32_t* slot_bytes);
+void xw_batch_destroy(xw_batch* b);
+
+/* Whole batched search through host buffers: upload, run until every job
+ * is solved or out of budget (or `iters` per replica when nonzero), read
+ * back.  The end-to-end call of the served-batch benchmark. */
+int32_t xw_batch_solve(const xw_job_spec* jobs, int32_t njobs, const xw_params* p,
+                       const int8_t* starts, uint64_t iters,
+                       xw_job_result* results, int8_t* best);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,135 @@
+"""Parity of the CUDA annealer with the oracle, through the C ABI.
+
+Every replica of a device run is replayed by the CPU oracle from the same
+start, key and temperature; after K iterations the whole replica state must
+be identical: W, best W, minority lists, iteration and move counters,
+scores, objective totals, temperature and counters.  Integer work, so the
+bar is bit-exact.  Tempering runs also replay the device's exchange sweeps.
+"""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+import xtax_b200 as X
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_job(n, w, seed, p: X.Params):
+    k0, k1 = X.philox_key(seed)
+    return O.make_job(n, w, tempering=p.tempering, move_set=p.move_set,
+                      candidate_samples=p.candidate_samples, target_samples=p.target_samples,
+                      moves_per_cool=p.moves_per_cool, stuck_threshold=p.stuck_threshold,
+                      key0=k0, key1=k1, objective=p.objective,
+                      greedy_fraction=p.greedy_fraction, target_fraction=p.target_fraction,
+                      double_sign_fraction=p.double_sign_fraction, sign_fraction=p.sign_fraction,
+                      switch_sign_fraction=p.switch_sign_fraction,
+                      squared_objective_fraction=p.squared_objective_fraction,
+                      parity_objective_fraction=p.parity_objective_fraction,
+                      t_min=p.t_min, cooling=p.cooling, reheat=p.reheat)
+
+
+def start_of(n, w, seed, r, p):
+    if p.start_kind == 1:
+        k0, k1 = X.philox_key(seed)
+        return O.row_start(n, w, k0, k1, r)
+    return O.random_start(n, w, (seed + r * 0x9e3779b9) & 0xffffffff)
+
+
+def compare(batch, job_index, r, rep):
+    st, W, B, M = batch.replica(job_index, r)
+    s, oW, oB, oM, _, _ = rep.get()
+    assert st.error == 0
+    ctx = f"job {job_index} replica {r}"
+    assert st.iterations == s.it, ctx
+    assert st.moves == s.moves, ctx
+    assert st.candidate_evaluations == s.cand_evals, ctx
+    assert (st.score, st.conflicts) == (s.score, s.conflicts), ctx
+    assert (st.best_score, st.best_conflicts) == (s.best_score, s.best_conflicts), ctx
+    assert st.objective_total == s.obj_total, ctx
+    assert st.temperature == s.temperature, ctx
+    assert st.moves_since_improvement == s.msi and st.cooling_counter == s.cool_ctr, ctx
+    assert st.rung == s.rung, ctx
+    assert (W == oW).all(), ctx
+    assert (B == oB).all(), ctx
+    assert (M == oM).all(), ctx
+
+
+CASES = [
+    # n, w, replicas, iterations, params
+    (12, 11, 6, 3000, dict(t_init=4.0, moves_per_launch=1000, stuck_threshold=700, moves_per_cool=50)),
+    (16, 4, 6, 2500, dict(t_init=3.0, moves_per_launch=1250, double_sign_fraction=0.4)),
+    (20, 10, 5, 2000, dict(t_init=5.0, moves_per_launch=2000)),
+    (13, 9, 5, 2000, dict(t_init=4.0, moves_per_launch=700, target_samples=12, candidate_samples=7)),
+    (26, 25, 4, 2000, dict(t_init=6.0, moves_per_launch=1000, target_samples=3)),
+    (40, 39, 3, 800, dict(t_init=6.0, moves_per_launch=400)),
+    (64, 4, 3, 800, dict(t_init=2.0, moves_per_launch=800)),
+    (70, 30, 2, 300, dict(t_init=8.0, moves_per_launch=300)),
+    (12, 11, 4, 2000, dict(t_init=4.0, moves_per_launch=1000, move_set=1, start_kind=1,
+                           objective=1, sign_fraction=0.3)),
+    (16, 4, 4, 1500, dict(t_init=2.0, moves_per_launch=500, move_set=1, start_kind=1, objective=0)),
+    (30, 29, 3, 1200, dict(t_init=6.0, moves_per_launch=600, objective=2)),
+]
+
+
+@pytest.mark.parametrize("n,w,R,iters,kw", CASES, ids=lambda v: str(v) if not isinstance(v, dict) else "")
+def test_cooling_population_matches_oracle(n, w, R, iters, kw):
+    p = X.Params(stop_on_solve=0, **kw)
+    seed = 1000 + n * 7 + w
+    batch = X.Batch([{"n": n, "w": w, "seed": seed, "replicas": R}], p)
+    temps = [batch.replica(0, r)[0].reheat_temperature for r in range(R)]
+    batch.run(iters)
+    batch.synchronize()
+    job = oracle_job(n, w, seed, p)
+    for r in range(R):
+        rep = O.Replica(job, r, start_of(n, w, seed, r, p), temps[r], r)
+        rep.run(iters, stop_on_solve=False)
+        assert rep.check() == 0
+        compare(batch, 0, r, rep)
+    batch.close()
+
+
+@pytest.mark.parametrize("n,w,R,interval,rounds", [(12, 11, 8, 300, 4), (26, 25, 6, 500, 3), (16, 4, 5, 250, 4)])
+def test_tempering_matches_oracle(n, w, R, interval, rounds):
+    p = X.Params(stop_on_solve=0, tempering=1, exchange_interval=interval, t_min=0.1, t_init=6.0,
+                 squared_objective_fraction=0.0, parity_objective_fraction=0.0)
+    seed = 77 + n
+    batch = X.Batch([{"n": n, "w": w, "seed": seed, "replicas": R},
+                     {"n": n, "w": w, "seed": seed + 1, "replicas": R}], p)
+    batch.run(interval * rounds)
+    batch.synchronize()
+    bottom, top = 0.1, 6.0
+    ratio = (top / bottom) ** (1.0 / (R - 1))
+    ladder, t = [], bottom
+    for _ in range(R):
+        ladder.append(t)
+        t *= ratio
+    for jidx, s in enumerate([seed, seed + 1]):
+        job = oracle_job(n, w, s, p)
+        reps = [O.Replica(job, r, start_of(n, w, s, r, p), ladder[r], r) for r in range(R)]
+        for k in range(rounds):
+            for rep in reps:
+                rep.run(interval, stop_on_solve=False)
+            O.exchange(job, reps, ladder, k)
+        for r, rep in enumerate(reps):
+            compare(batch, jidx, r, rep)
+    batch.close()
+
+
+def test_mixed_orders_in_one_launch_match_oracle():
+    # replicas of different (n, w) share one persistent launch
+    p = X.Params(stop_on_solve=0, t_init=4.0, moves_per_launch=600)
+    jobs = [{"n": 14, "w": 13, "seed": 5, "replicas": 3}, {"n": 24, "w": 23, "seed": 6, "replicas": 2},
+            {"n": 18, "w": 9, "seed": 7, "replicas": 2}, {"n": 33, "w": 32, "seed": 8, "replicas": 2}]
+    batch = X.Batch(jobs, p)
+    temps = [[batch.replica(j, r)[0].reheat_temperature for r in range(jb["replicas"])]
+             for j, jb in enumerate(jobs)]
+    batch.run(1800)
+    batch.synchronize()
+    for j, jb in enumerate(jobs):
+        job = oracle_job(jb["n"], jb["w"], jb["seed"], p)
+        for r in range(jb["replicas"]):
+            rep = O.Replica(job, r, start_of(jb["n"], jb["w"], jb["seed"], r, p), temps[j][r], r)
+            rep.run(1800, stop_on_solve=False)
+            compare(batch, j, r, rep)
+    batch.close()

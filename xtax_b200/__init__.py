@@ -1,0 +1,436 @@
+"""xtax_b200 -- B200-native weighing-matrix population annealer.
+
+Python view of the C ABI in include/xw.h (library: xtax_b200/libxw.so).
+The names follow the reference's xweigh_cuda interface
+(src/xweigh_cuda.hpp of flinty-mathematics/xtax): ``Params`` mirrors
+``xweigh_cuda::Params``, ``query_device`` and ``run_annealer`` mirror the
+functions of the same names, and ``RunResult`` mirrors ``RunResult``.
+Errors raise ``XwError`` with the library's message, as the reference's
+``std::runtime_error``s carry theirs.
+
+There is no CPU fallback: every call goes through the CUDA library, and
+importing this package fails loudly when libxw.so is missing.
+"""
+import ctypes as C
+import os
+from dataclasses import dataclass, field, fields
+from typing import List, Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libxw.so")
+HEADER = os.path.join(os.path.dirname(_HERE), "include", "xw.h")
+
+XW_OK, XW_ERR_INVALID, XW_ERR_CUDA, XW_ERR_CAPACITY, XW_ERR_INTERNAL = 0, 1, 2, 3, 4
+XW_ERR_NOT_FOUND, XW_ERR_TIMEOUT, XW_ERR_IO = 5, 6, 7
+MAX_ORDER_CUDA = 128
+MAX_CANDIDATE_SAMPLES = 32
+MAX_TARGET_SAMPLES = 64
+
+
+class XwError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(message)
+        self.code = code
+
+
+class _Params(C.Structure):
+    _fields_ = [("device", C.c_int32), ("replicas", C.c_int32), ("moves_per_launch", C.c_int32),
+                ("seed", C.c_uint64), ("max_seconds", C.c_double), ("save_interval", C.c_double),
+                ("sign_fraction", C.c_double), ("double_sign_fraction", C.c_double),
+                ("switch_sign_fraction", C.c_double), ("squared_objective_fraction", C.c_double),
+                ("parity_objective_fraction", C.c_double), ("greedy_fraction", C.c_double),
+                ("candidate_samples", C.c_int32), ("target_fraction", C.c_double),
+                ("target_samples", C.c_int32), ("t_init", C.c_double), ("t_min", C.c_double),
+                ("cooling", C.c_double), ("moves_per_cool", C.c_int32),
+                ("stuck_threshold", C.c_int32), ("reheat", C.c_double),
+                ("restart_interval", C.c_double), ("restart_fraction", C.c_double),
+                ("restart_kick_min", C.c_int32), ("restart_kick_max", C.c_int32),
+                ("max_moves", C.c_uint64), ("tempering", C.c_int32),
+                ("exchange_interval", C.c_int32), ("objective", C.c_int32),
+                ("move_set", C.c_int32), ("start_kind", C.c_int32), ("stop_on_solve", C.c_int32),
+                ("warps_per_block", C.c_int32), ("reserved", C.c_int32)]
+
+
+class _DeviceInfo(C.Structure):
+    _fields_ = [("name", C.c_char * 256), ("ordinal", C.c_int32), ("compute_major", C.c_int32),
+                ("compute_minor", C.c_int32), ("multiprocessors", C.c_int32),
+                ("global_memory", C.c_uint64), ("max_shared_memory_per_block", C.c_uint64)]
+
+
+class _Result(C.Structure):
+    _fields_ = [("score", C.c_int64), ("conflicts", C.c_int64), ("replicas", C.c_int32),
+                ("solved", C.c_int32), ("verified", C.c_int32), ("best_replica", C.c_int32),
+                ("moves", C.c_uint64), ("candidate_evaluations", C.c_uint64),
+                ("restarted_replicas", C.c_uint64), ("iterations", C.c_uint64),
+                ("initialization_seconds", C.c_double), ("search_seconds", C.c_double),
+                ("time_to_solution_seconds", C.c_double), ("device", _DeviceInfo)]
+
+
+class JobSpec(C.Structure):
+    """One search W(n,w) of a batch (xw_job_spec)."""
+    _fields_ = [("n", C.c_int32), ("w", C.c_int32), ("seed", C.c_uint64), ("replicas", C.c_int32),
+                ("reserved", C.c_int32), ("max_moves", C.c_uint64)]
+
+
+class JobResult(C.Structure):
+    _fields_ = [("score", C.c_int64), ("conflicts", C.c_int64), ("best_replica", C.c_int32),
+                ("solved", C.c_int32), ("verified", C.c_int32), ("error", C.c_int32),
+                ("moves", C.c_uint64), ("candidate_evaluations", C.c_uint64),
+                ("iterations", C.c_uint64), ("solved_iteration", C.c_uint64),
+                ("time_to_solution_seconds", C.c_double)]
+
+
+class ReplicaState(C.Structure):
+    _fields_ = [("iterations", C.c_uint64), ("moves", C.c_uint64),
+                ("candidate_evaluations", C.c_uint64), ("score", C.c_int64),
+                ("conflicts", C.c_int64), ("best_score", C.c_int64),
+                ("best_conflicts", C.c_int64), ("objective_total", C.c_int64),
+                ("temperature", C.c_double), ("reheat_temperature", C.c_double),
+                ("moves_since_improvement", C.c_int32), ("cooling_counter", C.c_int32),
+                ("rung", C.c_int32), ("objective_kind", C.c_int32), ("status", C.c_uint32),
+                ("error", C.c_uint32)]
+
+
+LOG_FN = C.CFUNCTYPE(None, C.c_char_p, C.c_void_p)
+CHECKPOINT_FN = C.CFUNCTYPE(None, C.POINTER(C.c_int8), C.c_int32, C.c_void_p)
+
+_lib = None
+
+
+def lib():
+    """The loaded libxw.so (raises if the library was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `make -C xtax_b200/csrc`")
+        L = C.CDLL(LIB_PATH)
+        P = C.POINTER
+        i32, u32, u64, i8 = C.c_int32, C.c_uint32, C.c_uint64, C.c_int8
+        sig = {
+            "xw_params_default": (None, [P(_Params)]),
+            "xw_last_error": (C.c_char_p, []),
+            "xw_validate_params": (i32, [i32, i32, P(_Params)]),
+            "xw_query_device": (i32, [i32, P(_DeviceInfo)]),
+            "xw_run": (i32, [i32, i32, P(_Params), P(i8), LOG_FN, CHECKPOINT_FN, C.c_void_p,
+                             P(_Result), P(i8)]),
+            "xw_request_stop": (None, []),
+            "xw_clear_stop": (None, []),
+            "xw_random_start": (i32, [i32, i32, u32, P(i8)]),
+            "xw_row_start": (i32, [i32, i32, u64, u32, P(i8)]),
+            "xw_sylvester": (i32, [i32, i32, P(i8)]),
+            "xw_score": (i32, [i32, i32, P(i8), P(C.c_int64)]),
+            "xw_verify": (i32, [i32, i32, P(i8)]),
+            "xw_read_csv": (i32, [C.c_char_p, i32, i32, P(i8)]),
+            "xw_write_csv": (i32, [C.c_char_p, i32, P(i8)]),
+            "xw_impossibility_reason": (C.c_char_p, [i32, i32]),
+            "xw_calibrate": (C.c_double, [i32, i32, P(i8), P(_Params), u32]),
+            "xw_batch_create": (i32, [P(JobSpec), i32, P(_Params), P(i8), P(C.c_void_p)]),
+            "xw_batch_set_stream": (i32, [C.c_void_p, C.c_void_p]),
+            "xw_batch_reset": (i32, [C.c_void_p]),
+            "xw_batch_run": (i32, [C.c_void_p, u64]),
+            "xw_batch_synchronize": (i32, [C.c_void_p]),
+            "xw_batch_launch_times": (i32, [C.c_void_p, P(C.c_float), i32, P(i32)]),
+            "xw_batch_results": (i32, [C.c_void_p, P(JobResult), P(i8)]),
+            "xw_batch_read_replica": (i32, [C.c_void_p, i32, i32, P(ReplicaState), P(i8), P(i8),
+                                            P(C.c_uint8)]),
+            "xw_batch_shape": (i32, [C.c_void_p, P(i32), P(i32), P(i32)]),
+            "xw_batch_destroy": (None, [C.c_void_p]),
+            "xw_batch_solve": (i32, [P(JobSpec), i32, P(_Params), P(i8), u64, P(JobResult), P(i8)]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != XW_OK:
+        raise XwError(rc, lib().xw_last_error().decode())
+
+
+def _i8(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int8))
+
+
+# ---- the reference interface -------------------------------------------------
+
+@dataclass
+class Params:
+    """xweigh_cuda::Params (xweigh_cuda.hpp:14-44) plus extensions."""
+    device: int = 0
+    replicas: int = 0
+    moves_per_launch: int = 4096
+    seed: int = 0
+    max_seconds: float = 0.0
+    save_interval: float = 2.0
+    output: str = "best_W.csv"
+    sign_fraction: float = 0.5
+    double_sign_fraction: float = 0.25
+    switch_sign_fraction: float = 0.5
+    squared_objective_fraction: float = 0.25
+    parity_objective_fraction: float = 0.25
+    greedy_fraction: float = 0.5
+    candidate_samples: int = 4
+    target_fraction: float = 0.7
+    target_samples: int = 8
+    t_init: float = 0.0
+    t_min: float = 0.25
+    cooling: float = 0.999
+    moves_per_cool: int = 500
+    stuck_threshold: int = 50000
+    reheat: float = 1.0
+    restart_interval: float = 5.0
+    restart_fraction: float = 0.25
+    restart_kick_min: int = 2
+    restart_kick_max: int = 64
+    max_moves: int = 0
+    tempering: int = 0
+    exchange_interval: int = 10000
+    objective: int = -1
+    move_set: int = 0
+    start_kind: int = 0
+    stop_on_solve: int = 1
+    warps_per_block: int = 0
+
+    def to_c(self):
+        p = _Params()
+        lib().xw_params_default(C.byref(p))
+        for f in fields(self):
+            if f.name != "output":
+                setattr(p, f.name, getattr(self, f.name))
+        return p
+
+
+@dataclass
+class DeviceInfo:
+    name: str
+    ordinal: int
+    compute_major: int
+    compute_minor: int
+    multiprocessors: int
+    global_memory: int
+    max_shared_memory_per_block: int
+
+
+@dataclass
+class State:
+    """The best matrix of a run: column-major int8 entries (State::entries)."""
+    order: int
+    weight: int
+    entries: np.ndarray
+    score: int
+    conflicts: int
+
+    def solved(self):
+        return self.score == 0
+
+    def matrix(self):
+        """Row-major n x n view."""
+        return self.entries.reshape(self.order, self.order).T.copy()
+
+
+@dataclass
+class RunResult:
+    """xweigh_cuda::RunResult (xweigh_cuda.hpp:56-65) plus solve metadata."""
+    best: State
+    device: DeviceInfo
+    replicas: int = 0
+    moves: int = 0
+    candidate_evaluations: int = 0
+    restarted_replicas: int = 0
+    initialization_seconds: float = 0.0
+    search_seconds: float = 0.0
+    solved: bool = False
+    verified: bool = False
+    time_to_solution_seconds: float = -1.0
+    log: List[str] = field(default_factory=list)
+
+
+def _device_info(d):
+    return DeviceInfo(d.name.decode(), d.ordinal, d.compute_major, d.compute_minor,
+                      d.multiprocessors, d.global_memory, d.max_shared_memory_per_block)
+
+
+def query_device(ordinal: int = 0) -> DeviceInfo:
+    """xweigh_cuda::query_device (xweigh_cuda.cu:1382-1417)."""
+    d = _DeviceInfo()
+    _check(lib().xw_query_device(ordinal, C.byref(d)))
+    return _device_info(d)
+
+
+def validate_params(order: int, weight: int, params: Params):
+    _check(lib().xw_validate_params(order, weight, C.byref(params.to_c())))
+
+
+def run_annealer(order: int, weight: int, params: Params,
+                 initial_state: Optional[np.ndarray] = None, echo=False) -> RunResult:
+    """xweigh_cuda::run_annealer (xweigh_cuda.cu:1419-2436)."""
+    lines = []
+
+    def on_log(line, _user):
+        s = line.decode()
+        lines.append(s)
+        if echo:
+            print(s, flush=True)
+
+    log_cb = LOG_FN(on_log)
+    ck_cb = CHECKPOINT_FN(lambda *_: None)
+    res = _Result()
+    best = np.zeros(order * order, dtype=np.int8)
+    start = None
+    if initial_state is not None:
+        start = np.ascontiguousarray(initial_state, dtype=np.int8).reshape(-1)
+    rc = lib().xw_run(order, weight, C.byref(params.to_c()), _i8(start) if start is not None else None,
+                      log_cb, ck_cb, None, C.byref(res), _i8(best))
+    _check(rc)
+    return RunResult(State(order, weight, best, res.score, res.conflicts), _device_info(res.device),
+                     res.replicas, res.moves, res.candidate_evaluations, res.restarted_replicas,
+                     res.initialization_seconds, res.search_seconds, bool(res.solved),
+                     bool(res.verified), res.time_to_solution_seconds, lines)
+
+
+# ---- host helpers ----------------------------------------------------------------
+
+def random_start(n, w, seed):
+    out = np.zeros(n * n, dtype=np.int8)
+    _check(lib().xw_random_start(n, w, seed & 0xffffffff, _i8(out)))
+    return out
+
+
+def row_start(n, w, seed, replica):
+    out = np.zeros(n * n, dtype=np.int8)
+    _check(lib().xw_row_start(n, w, seed, replica, _i8(out)))
+    return out
+
+
+def sylvester(n, w):
+    out = np.zeros(n * n, dtype=np.int8)
+    _check(lib().xw_sylvester(n, w, _i8(out)))
+    return out
+
+
+def score(n, w, W):
+    W = np.ascontiguousarray(W, dtype=np.int8)
+    st = np.zeros(4, dtype=np.int64)
+    _check(lib().xw_score(n, w, _i8(W), st.ctypes.data_as(C.POINTER(C.c_int64))))
+    return st
+
+
+def verify(n, w, W):
+    W = np.ascontiguousarray(W, dtype=np.int8)
+    return lib().xw_verify(n, w, _i8(W))
+
+
+def impossibility_reason(n, w):
+    return lib().xw_impossibility_reason(n, w).decode()
+
+
+def philox_key(seed):
+    """Philox key of a job: the reference's curand seed derivation
+    (xweigh_cuda.cu:1724-1727) split into two 32-bit words."""
+    base = seed & 0xffffffff
+    k = ((base << 32) ^ seed ^ 0xd1b54a32d192ed03) & 0xffffffffffffffff
+    return k & 0xffffffff, k >> 32
+
+
+# ---- batches -------------------------------------------------------------------
+
+class Batch:
+    """A population of independent searches resident on one device."""
+
+    def __init__(self, jobs, params: Params, starts: Optional[np.ndarray] = None):
+        self.specs = (JobSpec * len(jobs))()
+        for i, j in enumerate(jobs):
+            s = self.specs[i]
+            s.n, s.w, s.seed, s.replicas = j["n"], j["w"], j.get("seed", 1), j["replicas"]
+            s.max_moves = j.get("max_moves", 0)
+        self.jobs = [dict(j) for j in jobs]
+        self.params = params
+        h = C.c_void_p()
+        st = None
+        if starts is not None:
+            st = np.ascontiguousarray(starts, dtype=np.int8).reshape(-1)
+        _check(lib().xw_batch_create(self.specs, len(jobs), C.byref(params.to_c()),
+                                     _i8(st) if st is not None else None, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().xw_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def set_stream(self, stream_ptr):
+        _check(lib().xw_batch_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def reset(self):
+        _check(lib().xw_batch_reset(self.h))
+
+    def run(self, iters):
+        _check(lib().xw_batch_run(self.h, iters))
+
+    def synchronize(self):
+        _check(lib().xw_batch_synchronize(self.h))
+
+    def launch_times(self):
+        cap = 4096
+        ms = (C.c_float * cap)()
+        cnt = C.c_int32()
+        _check(lib().xw_batch_launch_times(self.h, ms, cap, C.byref(cnt)))
+        return [ms[i] for i in range(min(cnt.value, cap))]
+
+    def shape(self):
+        a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
+        _check(lib().xw_batch_shape(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def results(self):
+        res = (JobResult * len(self.jobs))()
+        total = sum(j["n"] * j["n"] for j in self.jobs)
+        best = np.zeros(total, dtype=np.int8)
+        _check(lib().xw_batch_results(self.h, res, _i8(best)))
+        out, off = [], 0
+        for j, r in zip(self.jobs, res):
+            nn = j["n"] * j["n"]
+            out.append((r, best[off:off + nn].copy()))
+            off += nn
+        return out
+
+    def replica(self, job, r):
+        n, w = self.jobs[job]["n"], self.jobs[job]["w"]
+        m = min(w, n - w)
+        st = ReplicaState()
+        W = np.zeros(n * n, dtype=np.int8)
+        B = np.zeros(n * n, dtype=np.int8)
+        M = np.zeros(max(n * m, 1), dtype=np.uint8)
+        _check(lib().xw_batch_read_replica(self.h, job, r, C.byref(st), _i8(W), _i8(B),
+                                           M.ctypes.data_as(C.POINTER(C.c_uint8))))
+        return st, W, B, M[: n * m]
+
+
+def batch_solve(jobs, params: Params, starts=None, iters=0):
+    """xw_batch_solve: upload, run, read back through host buffers."""
+    specs = (JobSpec * len(jobs))()
+    for i, j in enumerate(jobs):
+        specs[i].n, specs[i].w, specs[i].seed, specs[i].replicas = j["n"], j["w"], j.get("seed", 1), j["replicas"]
+        specs[i].max_moves = j.get("max_moves", 0)
+    res = (JobResult * len(jobs))()
+    best = np.zeros(sum(j["n"] * j["n"] for j in jobs), dtype=np.int8)
+    st = None if starts is None else np.ascontiguousarray(starts, dtype=np.int8).reshape(-1)
+    _check(lib().xw_batch_solve(specs, len(jobs), C.byref(params.to_c()),
+                                _i8(st) if st is not None else None, iters, res, _i8(best)))
+    return list(res), best
+
+
+def header_symbols(path=HEADER):
+    """Function names declared in the public C header."""
+    import re
+    text = open(path).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(xw_[a-z0-9_]+)\s*\(", text)) - {"xw_log_fn", "xw_checkpoint_fn"})

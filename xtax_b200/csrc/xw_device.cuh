@@ -1,0 +1,103 @@
+// xw_device.cuh -- device-side building blocks shared by the annealing and
+// rescoring kernels: the Philox4x32-10 counter-based generator, the draw
+// layout, the deterministic acceptance exponential and the job / replica
+// record layouts in HBM.
+#pragma once
+
+#include <cstdint>
+
+#include "xw_layout.h"
+
+namespace xw {
+
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): ten rounds of
+// (hi0,lo0)=M0*c0, (hi1,lo1)=M1*c2, c'=(hi1^c1^k0, lo1, hi0^c3^k1, lo0),
+// with the key bumped by the Weyl constants between rounds.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x);
+        const uint32_t lo1 = 0xCD9E8D57u * c.z;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z);
+        c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+
+__device__ __forceinline__ uint32_t pick(uint4 v, int j) {
+    return j == 0 ? v.x : j == 1 ? v.y : j == 2 ? v.z : v.w;
+}
+
+// Draw layout (identical in the oracle): word j of
+// Philox(ctr = {slot, it_lo, it_hi, stream}, key).  slot 0 is the move-level
+// block, slot 1 + 128*c + b is block b of candidate c; retries of a rejected
+// index draw set slot bits 24..31 to the retry number.
+__device__ __forceinline__ uint32_t cand_slot(int c, int b) {
+    return 1u + 128u * (uint32_t)c + (uint32_t)b;
+}
+
+__device__ __forceinline__ uint4 draw_block(uint32_t slot, uint64_t it, uint32_t stream,
+                                            uint32_t k0, uint32_t k1) {
+    return philox4x32_10(make_uint4(slot, (uint32_t)it, (uint32_t)(it >> 32), stream), k0, k1);
+}
+
+// Lemire multiply-shift index in [0,count) from a 32-bit word; a word in the
+// rejection zone (probability < count/2^32) is replaced by the same word of
+// the retry counters.
+__device__ __forceinline__ bool lemire_ok(uint32_t v, uint32_t count, uint32_t& out) {
+    const uint64_t prod = (uint64_t)v * count;
+    const uint32_t low = (uint32_t)prod;
+    out = (uint32_t)(prod >> 32);
+    return low >= count || low >= (0u - count) % count;
+}
+
+__device__ __noinline__ uint32_t lemire_retry(uint32_t slot, uint64_t it, uint32_t stream,
+                                              uint32_t k0, uint32_t k1, int j, uint32_t count) {
+    uint32_t out = 0;
+    for (uint32_t retry = 1; retry <= 255; ++retry) {
+        const uint4 b = draw_block((slot & 0x00ffffffu) | (retry << 24), it, stream, k0, k1);
+        const uint32_t v = pick(b, j);
+        if (lemire_ok(v, count, out) || retry == 255) return out;
+    }
+    return out;
+}
+
+// exp(x) for x <= 0 by Cody-Waite reduction and a degree-14 Taylor
+// polynomial, every step an explicitly rounded IEEE operation so that the
+// CPU oracle (same operations, -ffp-contract=off) produces the same bits.
+__device__ __forceinline__ double acceptance_exp(double x) {
+    if (x >= 0.0) return 1.0;
+    if (!(x > -40.0)) return (x > -745.0) ? 0x1p-60 : 0.0;
+    const double k = rint(__dmul_rn(x, 0x1.71547652b82fep+0));
+    double r = __fma_rn(-k, 0x1.62e42fee00000p-1, x);
+    r = __fma_rn(-k, 0x1.a39ef35793c76p-33, r);
+    double p = 0x1.93974a8c07c9dp-37;
+    p = __fma_rn(p, r, 0x1.6124613a86d09p-33);
+    p = __fma_rn(p, r, 0x1.1eed8eff8d898p-29);
+    p = __fma_rn(p, r, 0x1.ae64567f544e4p-26);
+    p = __fma_rn(p, r, 0x1.27e4fb7789f5cp-22);
+    p = __fma_rn(p, r, 0x1.71de3a556c734p-19);
+    p = __fma_rn(p, r, 0x1.a01a01a01a01ap-16);
+    p = __fma_rn(p, r, 0x1.a01a01a01a01ap-13);
+    p = __fma_rn(p, r, 0x1.6c16c16c16c17p-10);
+    p = __fma_rn(p, r, 0x1.1111111111111p-7);
+    p = __fma_rn(p, r, 0x1.5555555555555p-5);
+    p = __fma_rn(p, r, 0x1.5555555555555p-3);
+    p = __fma_rn(p, r, 0x1.0000000000000p-1);
+    p = __fma_rn(p, r, 1.0);
+    p = __fma_rn(p, r, 1.0);
+    const double scale = __longlong_as_double((long long)(1023 + (int)k) << 52);
+    return __dmul_rn(p, scale);
+}
+
+// Metropolis test u*2^-32 < exp(-delta/T), delta > 0.
+__device__ __forceinline__ bool metropolis_accept(int64_t delta, double temperature, uint32_t u) {
+    const double t = temperature > 1.0e-12 ? temperature : 1.0e-12;
+    const double x = __ddiv_rn(-(double)delta, t);
+    return __dmul_rn((double)u, 0x1p-32) < acceptance_exp(x);
+}
+
+}  // namespace xw

@@ -1,0 +1,1000 @@
+// xw_host.cpp -- host orchestration and the C ABI (include/xw.h).
+//
+// Replaces the host half of src/xweigh_cuda.cu (validate_params :1160,
+// query_device :1382, run_annealer :1419) with a batch engine: any number of
+// independent searches ("jobs") share one device arena of replica records
+// and one persistent anneal launch per round; rounds are captured into a
+// CUDA graph; results come back through a device-side collection kernel so
+// the host reads a few bytes per job instead of whole populations.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/xw.h"
+#include "xw_cpu.h"
+#include "xw_host_internal.h"
+#include "xw_kernels.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+std::atomic<int> g_stop{0};
+
+int32_t fail(int32_t code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+std::string fmt(const char* f, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, f);
+    vsnprintf(buf, sizeof buf, f, ap);
+    va_end(ap);
+    return buf;
+}
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+void check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess)
+        throw CudaError(fmt("%s failed: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e)));
+}
+
+uint64_t coin_threshold(double p) {
+    if (!(p > 0.0)) return 0;
+    if (p >= 1.0) return 4294967296ull;
+    return (uint64_t)std::ceil(p * 4294967296.0);
+}
+
+template <typename F>
+void parallel_for(int count, F f) {
+    const int threads = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(), count / 16 + 1));
+    if (threads <= 1) {
+        for (int i = 0; i < count; ++i) f(i);
+        return;
+    }
+    std::vector<std::thread> pool;
+    std::atomic<int> next{0};
+    std::exception_ptr err;
+    std::atomic<bool> failed{false};
+    for (int t = 0; t < threads; ++t)
+        pool.emplace_back([&]() {
+            for (;;) {
+                const int i = next.fetch_add(1);
+                if (i >= count || failed.load()) return;
+                try {
+                    f(i);
+                } catch (...) {
+                    if (!failed.exchange(true)) err = std::current_exception();
+                }
+            }
+        });
+    for (auto& th : pool) th.join();
+    if (err) std::rethrow_exception(err);
+}
+
+}  // namespace
+
+namespace xw {
+
+std::string validate(int n, int w, const xw_params& p) {
+    if (n < 1 || n > 32767) return "CUDA xweigh order is out of range";
+    if (w < 1 || w > n) return "CUDA xweigh weight must be in [1, n]";
+    if (p.replicas < 0) return "CUDA replica count must be nonnegative";
+    if (p.moves_per_launch < 1) return "CUDA moves per launch must be positive";
+    if (p.max_seconds < 0.0) return "CUDA max seconds must be nonnegative";
+    if (p.save_interval < 0.0) return "CUDA save interval must be nonnegative";
+    if (p.sign_fraction < 0.0 || p.sign_fraction > 1.0) return "CUDA sign fraction must be in [0, 1]";
+    if (p.double_sign_fraction < 0.0 || p.double_sign_fraction > 1.0)
+        return "CUDA double-sign fraction must be in [0, 1]";
+    if (p.switch_sign_fraction < 0.0 || p.switch_sign_fraction > 1.0)
+        return "CUDA switch-sign fraction must be in [0, 1]";
+    if (p.squared_objective_fraction < 0.0 || p.squared_objective_fraction > 1.0)
+        return "CUDA squared-objective fraction must be in [0, 1]";
+    if (p.parity_objective_fraction < 0.0 || p.parity_objective_fraction > 1.0)
+        return "CUDA parity-objective fraction must be in [0, 1]";
+    if (p.squared_objective_fraction + p.parity_objective_fraction > 1.0)
+        return "CUDA alternate objective fractions must sum to at most 1";
+    if (p.greedy_fraction < 0.0 || p.greedy_fraction > 1.0) return "CUDA greedy fraction must be in [0, 1]";
+    if (p.target_fraction < 0.0 || p.target_fraction > 1.0) return "CUDA target fraction must be in [0, 1]";
+    if (p.candidate_samples < 1 || p.candidate_samples > XW_MAX_CANDIDATE_SAMPLES)
+        return "CUDA candidate samples must be in [1, MAX_CANDIDATE_SAMPLES]";
+    if (p.target_samples < 1 || p.target_samples > XW_MAX_TARGET_SAMPLES)
+        return "CUDA target samples must be in [1, MAX_TARGET_SAMPLES]";
+    if (p.t_init < 0.0) return "CUDA initial temperature must be nonnegative";
+    if (p.t_min <= 0.0) return "CUDA minimum temperature must be positive";
+    if (p.cooling <= 0.0 || p.cooling >= 1.0) return "CUDA cooling factor must be in (0, 1)";
+    if (p.moves_per_cool < 1) return "CUDA moves per cool must be positive";
+    if (p.stuck_threshold < 1) return "CUDA stuck threshold must be positive";
+    if (p.reheat <= 0.0) return "CUDA reheat factor must be positive";
+    if (p.restart_interval < 0.0) return "CUDA restart interval must be nonnegative";
+    if (p.restart_fraction <= 0.0 || p.restart_fraction > 1.0) return "CUDA restart fraction must be in (0, 1]";
+    if (p.restart_kick_min < 0) return "CUDA minimum restart kick must be nonnegative";
+    if (p.restart_kick_max < p.restart_kick_min) return "CUDA maximum restart kick must be at least the minimum";
+    if (p.exchange_interval < 1) return "CUDA exchange interval must be positive";
+    if (p.objective < -1 || p.objective > 2) return "CUDA objective must be -1, 0, 1 or 2";
+    if (p.move_set < 0 || p.move_set > 1) return "CUDA move set must be 0 or 1";
+    if (p.start_kind < 0 || p.start_kind > 1) return "CUDA start kind must be 0 or 1";
+    if (p.warps_per_block < 0 || p.warps_per_block > 16) return "CUDA warps per block must be in [0, 16]";
+    return {};
+}
+
+// ------------------------------------------------------------------------
+// Batch: device arena of replica records for a set of jobs.
+
+Batch::~Batch() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    for (auto e : events) cudaEventDestroy(e);
+    for (void* ptr : {d_jobs, d_jobs0, d_arena, d_arena0, d_rec_off, d_items, d_counters, d_ladder,
+                      d_out, d_best_off, d_best, d_t0})
+        if (ptr) cudaFree(ptr);
+    if (own_stream && stream) cudaStreamDestroy(stream);
+}
+
+static size_t record_bytes(int n, int m) {
+    const uint32_t nn = xw_pad16((uint32_t)(n * n));
+    const size_t b = 128 + 2 * (size_t)nn + xw_pad16((uint32_t)(n * m));
+    return (b + 127) & ~size_t(127);
+}
+
+void Batch::build(const xw_job_spec* specs, int njobs, const xw_params& p, const int8_t* starts) {
+    params = p;
+    check(cudaSetDevice(p.device), "cudaSetDevice");
+    check(cudaGetDeviceProperties(&props, p.device), "cudaGetDeviceProperties");
+    if (njobs < 1) throw std::invalid_argument("batch needs at least one job");
+    jobs.resize(njobs);
+    rep_seed.resize(njobs);
+    size_t arena = 0;
+    uint32_t rep = 0;
+    size_t best_off = 0;
+    best_offsets.resize(njobs);
+    int max_opl = 1;
+    slot_bytes = 0;
+    tempering = p.tempering != 0;
+    for (int j = 0; j < njobs; ++j) {
+        const xw_job_spec& s = specs[j];
+        if (s.n < 1 || s.n > XW_MAX_ORDER_CUDA)
+            throw std::invalid_argument(fmt("job %d: order %d is outside [1, %d] of the device path", j, s.n,
+                                            XW_MAX_ORDER_CUDA));
+        if (s.w < 1 || s.w > s.n) throw std::invalid_argument(fmt("job %d: weight must be in [1, n]", j));
+        if (s.replicas < 1) throw std::invalid_argument(fmt("job %d: replica count must be positive", j));
+        if (tempering && s.replicas > XW_MAX_RUNGS)
+            throw std::invalid_argument(fmt("job %d: a tempering ladder has at most %d rungs", j, XW_MAX_RUNGS));
+        XwJob& J = jobs[j];
+        std::memset(&J, 0, sizeof J);
+        J.n = s.n;
+        J.w = s.w;
+        J.m = std::min(s.w, s.n - s.w);
+        J.sparse = s.w <= s.n - s.w;
+        J.tempering = tempering;
+        J.move_set = p.move_set;
+        J.candidate_samples = p.candidate_samples;
+        J.target_samples = p.target_samples;
+        J.moves_per_cool = p.moves_per_cool;
+        J.stuck_threshold = p.stuck_threshold;
+        J.objective = p.objective;
+        J.replicas = s.replicas;
+        // the Philox key follows the reference's curand seed derivation
+        // (xweigh_cuda.cu:1724-1727)
+        const uint32_t base = (uint32_t)s.seed;
+        const uint64_t key = ((uint64_t)base << 32) ^ s.seed ^ 0xd1b54a32d192ed03ull;
+        J.key0 = (uint32_t)key;
+        J.key1 = (uint32_t)(key >> 32);
+        J.rep_begin = rep;
+        const uint32_t nn = xw_pad16((uint32_t)(s.n * s.n));
+        J.off_w = 128;
+        J.off_best = 128 + nn;
+        J.off_mino = 128 + 2 * nn;
+        J.record_bytes = (uint32_t)record_bytes(s.n, J.m);
+        J.thr_greedy = coin_threshold(p.greedy_fraction);
+        J.thr_target = coin_threshold(p.target_fraction);
+        J.thr_double = p.move_set == 0 ? coin_threshold(p.double_sign_fraction) : 0;
+        J.thr_sign = coin_threshold(p.sign_fraction);
+        J.thr_swsign = coin_threshold(p.switch_sign_fraction);
+        J.t_min = p.t_min;
+        J.cooling = p.cooling;
+        J.reheat = p.reheat;
+        const uint64_t budget = s.max_moves ? s.max_moves : p.max_moves;
+        J.budget_iters = budget ? (budget + (uint64_t)s.replicas - 1) / (uint64_t)s.replicas : 0;
+        rep_seed[j] = base;
+        rep += (uint32_t)s.replicas;
+        arena += (size_t)s.replicas * J.record_bytes;
+        best_offsets[j] = best_off;
+        best_off += (size_t)s.n * s.n;
+        max_opl = std::max(max_opl, anneal_opl(s.n));
+        slot_bytes = std::max(slot_bytes, anneal_slot_bytes(s.n, J.m));
+    }
+    total_replicas = rep;
+    best_bytes = best_off;
+    opl = max_opl;
+
+    // host records
+    std::vector<uint8_t> host((size_t)arena, 0);
+    rec_off.resize(total_replicas);
+    ladder.clear();
+    size_t off = 0;
+    size_t start_off = 0;
+    t_init_used.assign(njobs, 0.0);
+    for (int j = 0; j < njobs; ++j) {
+        XwJob& J = jobs[j];
+        const int R = J.replicas, n = J.n, w = J.w;
+        std::vector<std::vector<int8_t>> W(R);
+        std::vector<double> t0s(1, p.t_init);
+        auto start_of = [&](int r) -> std::vector<int8_t> {
+            if (starts) return std::vector<int8_t>(starts + start_off + (size_t)r * n * n,
+                                                   starts + start_off + (size_t)(r + 1) * n * n);
+            if (p.start_kind == 1) return row_start(n, w, J.key0, J.key1, (uint32_t)r);
+            return CpuState::random_start(n, w, rep_seed[j] + (uint32_t)r * 0x9e3779b9u).entries();
+        };
+        parallel_for(R, [&](int r) { W[r] = start_of(r); });
+        if (starts) start_off += (size_t)R * n * n;
+        // calibrate_temperature on replica 0 (xweigh_cuda.cu:1563-1567)
+        double t_init = p.t_init;
+        if (t_init <= 0.0) {
+            CpuParams cp;
+            cp.sign_fraction = p.sign_fraction;
+            cp.target_fraction = p.target_fraction;
+            cp.target_samples = p.target_samples;
+            // the reference calibrates on replica 0's State as random_start
+            // left it (minority lists in switch order) or as read from CSV
+            const CpuState s0 = (!starts && p.start_kind == 0) ? CpuState::random_start(n, w, rep_seed[j])
+                                                               : CpuState::from_entries(n, w, W[0]);
+            t_init = calibrate_temperature(s0, cp, rep_seed[j]);
+        }
+        t_init_used[j] = t_init;
+        // geometric ladder from min(t_min, t_init) to t_init (xweigh_cuda.cu:1580-1594)
+        const double bottom = std::min(p.t_min, t_init);
+        const double ratio = R > 1 ? std::pow(t_init / std::max(bottom, 1.0e-12), 1.0 / (double)(R - 1)) : 1.0;
+        std::vector<double> temps(R);
+        double t = bottom;
+        for (int r = 0; r < R; ++r) {
+            temps[r] = t;
+            t *= ratio;
+        }
+        J.ladder_off = ladder.size();
+        if (tempering) ladder.insert(ladder.end(), temps.begin(), temps.end());
+        for (int r = 0; r < R; ++r) {
+            rec_off[J.rep_begin + r] = off;
+            RepHeader* H = reinterpret_cast<RepHeader*>(host.data() + off);
+            std::memset(H, 0, sizeof *H);
+            H->job = (uint32_t)j;
+            H->stream = (uint32_t)r;
+            H->temperature = temps[r];
+            H->reheat_temperature = temps[r];
+            H->rung = r;
+            if (p.objective >= 0) {
+                H->obj_kind = p.objective;
+            } else {
+                const uint32_t h = (uint32_t)r * 0x9e3779b9u + 0x85ebca6bu;
+                const double choice = (double)h * (1.0 / 4294967296.0);
+                H->obj_kind = choice < p.squared_objective_fraction ? 1
+                    : choice < p.squared_objective_fraction + p.parity_objective_fraction ? 2 : 0;
+            }
+            if (W[r].size() != (size_t)n * n) throw std::invalid_argument("start state size mismatch");
+            std::memcpy(host.data() + off + J.off_w, W[r].data(), (size_t)n * n);
+            std::memcpy(host.data() + off + J.off_best, W[r].data(), (size_t)n * n);
+            off += J.record_bytes;
+        }
+    }
+    if (ladder.empty()) ladder.push_back(0.0);
+
+    // work items: longest replicas first (cost grows with n)
+    items.resize(total_replicas);
+    for (uint32_t i = 0; i < total_replicas; ++i) items[i] = i;
+    std::vector<int> job_of(total_replicas);
+    for (int j = 0; j < njobs; ++j)
+        for (int r = 0; r < jobs[j].replicas; ++r) job_of[jobs[j].rep_begin + r] = j;
+    std::stable_sort(items.begin(), items.end(), [&](uint32_t a, uint32_t b) {
+        return jobs[job_of[a]].n > jobs[job_of[b]].n;
+    });
+
+    arena_bytes = arena;
+    auto dmalloc = [&](void** ptr, size_t bytes, const char* what) {
+        check(cudaMalloc(ptr, std::max<size_t>(bytes, 16)), what);
+    };
+    size_t free_b = 0, total_b = 0;
+    check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    const size_t need = 2 * arena + 2 * sizeof(XwJob) * njobs + 8 * total_replicas + best_bytes;
+    if (need > free_b)
+        throw std::length_error(fmt("CUDA replica state requires %g MiB, but only %g MiB is free",
+                                    need / 1048576.0, free_b / 1048576.0));
+    if (!stream) {
+        check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        own_stream = true;
+    }
+    dmalloc(&d_jobs, sizeof(XwJob) * njobs, "cudaMalloc jobs");
+    dmalloc(&d_jobs0, sizeof(XwJob) * njobs, "cudaMalloc jobs");
+    dmalloc(&d_arena, arena, "cudaMalloc replica records");
+    dmalloc(&d_arena0, arena, "cudaMalloc replica records");
+    dmalloc(&d_rec_off, sizeof(uint64_t) * total_replicas, "cudaMalloc record offsets");
+    dmalloc(&d_items, sizeof(uint32_t) * total_replicas, "cudaMalloc items");
+    dmalloc(&d_ladder, sizeof(double) * ladder.size(), "cudaMalloc ladder");
+    dmalloc(&d_out, sizeof(JobOut) * njobs, "cudaMalloc results");
+    dmalloc(&d_best_off, sizeof(uint64_t) * njobs, "cudaMalloc result offsets");
+    dmalloc(&d_best, best_bytes, "cudaMalloc best states");
+    dmalloc(&d_t0, sizeof(uint64_t), "cudaMalloc clock");
+    check(cudaMemcpyAsync(d_jobs0, jobs.data(), sizeof(XwJob) * njobs, cudaMemcpyHostToDevice, stream), "upload jobs");
+    check(cudaMemcpyAsync(d_arena0, host.data(), arena, cudaMemcpyHostToDevice, stream), "upload records");
+    check(cudaMemcpyAsync(d_rec_off, rec_off.data(), sizeof(uint64_t) * total_replicas, cudaMemcpyHostToDevice, stream),
+          "upload offsets");
+    check(cudaMemcpyAsync(d_items, items.data(), sizeof(uint32_t) * total_replicas, cudaMemcpyHostToDevice, stream),
+          "upload items");
+    check(cudaMemcpyAsync(d_ladder, ladder.data(), sizeof(double) * ladder.size(), cudaMemcpyHostToDevice, stream),
+          "upload ladder");
+    check(cudaMemcpyAsync(d_best_off, best_offsets.data(), sizeof(uint64_t) * njobs, cudaMemcpyHostToDevice, stream),
+          "upload result offsets");
+    reset();
+    check(cudaStreamSynchronize(stream), "cudaStreamSynchronize upload");
+    configure_shape(p.warps_per_block);
+}
+
+void Batch::configure_shape(int wpb) {
+    const void* fn = anneal_kernel_fn(opl);
+    int optin = 0;
+    check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, params.device),
+          "cudaDeviceGetAttribute max opt-in shared memory");
+    if (slot_bytes > (uint32_t)optin)
+        throw std::length_error(fmt("CUDA replica requires %.2f KiB of shared memory, but device %d permits "
+                                    "%.2f KiB per opt-in block",
+                                    slot_bytes / 1024.0, params.device, optin / 1024.0));
+    if (wpb <= 0) wpb = tuned_warps_per_block(opl, slot_bytes, params.device);
+    wpb = std::max(1, std::min(wpb, std::min(16, (int)(optin / slot_bytes))));
+    const size_t smem = (size_t)wpb * slot_bytes;
+    check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+          "cudaFuncSetAttribute max dynamic shared memory");
+    int per_sm = 0;
+    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * wpb, smem),
+          "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (per_sm < 1) throw std::length_error("CUDA anneal kernel has zero occupancy on the selected device");
+    warps_per_block = wpb;
+    blocks_per_sm = per_sm;
+    const int want = (int)((total_replicas + wpb - 1) / wpb);
+    blocks = std::max(1, std::min(want, per_sm * props.multiProcessorCount));
+    if (graph_exec) {
+        cudaGraphExecDestroy(graph_exec);
+        graph_exec = nullptr;
+    }
+}
+
+void Batch::reset() {
+    check(cudaMemcpyAsync(d_jobs, d_jobs0, sizeof(XwJob) * jobs.size(), cudaMemcpyDeviceToDevice, stream),
+          "reset jobs");
+    check(cudaMemcpyAsync(d_arena, d_arena0, arena_bytes, cudaMemcpyDeviceToDevice, stream), "reset records");
+    check(cudaMemsetAsync(d_t0, 0, sizeof(uint64_t), stream), "reset clock");
+}
+
+uint64_t Batch::round_iters() const {
+    return tempering ? (uint64_t)params.exchange_interval : (uint64_t)params.moves_per_launch;
+}
+
+void Batch::enqueue_rounds(uint64_t iters) {
+    const uint64_t per = round_iters();
+    const int rounds = (int)((iters + per - 1) / per);
+    if ((int)events.size() < 2 * rounds) {
+        while ((int)events.size() < 2 * rounds) {
+            cudaEvent_t e;
+            check(cudaEventCreate(&e), "cudaEventCreate");
+            events.push_back(e);
+        }
+    }
+    if (counters_cap < rounds) {
+        if (d_counters) cudaFree(d_counters);
+        check(cudaMalloc(&d_counters, sizeof(uint32_t) * rounds), "cudaMalloc counters");
+        counters_cap = rounds;
+    }
+    check(launch_mark_t0(static_cast<uint64_t*>(d_t0), stream), "launch mark_t0");
+    check(cudaMemsetAsync(d_counters, 0, sizeof(uint32_t) * rounds, stream), "cudaMemsetAsync counters");
+    uint64_t left = iters;
+    for (int k = 0; k < rounds; ++k) {
+        AnnealArgs a;
+        a.jobs = static_cast<XwJob*>(d_jobs);
+        a.arena = static_cast<uint8_t*>(d_arena);
+        a.rec_off = static_cast<const uint64_t*>(d_rec_off);
+        a.items = static_cast<const uint32_t*>(d_items);
+        a.n_items = total_replicas;
+        a.slot_bytes = slot_bytes;
+        a.counter = static_cast<uint32_t*>(d_counters) + k;
+        a.iters = std::min(left, per);
+        a.stop_on_solve = params.stop_on_solve;
+        a.pad = 0;
+        left -= a.iters;
+        check(cudaEventRecord(events[2 * k], stream), "cudaEventRecord");
+        check(launch_anneal(a, opl, warps_per_block, blocks, stream), "launch anneal_kernel");
+        check(cudaEventRecord(events[2 * k + 1], stream), "cudaEventRecord");
+        if (tempering)
+            check(launch_exchange(static_cast<XwJob*>(d_jobs), (int)jobs.size(), static_cast<uint8_t*>(d_arena),
+                                  static_cast<const uint64_t*>(d_rec_off), static_cast<const double*>(d_ladder),
+                                  stream),
+                  "launch exchange_kernel");
+    }
+    last_rounds = rounds;
+}
+
+void Batch::run(uint64_t iters, bool use_graph) {
+    if (iters == 0) return;
+    if (!use_graph) {
+        enqueue_rounds(iters);
+        return;
+    }
+    if (!graph_exec || graph_iters != iters) {
+        if (graph_exec) {
+            cudaGraphExecDestroy(graph_exec);
+            graph_exec = nullptr;
+        }
+        cudaGraph_t g;
+        check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+        try {
+            enqueue_rounds(iters);
+        } catch (...) {
+            cudaStreamEndCapture(stream, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        check(cudaStreamEndCapture(stream, &g), "cudaStreamEndCapture");
+        const cudaError_t e = cudaGraphInstantiate(&graph_exec, g, 0);
+        cudaGraphDestroy(g);
+        check(e, "cudaGraphInstantiate");
+        graph_iters = iters;
+    }
+    check(cudaGraphLaunch(graph_exec, stream), "cudaGraphLaunch");
+}
+
+void Batch::collect(std::vector<JobOut>& out, int8_t* best_host, bool want_best) {
+    check(launch_collect(static_cast<const XwJob*>(d_jobs), (int)jobs.size(), static_cast<const uint8_t*>(d_arena),
+                         static_cast<const uint64_t*>(d_rec_off), static_cast<const uint64_t*>(d_best_off),
+                         static_cast<JobOut*>(d_out), want_best ? static_cast<int8_t*>(d_best) : nullptr, stream),
+          "launch collect_kernel");
+    out.resize(jobs.size());
+    check(cudaMemcpyAsync(out.data(), d_out, sizeof(JobOut) * jobs.size(), cudaMemcpyDeviceToHost, stream),
+          "cudaMemcpy results to host");
+    if (want_best && best_host)
+        check(cudaMemcpyAsync(best_host, d_best, best_bytes, cudaMemcpyDeviceToHost, stream),
+              "cudaMemcpy best states to host");
+    check(cudaMemcpyAsync(&t0_host, d_t0, sizeof(uint64_t), cudaMemcpyDeviceToHost, stream), "cudaMemcpy clock");
+    check(cudaStreamSynchronize(stream), "cudaStreamSynchronize results");
+}
+
+void Batch::fill_results(const std::vector<JobOut>& out, const int8_t* best_host, xw_job_result* res) const {
+    for (size_t j = 0; j < jobs.size(); ++j) {
+        const JobOut& o = out[j];
+        xw_job_result& r = res[j];
+        std::memset(&r, 0, sizeof r);
+        r.score = o.score;
+        r.conflicts = o.conflicts;
+        r.best_replica = o.best_replica;
+        r.solved = o.score == 0;
+        r.error = o.err;
+        r.moves = o.moves;
+        r.candidate_evaluations = o.cand_evals;
+        r.iterations = o.iters;
+        r.solved_iteration = o.solved_it;
+        r.time_to_solution_seconds = (o.solved && o.solve_ns >= t0_host) ? (o.solve_ns - t0_host) * 1e-9 : -1.0;
+        if (best_host && r.solved) {
+            const int n = jobs[j].n;
+            std::vector<int8_t> e(best_host + best_offsets[j], best_host + best_offsets[j] + (size_t)n * n);
+            try {
+                r.verified = CpuState::from_entries(n, jobs[j].w, e).verify_weighing() ? 1 : 0;
+            } catch (const std::exception&) {
+                r.verified = 0;
+            }
+        }
+    }
+}
+
+}  // namespace xw
+
+// ==========================================================================
+// C ABI
+using namespace xw;
+
+extern "C" {
+
+void xw_params_default(xw_params* p) {
+    std::memset(p, 0, sizeof *p);
+    p->device = 0;
+    p->replicas = 0;
+    p->moves_per_launch = 4096;
+    p->seed = 0;
+    p->max_seconds = 0.0;
+    p->save_interval = 2.0;
+    p->sign_fraction = 0.5;
+    p->double_sign_fraction = 0.25;
+    p->switch_sign_fraction = 0.5;
+    p->squared_objective_fraction = 0.25;
+    p->parity_objective_fraction = 0.25;
+    p->greedy_fraction = 0.5;
+    p->candidate_samples = 4;
+    p->target_fraction = 0.7;
+    p->target_samples = 8;
+    p->t_init = 0.0;
+    p->t_min = 0.25;
+    p->cooling = 0.999;
+    p->moves_per_cool = 500;
+    p->stuck_threshold = 50000;
+    p->reheat = 1.0;
+    p->restart_interval = 5.0;
+    p->restart_fraction = 0.25;
+    p->restart_kick_min = 2;
+    p->restart_kick_max = 64;
+    p->max_moves = 0;
+    p->tempering = 0;
+    p->exchange_interval = 10000;
+    p->objective = -1;
+    p->move_set = 0;
+    p->start_kind = 0;
+    p->stop_on_solve = 1;
+    p->warps_per_block = 0;
+}
+
+const char* xw_last_error(void) { return g_last_error.c_str(); }
+
+int32_t xw_validate_params(int32_t n, int32_t w, const xw_params* p) {
+    if (!p) return fail(XW_ERR_INVALID, "null params");
+    const std::string e = validate(n, w, *p);
+    return e.empty() ? XW_OK : fail(XW_ERR_INVALID, e);
+}
+
+int32_t xw_query_device(int32_t ordinal, xw_device_info* out) {
+    if (!out) return fail(XW_ERR_INVALID, "null output");
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess)
+        return fail(XW_ERR_CUDA, fmt("cudaGetDeviceCount failed: %s (%s)", cudaGetErrorName(e), cudaGetErrorString(e)));
+    if (ordinal < 0 || ordinal >= count)
+        return fail(XW_ERR_INVALID,
+                    fmt("CUDA device ordinal %d is out of range; found %d device(s)", ordinal, count));
+    cudaDeviceProp prop{};
+    e = cudaGetDeviceProperties(&prop, ordinal);
+    if (e != cudaSuccess) return fail(XW_ERR_CUDA, fmt("cudaGetDeviceProperties failed: %s", cudaGetErrorString(e)));
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ordinal);
+    if (optin <= 0) optin = (int)prop.sharedMemPerBlock;
+    std::memset(out, 0, sizeof *out);
+    std::snprintf(out->name, sizeof out->name, "%s", prop.name);
+    out->ordinal = ordinal;
+    out->compute_major = prop.major;
+    out->compute_minor = prop.minor;
+    out->multiprocessors = prop.multiProcessorCount;
+    out->global_memory = prop.totalGlobalMem;
+    out->max_shared_memory_per_block = (uint64_t)optin;
+    return XW_OK;
+}
+
+void xw_request_stop(void) { g_stop.store(1, std::memory_order_relaxed); }
+void xw_clear_stop(void) { g_stop.store(0, std::memory_order_relaxed); }
+
+int32_t xw_random_start(int32_t n, int32_t w, uint32_t seed, int8_t* out) {
+    if (n < 1 || w < 1 || w > n || !out) return fail(XW_ERR_INVALID, "invalid W(n,w) or output");
+    const CpuState s = CpuState::random_start(n, w, seed);
+    std::memcpy(out, s.entries().data(), (size_t)n * n);
+    return XW_OK;
+}
+
+int32_t xw_row_start(int32_t n, int32_t w, uint64_t seed, uint32_t replica, int8_t* out) {
+    if (n < 1 || w < 1 || w > n || !out) return fail(XW_ERR_INVALID, "invalid W(n,w) or output");
+    const uint32_t base = (uint32_t)seed;
+    const uint64_t key = ((uint64_t)base << 32) ^ seed ^ 0xd1b54a32d192ed03ull;
+    const std::vector<int8_t> e = row_start(n, w, (uint32_t)key, (uint32_t)(key >> 32), replica);
+    std::memcpy(out, e.data(), e.size());
+    return XW_OK;
+}
+
+int32_t xw_sylvester(int32_t n, int32_t w, int8_t* out) {
+    if (n < 1 || w < 1 || w > n || !out || (w & (w - 1)) != 0 || n % w != 0)
+        return fail(XW_ERR_INVALID, "Sylvester blocks need w a power of two dividing n");
+    const CpuState s = CpuState::sylvester_blocks(n, w);
+    std::memcpy(out, s.entries().data(), (size_t)n * n);
+    return XW_OK;
+}
+
+int32_t xw_score(int32_t n, int32_t w, const int8_t* W, int64_t stats[4]) {
+    if (n < 1 || !W || !stats) return fail(XW_ERR_INVALID, "invalid arguments");
+    (void)w;
+    int64_t s = 0, c = 0, q = 0, par = 0;
+    for (int a = 0; a < n; ++a)
+        for (int b = a + 1; b < n; ++b) {
+            int64_t d = 0;
+            for (int k = 0; k < n; ++k) d += (int64_t)W[(size_t)k * n + a] * W[(size_t)k * n + b];
+            const int64_t ad = d < 0 ? -d : d;
+            s += ad;
+            c += d != 0;
+            q += d * d;
+            par += ad & 1;
+        }
+    stats[0] = s; stats[1] = c; stats[2] = q; stats[3] = par;
+    return XW_OK;
+}
+
+int32_t xw_verify(int32_t n, int32_t w, const int8_t* W) {
+    if (n < 1 || w < 1 || !W) return 0;
+    try {
+        const CpuState s = CpuState::from_entries(n, w, std::vector<int8_t>(W, W + (size_t)n * n));
+        if (!s.verify_support()) return 0;
+        return s.verify_weighing() ? 3 : 1;
+    } catch (const std::exception&) {
+        return 0;
+    }
+}
+
+int32_t xw_read_csv(const char* path, int32_t n, int32_t w, int8_t* out) {
+    if (!path || !out) return fail(XW_ERR_INVALID, "null argument");
+    try {
+        const std::vector<int8_t> e = read_csv(path, n, w);
+        std::memcpy(out, e.data(), e.size());
+        return XW_OK;
+    } catch (const std::exception& ex) {
+        return fail(XW_ERR_IO, ex.what());
+    }
+}
+
+int32_t xw_write_csv(const char* path, int32_t n, const int8_t* W) {
+    if (!path || !W || n < 1) return fail(XW_ERR_INVALID, "null argument");
+    try {
+        write_csv(std::vector<int8_t>(W, W + (size_t)n * n), n, path);
+        return XW_OK;
+    } catch (const std::exception& ex) {
+        return fail(XW_ERR_IO, ex.what());
+    }
+}
+
+const char* xw_impossibility_reason(int32_t n, int32_t w) {
+    static thread_local std::string reason;
+    reason = impossibility_reason(n, w);
+    return reason.c_str();
+}
+
+double xw_calibrate(int32_t n, int32_t w, const int8_t* W, const xw_params* p, uint32_t seed) {
+    try {
+        CpuParams cp;
+        cp.sign_fraction = p->sign_fraction;
+        cp.target_fraction = p->target_fraction;
+        cp.target_samples = p->target_samples;
+        cp.t_init = p->t_init;
+        const CpuState s = CpuState::from_entries(n, w, std::vector<int8_t>(W, W + (size_t)n * n));
+        return calibrate_temperature(s, cp, seed);
+    } catch (const std::exception& ex) {
+        g_last_error = ex.what();
+        return -1.0;
+    }
+}
+
+// ---- batches ---------------------------------------------------------------
+
+struct xw_batch {
+    std::unique_ptr<Batch> b;
+};
+
+#define XW_GUARD(...)                                                         \
+    try {                                                                     \
+        __VA_ARGS__                                                           \
+    } catch (const CudaError& ex) {                                           \
+        return fail(XW_ERR_CUDA, ex.what());                                  \
+    } catch (const std::length_error& ex) {                                   \
+        return fail(XW_ERR_CAPACITY, ex.what());                              \
+    } catch (const std::invalid_argument& ex) {                               \
+        return fail(XW_ERR_INVALID, ex.what());                               \
+    } catch (const std::bad_alloc&) {                                         \
+        return fail(XW_ERR_CAPACITY, "insufficient host memory");             \
+    } catch (const std::exception& ex) {                                      \
+        return fail(XW_ERR_INTERNAL, ex.what());                              \
+    }
+
+int32_t xw_batch_create(const xw_job_spec* jobs, int32_t njobs, const xw_params* p, const int8_t* starts,
+                        xw_batch** out) {
+    if (!jobs || !p || !out || njobs < 1) return fail(XW_ERR_INVALID, "invalid batch arguments");
+    for (int j = 0; j < njobs; ++j) {
+        const std::string e = validate(jobs[j].n, jobs[j].w, *p);
+        if (!e.empty()) return fail(XW_ERR_INVALID, e);
+    }
+    XW_GUARD({
+        auto h = std::make_unique<xw_batch>();
+        h->b = std::make_unique<Batch>();
+        h->b->build(jobs, njobs, *p, starts);
+        *out = h.release();
+        return XW_OK;
+    })
+}
+
+int32_t xw_batch_set_stream(xw_batch* h, void* s) {
+    if (!h) return fail(XW_ERR_INVALID, "null batch");
+    XW_GUARD({
+        Batch& b = *h->b;
+        check(cudaStreamSynchronize(b.stream), "cudaStreamSynchronize");
+        if (b.own_stream) cudaStreamDestroy(b.stream);
+        b.own_stream = s == nullptr;
+        if (s) b.stream = static_cast<cudaStream_t>(s);
+        else check(cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        if (b.graph_exec) {
+            cudaGraphExecDestroy(b.graph_exec);
+            b.graph_exec = nullptr;
+        }
+        return XW_OK;
+    })
+}
+
+int32_t xw_batch_reset(xw_batch* h) {
+    if (!h) return fail(XW_ERR_INVALID, "null batch");
+    XW_GUARD({
+        h->b->reset();
+        return XW_OK;
+    })
+}
+
+int32_t xw_batch_run(xw_batch* h, uint64_t iters) {
+    if (!h) return fail(XW_ERR_INVALID, "null batch");
+    XW_GUARD({
+        h->b->run(iters, true);
+        return XW_OK;
+    })
+}
+
+int32_t xw_batch_synchronize(xw_batch* h) {
+    if (!h) return fail(XW_ERR_INVALID, "null batch");
+    XW_GUARD({
+        check(cudaStreamSynchronize(h->b->stream), "cudaStreamSynchronize");
+        return XW_OK;
+    })
+}
+
+int32_t xw_batch_launch_times(xw_batch* h, float* ms, int32_t cap, int32_t* count) {
+    if (!h || !count) return fail(XW_ERR_INVALID, "null argument");
+    XW_GUARD({
+        Batch& b = *h->b;
+        check(cudaStreamSynchronize(b.stream), "cudaStreamSynchronize");
+        *count = b.last_rounds;
+        for (int k = 0; k < b.last_rounds && k < cap; ++k)
+            check(cudaEventElapsedTime(&ms[k], b.events[2 * k], b.events[2 * k + 1]), "cudaEventElapsedTime");
+        return XW_OK;
+    })
+}
+
+int32_t xw_batch_results(xw_batch* h, xw_job_result* results, int8_t* best) {
+    if (!h || !results) return fail(XW_ERR_INVALID, "null argument");
+    XW_GUARD({
+        Batch& b = *h->b;
+        std::vector<JobOut> out;
+        std::vector<int8_t> tmp;
+        int8_t* dst = best;
+        if (!dst) {
+            tmp.resize(b.best_bytes);
+            dst = tmp.data();
+        }
+        b.collect(out, dst, true);
+        b.fill_results(out, dst, results);
+        return XW_OK;
+    })
+}
+
+int32_t xw_batch_read_replica(xw_batch* h, int32_t job, int32_t replica, xw_replica_state* st, int8_t* W,
+                              int8_t* best_W, uint8_t* minority) {
+    if (!h) return fail(XW_ERR_INVALID, "null batch");
+    Batch& b = *h->b;
+    if (job < 0 || job >= (int)b.jobs.size()) return fail(XW_ERR_INVALID, "job index out of range");
+    const XwJob& J = b.jobs[job];
+    if (replica < 0 || replica >= J.replicas) return fail(XW_ERR_INVALID, "replica index out of range");
+    XW_GUARD({
+        std::vector<uint8_t> rec(J.record_bytes);
+        check(cudaStreamSynchronize(b.stream), "cudaStreamSynchronize");
+        check(cudaMemcpy(rec.data(), static_cast<uint8_t*>(b.d_arena) + b.rec_off[J.rep_begin + replica],
+                         J.record_bytes, cudaMemcpyDeviceToHost),
+              "cudaMemcpy replica to host");
+        const RepHeader* H = reinterpret_cast<const RepHeader*>(rec.data());
+        if (st) {
+            st->iterations = H->it;
+            st->moves = H->moves;
+            st->candidate_evaluations = H->cand_evals;
+            st->score = H->score;
+            st->conflicts = H->conflicts;
+            st->best_score = H->best_score;
+            st->best_conflicts = H->best_conflicts;
+            st->objective_total = H->obj_total;
+            st->temperature = H->temperature;
+            st->reheat_temperature = H->reheat_temperature;
+            st->moves_since_improvement = H->msi;
+            st->cooling_counter = H->cool_ctr;
+            st->rung = H->rung;
+            st->objective_kind = H->obj_kind;
+            st->status = H->status;
+            st->error = H->err;
+        }
+        const size_t nn = (size_t)J.n * J.n;
+        if (W) std::memcpy(W, rec.data() + J.off_w, nn);
+        if (best_W) std::memcpy(best_W, rec.data() + J.off_best, nn);
+        if (minority) std::memcpy(minority, rec.data() + J.off_mino, (size_t)J.n * J.m);
+        return XW_OK;
+    })
+}
+
+int32_t xw_batch_shape(xw_batch* h, int32_t* wpb, int32_t* blocks, int32_t* slot) {
+    if (!h) return fail(XW_ERR_INVALID, "null batch");
+    if (wpb) *wpb = h->b->warps_per_block;
+    if (blocks) *blocks = h->b->blocks;
+    if (slot) *slot = (int32_t)h->b->slot_bytes;
+    return XW_OK;
+}
+
+void xw_batch_destroy(xw_batch* h) { delete h; }
+
+int32_t xw_batch_solve(const xw_job_spec* jobs, int32_t njobs, const xw_params* p, const int8_t* starts,
+                       uint64_t iters, xw_job_result* results, int8_t* best) {
+    xw_batch* h = nullptr;
+    int32_t rc = xw_batch_create(jobs, njobs, p, starts, &h);
+    if (rc != XW_OK) return rc;
+    std::unique_ptr<xw_batch> guard(h);
+    XW_GUARD({
+        Batch& b = *h->b;
+        uint64_t target = iters;
+        if (target == 0) {
+            for (const XwJob& J : b.jobs) target = std::max<uint64_t>(target, J.budget_iters);
+            if (target == 0) return fail(XW_ERR_INVALID, "xw_batch_solve needs iters or a move budget");
+        }
+        b.run(target, false);
+        std::vector<JobOut> out;
+        std::vector<int8_t> tmp;
+        int8_t* dst = best;
+        if (!dst) {
+            tmp.resize(b.best_bytes);
+            dst = tmp.data();
+        }
+        b.collect(out, dst, true);
+        b.fill_results(out, dst, results);
+        return XW_OK;
+    })
+}
+
+// ---- xw_run: the xweigh_cuda run_annealer drop-in -------------------------
+
+int32_t xw_run(int32_t n, int32_t w, const xw_params* pin, const int8_t* start, xw_log_fn log,
+               xw_checkpoint_fn checkpoint, void* user, xw_result* out, int8_t* best_out) {
+    if (!pin || !out) return fail(XW_ERR_INVALID, "null argument");
+    xw_params p = *pin;
+    {
+        const std::string e = validate(n, w, p);
+        if (!e.empty()) return fail(XW_ERR_INVALID, e);
+    }
+    auto say = [&](const std::string& line) {
+        if (log) log(line.c_str(), user);
+    };
+    std::memset(out, 0, sizeof *out);
+    if (start) {
+        try {
+            const CpuState s = CpuState::from_entries(n, w, std::vector<int8_t>(start, start + (size_t)n * n));
+            if (!s.verify_support()) return fail(XW_ERR_INVALID, "CUDA initial state is not fixed-weight");
+        } catch (const std::exception&) {
+            return fail(XW_ERR_INVALID, "CUDA initial state is not fixed-weight");
+        }
+    }
+    int32_t rc = xw_query_device(p.device, &out->device);
+    if (rc != XW_OK) return rc;
+    if (n > XW_MAX_ORDER_CUDA) {
+        const double need = anneal_slot_bytes(std::min(n, 4096), std::min(w, n - w)) / 1024.0;
+        return fail(XW_ERR_CAPACITY,
+                    fmt("CUDA replica requires %.2f KiB of shared memory, but device %d permits %.2f KiB per "
+                        "opt-in block",
+                        need, p.device, out->device.max_shared_memory_per_block / 1024.0));
+    }
+    XW_GUARD({
+        check(cudaSetDevice(p.device), "cudaSetDevice");
+        const auto t_init0 = std::chrono::steady_clock::now();
+        if (p.seed == 0) p.seed = (uint64_t)std::random_device{}();
+        Batch b;
+        xw_job_spec spec{};
+        spec.n = n;
+        spec.w = w;
+        spec.seed = p.seed;
+        int replicas = p.replicas;
+        const int m = std::min(w, n - w);
+        const uint32_t slot = anneal_slot_bytes(n, m);
+        if (replicas == 0) {
+            // one resident wave: warp slots per SM times SMs
+            const int wpb = p.warps_per_block > 0 ? p.warps_per_block : 4;
+            int per_sm = 0;
+            const void* fn = anneal_kernel_fn(anneal_opl(n));
+            cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(wpb * slot));
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * wpb, (size_t)wpb * slot);
+            replicas = std::max(1, per_sm * wpb * out->device.multiprocessors);
+        }
+        if (p.tempering && replicas > XW_MAX_RUNGS) replicas = XW_MAX_RUNGS;
+        spec.replicas = replicas;
+        spec.max_moves = p.max_moves;
+        say(fmt("[cuda] device=%s compute=%d.%d multiprocessors=%d replicas=%d shared_kib=%g", out->device.name,
+                out->device.compute_major, out->device.compute_minor, out->device.multiprocessors, replicas,
+                slot / 1024.0));
+        std::vector<int8_t> starts;
+        if (start) {
+            starts.resize((size_t)replicas * n * n);
+            for (int r = 0; r < replicas; ++r) std::memcpy(starts.data() + (size_t)r * n * n, start, (size_t)n * n);
+        }
+        b.build(&spec, 1, p, start ? starts.data() : nullptr);
+        const double init_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_init0).count();
+        const double rec_mib = b.jobs[0].record_bytes / 1048576.0;
+        say(fmt("[init] seconds=%g replica_mib=%g total_replica_mib=%g", init_s, rec_mib, rec_mib * replicas));
+        std::vector<JobOut> res;
+        std::vector<int8_t> best((size_t)n * n);
+        b.collect(res, best.data(), true);
+        say(fmt("[t=0s] start score=%lld conflicts=%lld n=%d w=%d replicas=%d t_init=%g", (long long)res[0].score,
+                (long long)res[0].conflicts, n, w, replicas, b.t_init_used[0]));
+        int64_t gbest = res[0].score, gconf = res[0].conflicts;
+        int best_rep = res[0].best_replica;
+        const auto t0 = std::chrono::steady_clock::now();
+        double last_save = -1e300, last_progress = 0.0;
+        bool pending = true;
+        double solve_s = -1.0;
+        const uint64_t budget = b.jobs[0].budget_iters;
+        uint64_t done_iters = 0;
+        while (gbest != 0) {
+            const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            if (g_stop.load(std::memory_order_relaxed) || (p.max_seconds > 0.0 && el >= p.max_seconds)) break;
+            if (budget && done_iters >= budget) break;
+            uint64_t it = b.round_iters();
+            if (budget) it = std::min<uint64_t>(it, budget - done_iters);
+            b.run(it, false);
+            done_iters += it;
+            b.collect(res, best.data(), true);
+            const double now = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            if (res[0].err) throw std::runtime_error("CUDA replica failed its device self-check");
+            if (res[0].score < gbest || (res[0].score == gbest && res[0].conflicts < gconf)) {
+                gbest = res[0].score;
+                gconf = res[0].conflicts;
+                best_rep = res[0].best_replica;
+                pending = true;
+                say(fmt("[t=%gs] new best score=%lld conflicts=%lld (replica %d)", now, (long long)gbest,
+                        (long long)gconf, best_rep));
+                if (gbest == 0) solve_s = now;
+            }
+            if (pending && now - last_save >= p.save_interval) {
+                if (checkpoint) checkpoint(best.data(), n, user);
+                pending = false;
+                last_save = now;
+            }
+            if (now - last_progress >= 2.0 && gbest != 0) {
+                say(fmt("[t=%gs] moves=%llu best score=%lld conflicts=%lld", now, (unsigned long long)res[0].moves,
+                        (long long)gbest, (long long)gconf));
+                last_progress = now;
+            }
+        }
+        b.collect(res, best.data(), true);
+        const double search_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        const CpuState fin = CpuState::from_entries(n, w, best);
+        if (fin.score() != res[0].score || fin.conflicts() != res[0].conflicts)
+            throw std::runtime_error("CUDA final best snapshot score mismatch");
+        const uint64_t moves = res[0].moves, evals = res[0].cand_evals;
+        say(fmt("done moves=%llu candidate_evaluations=%llu seconds=%g moves_per_sec=%g "
+                "candidate_evaluations_per_sec=%g restarted_replicas=0",
+                (unsigned long long)moves, (unsigned long long)evals, search_s,
+                search_s > 0 ? moves / search_s : 0.0, search_s > 0 ? evals / search_s : 0.0));
+        out->score = res[0].score;
+        out->conflicts = res[0].conflicts;
+        out->replicas = replicas;
+        out->solved = res[0].score == 0;
+        out->verified = out->solved ? (fin.verify_weighing() ? 1 : 0) : 0;
+        out->best_replica = res[0].best_replica;
+        out->moves = moves;
+        out->candidate_evaluations = evals;
+        out->restarted_replicas = 0;
+        out->iterations = res[0].iters;
+        out->initialization_seconds = init_s;
+        out->search_seconds = search_s;
+        out->time_to_solution_seconds = solve_s;
+        if (best_out) std::memcpy(best_out, best.data(), best.size());
+        if (out->solved && !out->verified) return fail(XW_ERR_INTERNAL, "score reached zero but exact verification failed");
+        return XW_OK;
+    })
+}
+
+}  // extern "C"

@@ -1,0 +1,79 @@
+// xw_host_internal.h -- the batch engine shared by the C ABI entry points.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/xw.h"
+#include "xw_kernels.h"
+
+namespace xw {
+
+std::string validate(int n, int w, const xw_params& p);
+
+// Warps per block for the anneal kernel of a given lanes-per-row class and
+// shared-memory slot, from the autotuner's cache (xw_tune.cpp).
+int tuned_warps_per_block(int opl, uint32_t slot_bytes, int device);
+
+struct Batch {
+    xw_params params{};
+    cudaDeviceProp props{};
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+
+    std::vector<XwJob> jobs;
+    std::vector<uint32_t> rep_seed;
+    std::vector<uint64_t> rec_off;
+    std::vector<uint32_t> items;
+    std::vector<double> ladder;
+    std::vector<size_t> best_offsets;
+    std::vector<double> t_init_used;
+    uint32_t total_replicas = 0;
+    size_t arena_bytes = 0;
+    size_t best_bytes = 0;
+    bool tempering = false;
+
+    int opl = 1;
+    uint32_t slot_bytes = 0;
+    int warps_per_block = 4;
+    int blocks_per_sm = 1;
+    int blocks = 1;
+
+    void* d_jobs = nullptr;
+    void* d_jobs0 = nullptr;
+    void* d_arena = nullptr;
+    void* d_arena0 = nullptr;
+    void* d_rec_off = nullptr;
+    void* d_items = nullptr;
+    void* d_counters = nullptr;
+    int counters_cap = 0;
+    void* d_ladder = nullptr;
+    void* d_out = nullptr;
+    void* d_best_off = nullptr;
+    void* d_best = nullptr;
+    void* d_t0 = nullptr;
+    uint64_t t0_host = 0;
+
+    std::vector<cudaEvent_t> events;
+    int last_rounds = 0;
+    cudaGraphExec_t graph_exec = nullptr;
+    uint64_t graph_iters = 0;
+
+    Batch() = default;
+    Batch(const Batch&) = delete;
+    Batch& operator=(const Batch&) = delete;
+    ~Batch();
+
+    void build(const xw_job_spec* specs, int njobs, const xw_params& p, const int8_t* starts);
+    void configure_shape(int warps_per_block);
+    void reset();
+    uint64_t round_iters() const;
+    void enqueue_rounds(uint64_t iters);
+    void run(uint64_t iters, bool use_graph);
+    void collect(std::vector<JobOut>& out, int8_t* best_host, bool want_best);
+    void fill_results(const std::vector<JobOut>& out, const int8_t* best_host, xw_job_result* res) const;
+};
+
+}  // namespace xw

@@ -1,0 +1,51 @@
+// xw_kernels.h -- host-side declarations of the annealing kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "xw_layout.h"
+
+#define XW_MAX_RUNGS 256
+
+namespace xw {
+
+struct AnnealArgs {
+    XwJob* jobs;
+    uint8_t* arena;            // replica records
+    const uint64_t* rec_off;   // byte offset of each replica record
+    const uint32_t* items;     // replica ids this launch runs
+    uint32_t n_items;
+    uint32_t slot_bytes;       // shared memory per warp
+    uint32_t* counter;         // persistent work counter, zeroed per launch
+    uint64_t iters;            // iterations per replica this launch
+    int32_t stop_on_solve;
+    int32_t pad;
+};
+
+// shared-memory bytes one warp needs for a replica of order n, minority m
+uint32_t anneal_slot_bytes(int n, int m);
+// lanes' rows per lane: 1 for n <= 32, 2 for n <= 64, 4 for n <= 128
+int anneal_opl(int n);
+const void* anneal_kernel_fn(int opl);
+cudaError_t launch_anneal(const AnnealArgs& args, int opl, int warps_per_block, int blocks,
+                          cudaStream_t stream);
+cudaError_t launch_exchange(XwJob* jobs, int njobs, uint8_t* arena, const uint64_t* rec_off,
+                            const double* ladder, cudaStream_t stream);
+
+}  // namespace xw
+
+namespace xw {
+
+struct JobOut {
+    int64_t score, conflicts;
+    int32_t best_replica, solved, err, pad;
+    uint64_t moves, cand_evals, iters, solved_it, solve_ns;
+};
+
+cudaError_t launch_collect(const XwJob* jobs, int njobs, const uint8_t* arena, const uint64_t* rec_off,
+                           const uint64_t* best_out_off, JobOut* out, int8_t* best_out,
+                           cudaStream_t stream);
+cudaError_t launch_mark_t0(uint64_t* t0, cudaStream_t stream);
+
+}  // namespace xw

@@ -1,0 +1,80 @@
+// xw_layout.h -- HBM layout of annealing jobs and replica records, shared by
+// the host orchestrator and the kernels.
+//
+// A job is one independent search W(n,w) with its own Philox key: one
+// xweigh_cuda run, one tempering instance, or one served request.  Its
+// replicas are records in one byte arena:
+//
+//   [RepHeader 128 B][W: n*n int8, column-major][best W: n*n int8][minority: n*m u8]
+//
+// each section padded to 16 bytes.  The Gram matrix, the row residuals and
+// the row support masks are not stored: the kernel rebuilds them in shared
+// memory from W when it loads a replica (O(n^3/32) per lane, negligible next
+// to the thousands of moves per launch) and checks the rebuilt score against
+// the tracked one.
+#pragma once
+
+#include <stdint.h>
+
+#define XW_MAX_N 128
+#define XW_MAX_CANDIDATES 32
+#define XW_MAX_TARGET_SAMPLES 64
+
+#define XW_STATUS_INIT 1u      // record holds incremental state (score etc.)
+#define XW_STATUS_SOLVED 2u    // best score reached 0
+#define XW_ERR_SCORE 1u        // rebuilt score differs from the tracked one
+#define XW_ERR_MINORITY 2u     // W row weights disagree with the minority lists
+
+struct XwJob {
+    int32_t n, w, m, sparse;        // m = min(w, n-w); sparse = (w <= n-w)
+    int32_t tempering;              // 0 cooling/reheat, 1 fixed rung temperatures
+    int32_t move_set;               // 0 flip/switch/double, 1 flip/within-row swap
+    int32_t candidate_samples, target_samples;
+    int32_t moves_per_cool, stuck_threshold;
+    int32_t objective;              // -1 hash rule, else forced objective
+    int32_t replicas;               // R
+    uint32_t key0, key1;            // Philox key
+    uint32_t rep_begin;             // first replica id of the job
+    uint32_t record_bytes;
+    uint32_t off_w, off_best, off_mino;
+    uint32_t pad0;
+    uint64_t thr_greedy, thr_target, thr_double, thr_sign, thr_swsign;
+    double t_min, cooling, reheat;
+    uint64_t budget_iters;          // per-replica iteration cap, 0 = none
+    uint64_t exch_round;            // tempering exchange rounds done
+    uint64_t ladder_off;            // index of the first rung temperature
+    int32_t solved;                 // set on device when a replica solves
+    int32_t solved_replica;
+    uint64_t solved_it;
+    uint64_t solve_ns;              // %globaltimer at the solve
+    int32_t done;                   // host: job retired, skip its replicas
+    int32_t pad1;
+};
+
+struct RepHeader {
+    uint64_t it;                    // iterations run (the Philox counter)
+    uint64_t moves;                 // iterations with a valid candidate
+    uint64_t cand_evals;
+    int32_t score, conflicts;       // L1 score and conflicts of W
+    int32_t best_score, best_conflicts;
+    int64_t obj_total;              // total of the replica's own objective
+    double temperature, reheat_temperature;
+    int32_t msi, cool_ctr, rung, obj_kind;
+    uint32_t job, stream;           // job id; replica index within the job
+    uint32_t status, err;
+    uint64_t solve_it;
+    uint64_t solve_ns;
+    uint32_t pad[4];
+};
+
+#ifdef __cplusplus
+static_assert(sizeof(RepHeader) == 128, "replica header is 128 bytes");
+#endif
+
+#ifdef __CUDACC__
+#define XW_HD __host__ __device__
+#else
+#define XW_HD
+#endif
+
+static inline XW_HD uint32_t xw_pad16(uint32_t v) { return (v + 15u) & ~15u; }
