@@ -196,8 +196,12 @@ int32_t xw_batch_reset(xw_batch* b);
  * exchange launch when tempering), as one captured CUDA graph.  Returns
  * without waiting. */
 int32_t xw_batch_run(xw_batch* b, uint64_t iters);
+/* Same work as xw_batch_run, as plain stream launches with a CUDA event
+ * pair around every anneal launch (for per-launch timing). */
+int32_t xw_batch_run_timed(xw_batch* b, uint64_t iters);
 int32_t xw_batch_synchronize(xw_batch* b);
-/* Device milliseconds of each anneal launch of the last xw_batch_run. */
+/* Device milliseconds of each anneal launch of the last xw_batch_run_timed,
+ * or of the whole graph launch of the last xw_batch_run (count 1). */
 int32_t xw_batch_launch_times(xw_batch* b, float* ms, int32_t cap, int32_t* count);
 /* Results per job; best (nullable) receives each job's best W in job order. */
 int32_t xw_batch_results(xw_batch* b, xw_job_result* results, int8_t* best);

@@ -130,6 +130,7 @@ def lib():
             "xw_batch_set_stream": (i32, [C.c_void_p, C.c_void_p]),
             "xw_batch_reset": (i32, [C.c_void_p]),
             "xw_batch_run": (i32, [C.c_void_p, u64]),
+            "xw_batch_run_timed": (i32, [C.c_void_p, u64]),
             "xw_batch_synchronize": (i32, [C.c_void_p]),
             "xw_batch_launch_times": (i32, [C.c_void_p, P(C.c_float), i32, P(i32)]),
             "xw_batch_results": (i32, [C.c_void_p, P(JobResult), P(i8)]),
@@ -374,6 +375,9 @@ class Batch:
 
     def run(self, iters):
         _check(lib().xw_batch_run(self.h, iters))
+
+    def run_timed(self, iters):
+        _check(lib().xw_batch_run_timed(self.h, iters))
 
     def synchronize(self):
         _check(lib().xw_batch_synchronize(self.h))

@@ -4,8 +4,8 @@
 // int32 Gram, row residuals, minority lists and row support masks live in the
 // warp's shared-memory slot; lane o owns "other" rows o, o+32, ... of every
 // O(n) delta, so a candidate's exact change to W W^T and to the score is one
-// pass over registers and shared memory plus one redux.sync.  The whole
-// iteration is warp-synchronous: no __syncthreads, no block-wide reductions.
+// pass over shared memory plus one redux.sync.  The whole iteration is
+// warp-synchronous: no __syncthreads, no block-wide reductions.
 //
 // Per iteration (the semantics of the reference kernel anneal_kernel,
 // src/xweigh_cuda.cu:988-1130, with cuRAND replaced by counter-based Philox):
@@ -22,6 +22,14 @@
 //   G  the warp commits the move (commit_*, xweigh_cuda.cu:607-877);
 //   H  best tracking, cooling and reheat (xweigh_cuda.cu:1087-1129).
 //
+// Every move kind changes at most two rows of W, and each changed Gram row
+// is old + a*W[:,x] + b*W[:,y] for two columns x, y; evaluation and commit
+// run that one form (plus the row1-row2 pair term of a double flip over two
+// rows), so the hot loop has one code path instead of one per move kind.
+// Instruction-cache misses, not arithmetic, bound this kernel when the
+// per-kind paths are specialised and inlined; the proposal helpers are kept
+// out of line for the same reason.
+//
 // Work distribution is persistent: each warp takes replica ids from a
 // global counter until the launch's item list is exhausted, so replicas of
 // different orders and weights share one launch.
@@ -36,8 +44,21 @@ namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
 
+// Replica-constant fields the proposal code reads, kept in the warp's slot.
+struct View {
+    const int8_t* W;
+    const uint8_t* mino;
+    const int32_t* res;
+    const uint64_t* mask;      // 2 words per row: nonzero support
+    const uint32_t* dw;        // cached draw words of this iteration
+    uint64_t valid_lo, valid_hi;
+    uint64_t thr_target, thr_dbl, thr_sign, thr_swsign;
+    int n, w, m, sparse, ts, bpc, cc, move_set;
+    uint32_t stream, k0, k1, pad;
+};
+
 struct SlotLayout {
-    uint32_t off_g, off_res, off_mino, off_mask, off_draws, bytes;
+    uint32_t off_g, off_res, off_mino, off_mask, off_draws, off_view, bytes;
     int ld;
 };
 
@@ -50,7 +71,8 @@ __host__ __device__ inline SlotLayout slot_layout(int n, int m) {
     L.off_mino = L.off_res + xw_pad16((uint32_t)n * 4u);
     L.off_mask = L.off_mino + xw_pad16((uint32_t)(n * m));
     L.off_draws = L.off_mask + xw_pad16((uint32_t)n * 16u);
-    L.bytes = L.off_draws + 32u * 16u;
+    L.off_view = L.off_draws + 32u * 16u;
+    L.bytes = L.off_view + xw_pad16((uint32_t)sizeof(View));
     return L;
 }
 
@@ -67,158 +89,244 @@ __device__ __forceinline__ int cyclic_first(uint64_t lo, uint64_t hi, int start)
     return -1;
 }
 
-// Per-lane view of a replica for the scalar proposal code.
-struct View {
+// Draw words outside the cached blocks (rare: attempts past the first,
+// tournaments past 8 samples, candidates past the cached ones).
+__device__ __noinline__ uint32_t slow_word(uint32_t slot, uint64_t it, uint32_t stream, uint32_t k0, uint32_t k1,
+                                           int j) {
+    return pick(draw_block(slot, it, stream, k0, k1), j);
+}
+
+__device__ __forceinline__ uint32_t word(const View* v, uint64_t it, int c, int b, int j) {
+    if (c < v->cc && b < v->bpc) return v->dw[(1 + c * v->bpc + b) * 4 + j];
+    return slow_word(cand_slot(c, b), it, v->stream, v->k0, v->k1, j);
+}
+
+__device__ __forceinline__ uint32_t index(const View* v, uint64_t it, int c, int b, int j, uint32_t count) {
+    return draw_index(word(v, it, c, b, j), count, cand_slot(c, b), it, v->stream, v->k0, v->k1, j);
+}
+
+__device__ __forceinline__ int at(const View* v, int r, int c) { return v->W[c * v->n + r]; }
+
+// The same replica context in registers, for the inlined common path of a
+// proposal: reading it from shared memory would put two dependent loads in
+// front of every draw.
+struct Reg {
     const int8_t* W;
     const uint8_t* mino;
-    const int32_t* res;
-    const uint64_t* mask;      // 2 words per row: nonzero support
-    const uint32_t* dw;        // cached draw words
-    int n, w, m, sparse, ts, bpc, cc;
+    const uint64_t* mask;
+    const uint32_t* cw;        // this candidate's cached draw words
     uint64_t it;
+    uint64_t thr_target, thr_dbl, thr_sign, thr_swsign;
+    int n, w, m, sparse, move_set;
+    bool cached;               // candidate's blocks 0..bpc-1 are in cw
     uint32_t stream, k0, k1;
-    uint64_t valid_lo, valid_hi;
-
-    __device__ __forceinline__ int at(int r, int c) const { return W[c * n + r]; }
 
     __device__ __forceinline__ uint32_t word(int c, int b, int j) const {
-        if (c < cc && b < bpc) return dw[(1 + c * bpc + b) * 4 + j];
-        return pick(draw_block(cand_slot(c, b), it, stream, k0, k1), j);
+        if (cached) return cw[b * 4 + j];
+        return slow_word(cand_slot(c, b), it, stream, k0, k1, j);
     }
-
     __device__ __forceinline__ uint32_t index(int c, int b, int j, uint32_t count) const {
-        uint32_t out;
-        if (lemire_ok(word(c, b, j), count, out)) return out;
-        return lemire_retry(cand_slot(c, b), it, stream, k0, k1, j, count);
+        return draw_index(word(c, b, j), count, cand_slot(c, b), it, stream, k0, k1, j);
     }
+    __device__ __forceinline__ int at(int r, int c) const { return W[c * n + r]; }
 };
 
-struct Move {
-    int kind, r1, r2, c1, c2, p1, p2, v1, v2;
-};
-
-__device__ __forceinline__ uint32_t pack0(const Move& mv) {
-    return 1u | ((uint32_t)mv.kind << 1) | ((uint32_t)mv.r1 << 3) | ((uint32_t)mv.r2 << 10) |
-           ((uint32_t)mv.c1 << 17) | ((uint32_t)mv.c2 << 24);
+// Move descriptor, two words:
+//   d0 = valid | kind<<1 | r1<<3 | r2<<10 | c1<<17 | c2<<24
+//   d1 = (v1+1) | (v2+1)<<2 | p1<<4 | p2<<11
+// kinds: 0 sign flip (r1,c1); 1 support switch with new values v1 at
+// (r1,c2) and v2 at (r2,c1); 2 double flip (r1,c1),(r2,c2); 3 within-row
+// swap: the nonzero at (r1,c1) moves to (r1,c2) with value v1.
+__device__ __forceinline__ uint2 pack(int kind, int r1, int r2, int c1, int c2, int v1, int v2, int p1, int p2) {
+    return make_uint2(1u | ((uint32_t)kind << 1) | ((uint32_t)r1 << 3) | ((uint32_t)r2 << 10) |
+                          ((uint32_t)c1 << 17) | ((uint32_t)c2 << 24),
+                      (uint32_t)(v1 + 1) | ((uint32_t)(v2 + 1) << 2) | ((uint32_t)p1 << 4) | ((uint32_t)p2 << 11));
 }
-__device__ __forceinline__ uint32_t pack1(const Move& mv) {
-    return (uint32_t)(mv.v1 + 1) | ((uint32_t)(mv.v2 + 1) << 2) | ((uint32_t)mv.p1 << 4) |
-           ((uint32_t)mv.p2 << 11);
-}
 
-// propose_sign_flip (xweigh_cuda.cu:302-325): a nonzero of `row`, from the
-// minority list when the row is sparse, else the first nonzero at or after
-// a random column.
-__device__ bool d_flip(const View& v, int c, int b, int j, int row, Move& mv) {
-    int col;
-    if (v.sparse && v.m > 0) {
-        col = v.mino[row * v.m + (int)v.index(c, b, j, (uint32_t)v.m)];
-    } else {
-        const int start = (int)v.index(c, b, j, (uint32_t)v.n);
-        col = cyclic_first(v.mask[2 * row], v.mask[2 * row + 1], start);
-        if (col < 0) return false;
-    }
-    mv.kind = 0; mv.r1 = row; mv.c1 = col; mv.r2 = 0; mv.c2 = 0;
-    mv.p1 = 0; mv.p2 = 0; mv.v1 = 0; mv.v2 = 0;
-    return true;
+// propose_sign_flip (xweigh_cuda.cu:302-325): a nonzero column of `row`,
+// from the minority list when the row is sparse, else the first nonzero at
+// or after a random column; -1 when the row has none.
+__device__ __noinline__ int d_flip_col(const View* v, uint64_t it, int c, int b, int j, int row) {
+    if (v->sparse && v->m > 0) return v->mino[row * v->m + (int)index(v, it, c, b, j, (uint32_t)v->m)];
+    const int start = (int)index(v, it, c, b, j, (uint32_t)v->n);
+    return cyclic_first(v->mask[2 * row], v->mask[2 * row + 1], start);
 }
 
 // hot_row (xweigh_cuda.cu:291-300), serial form
-__device__ int d_hot_row(const View& v, int c) {
-    int best = (int)v.index(c, 4, 0, (uint32_t)v.n);
-    for (int k = 1; k < v.ts; ++k) {
-        const int cand = (int)v.index(c, 4 + k / 4, k % 4, (uint32_t)v.n);
-        if (v.res[cand] > v.res[best]) best = cand;
+__device__ __noinline__ int d_hot_row(const View* v, uint64_t it, int c) {
+    int best = (int)index(v, it, c, 4, 0, (uint32_t)v->n);
+#pragma unroll 1
+    for (int k = 1; k < v->ts; ++k) {
+        const int cand = (int)index(v, it, c, 4 + k / 4, k % 4, (uint32_t)v->n);
+        if (v->res[cand] > v->res[best]) best = cand;
     }
     return best;
 }
 
-// propose_double_sign_flip (xweigh_cuda.cu:389-421)
-__device__ bool d_double(const View& v, int c, int row1, Move& mv) {
-    Move first;
-    if (!d_flip(v, c, 2, 3, row1, first)) return false;
-    for (int a = 0; a < 16; ++a) {
-        const int b = a == 0 ? 3 : 20 + (a - 1);
-        const int row2 = v.word(c, b, 0) < 0x80000000u ? row1 : (int)v.index(c, b, 1, (uint32_t)v.n);
-        Move second;
-        if (!d_flip(v, c, b, 2, row2, second)) continue;
-        if (first.r1 == second.r1 && first.c1 == second.c1) continue;
-        mv.kind = 2; mv.r1 = first.r1; mv.c1 = first.c1; mv.r2 = second.r1; mv.c2 = second.c1;
-        mv.p1 = 0; mv.p2 = 0; mv.v1 = 0; mv.v2 = 0;
-        return true;
+// propose_double_sign_flip (xweigh_cuda.cu:389-421), second-flip attempts
+// 1..15 (attempt 0 is evaluated inline by d_propose)
+__device__ __noinline__ uint2 d_double_rest(const View* v, uint64_t it, int c, int row1, int col1) {
+#pragma unroll 1
+    for (int a = 1; a < 16; ++a) {
+        const int b = 20 + (a - 1);
+        const int row2 = word(v, it, c, b, 0) < 0x80000000u ? row1 : (int)index(v, it, c, b, 1, (uint32_t)v->n);
+        const int col2 = d_flip_col(v, it, c, b, 2, row2);
+        if (col2 < 0 || (row2 == row1 && col2 == col1)) continue;
+        return pack(2, row1, row2, col1, col2, 0, 0, 0, 0);
     }
-    return false;
+    return make_uint2(0u, 0u);
 }
 
-// propose_support_switch (xweigh_cuda.cu:327-387)
-__device__ bool d_switch(const View& v, int c, int row1, uint64_t thr_swsign, Move& mv) {
-    if (v.m == 0 || v.n < 2) return false;
-    for (int a = 0; a < 24; ++a) {
-        int br, jr, bp1, jp1, bp2, jp2, bs1, js1, bs2, js2;
-        if (a == 0) {
-            br = 1; jr = 1; bp1 = 1; jp1 = 2; bp2 = 1; jp2 = 3; bs1 = 2; js1 = 0; bs2 = 2; js2 = 1;
-        } else {
-            const int B = 36 + 2 * (a - 1);
-            br = B; jr = 0; bp1 = B; jp1 = 1; bp2 = B; jp2 = 2; bs1 = B; js1 = 3; bs2 = B + 1; js2 = 0;
-        }
-        int row2 = (int)v.index(c, br, jr, (uint32_t)(v.n - 1));
+// propose_support_switch (xweigh_cuda.cu:327-387), new signs per
+// switch_sign_fraction (xweigh_cuda.cu:378-383); attempts a0..23
+__device__ __noinline__ uint2 d_switch(const View* v, uint64_t it, int c, int row1, int a0) {
+    if (v->m == 0 || v->n < 2) return make_uint2(0u, 0u);
+#pragma unroll 1
+    for (int a = a0; a < 24; ++a) {
+        // attempt 0 in cached blocks 1-2, attempt a>0 in blocks 36+2(a-1), +1
+        const int B = a == 0 ? 1 : 36 + 2 * (a - 1);
+        const int o = a == 0 ? 1 : 0;
+        int row2 = (int)index(v, it, c, B, o, (uint32_t)(v->n - 1));
         if (row2 >= row1) ++row2;
-        const int p1 = (int)v.index(c, bp1, jp1, (uint32_t)v.m);
-        const int p2 = (int)v.index(c, bp2, jp2, (uint32_t)v.m);
-        int c1, c2;
-        if (v.sparse) { c1 = v.mino[row1 * v.m + p1]; c2 = v.mino[row2 * v.m + p2]; }
-        else { c2 = v.mino[row1 * v.m + p1]; c1 = v.mino[row2 * v.m + p2]; }
-        if (c1 == c2 || v.at(row1, c2) != 0 || v.at(row2, c1) != 0) continue;
-        const int v1 = v.at(row1, c1), v2 = v.at(row2, c2);
+        const int p1 = (int)index(v, it, c, B, o + 1, (uint32_t)v->m);
+        const int p2 = (int)index(v, it, c, B, o + 2, (uint32_t)v->m);
+        const int q1 = v->mino[row1 * v->m + p1], q2 = v->mino[row2 * v->m + p2];
+        const int c1 = v->sparse ? q1 : q2, c2 = v->sparse ? q2 : q1;
+        if (c1 == c2 || at(v, row1, c2) != 0 || at(v, row2, c1) != 0) continue;
+        const int v1 = at(v, row1, c1), v2 = at(v, row2, c2);
         if (v1 == 0 || v2 == 0) continue;
-        mv.kind = 1; mv.r1 = row1; mv.r2 = row2; mv.c1 = c1; mv.c2 = c2; mv.p1 = p1; mv.p2 = p2;
-        mv.v1 = (uint64_t)v.word(c, bs1, js1) < thr_swsign ? -v1 : v1;
-        mv.v2 = (uint64_t)v.word(c, bs2, js2) < thr_swsign ? -v2 : v2;
-        return true;
+        const uint32_t s1 = a == 0 ? word(v, it, c, 2, 0) : word(v, it, c, B, 3);
+        const uint32_t s2 = a == 0 ? word(v, it, c, 2, 1) : word(v, it, c, B + 1, 0);
+        return pack(1, row1, row2, c1, c2, (uint64_t)s1 < v->thr_swsign ? -v1 : v1,
+                    (uint64_t)s2 < v->thr_swsign ? -v2 : v2, p1, p2);
     }
-    return false;
+    return make_uint2(0u, 0u);
 }
 
 // within-row swap: a nonzero of the row moves to one of its zeros
-__device__ bool d_row_swap(const View& v, int c, int row, Move& mv) {
-    if (v.m == 0) return false;
-    const uint64_t nz_lo = v.mask[2 * row], nz_hi = v.mask[2 * row + 1];
+__device__ __noinline__ uint2 d_row_swap(const View* v, uint64_t it, int c, int row) {
+    if (v->m == 0) return make_uint2(0u, 0u);
+    const uint64_t nz_lo = v->mask[2 * row], nz_hi = v->mask[2 * row + 1];
     int c1, c2, pos;
-    if (v.sparse) {
-        pos = (int)v.index(c, 1, 1, (uint32_t)v.m);
-        c1 = v.mino[row * v.m + pos];
-        c2 = cyclic_first(~nz_lo & v.valid_lo, ~nz_hi & v.valid_hi, (int)v.index(c, 1, 2, (uint32_t)v.n));
-        if (c2 < 0) return false;
+    if (v->sparse) {
+        pos = (int)index(v, it, c, 1, 1, (uint32_t)v->m);
+        c1 = v->mino[row * v->m + pos];
+        c2 = cyclic_first(~nz_lo & v->valid_lo, ~nz_hi & v->valid_hi, (int)index(v, it, c, 1, 2, (uint32_t)v->n));
     } else {
-        pos = (int)v.index(c, 1, 2, (uint32_t)v.m);
-        c2 = v.mino[row * v.m + pos];
-        c1 = cyclic_first(nz_lo, nz_hi, (int)v.index(c, 1, 1, (uint32_t)v.n));
-        if (c1 < 0) return false;
+        pos = (int)index(v, it, c, 1, 2, (uint32_t)v->m);
+        c2 = v->mino[row * v->m + pos];
+        c1 = cyclic_first(nz_lo, nz_hi, (int)index(v, it, c, 1, 1, (uint32_t)v->n));
     }
-    mv.kind = 3; mv.r1 = row; mv.r2 = 0; mv.c1 = c1; mv.c2 = c2; mv.p1 = pos; mv.p2 = 0;
-    mv.v1 = v.word(c, 1, 3) < 0x80000000u ? 1 : -1;
-    mv.v2 = 0;
-    return true;
+    if (c1 < 0 || c2 < 0) return make_uint2(0u, 0u);
+    return pack(3, row, 0, c1, c2, word(v, it, c, 1, 3) < 0x80000000u ? 1 : -1, 0, pos, 0);
 }
 
-struct Thresholds {
-    uint64_t target, dbl, sign, swsign;
+__device__ __forceinline__ uint2 flip_move(const View* v, uint64_t it, int c, int b, int j, int row) {
+    const int col = d_flip_col(v, it, c, b, j, row);
+    return col < 0 ? make_uint2(0u, 0u) : pack(0, row, 0, col, 0, 0, 0, 0, 0);
+}
+
+// flip column from a draw word without the out-of-line call: minority pick
+// for a sparse row, else the cyclic first nonzero from a random column
+__device__ __forceinline__ int flip_col_w(const Reg& r, int c, int b, int j, int row) {
+    if (r.sparse && r.m > 0) return r.mino[row * r.m + (int)r.index(c, b, j, (uint32_t)r.m)];
+    const int start = (int)r.index(c, b, j, (uint32_t)r.n);
+    return cyclic_first(r.mask[2 * row], r.mask[2 * row + 1], start);
+}
+
+// propose_move (xweigh_cuda.cu:423-447).  The first attempt of every move
+// kind is computed unconditionally from the cached draw words and the
+// choice is made afterwards, so the candidate lanes of a warp run one
+// instruction stream whatever kinds they pick; only the rare further
+// attempts (a second flip that repeats the first, a switch whose 2x2 is not
+// legal) branch into out-of-line code.  Move set 1 replaces the switch by
+// the within-row swap and has no double flips.  The result equals the
+// sequential reference order of draws and tests.
+__device__ __forceinline__ uint2 d_propose(const Reg& r, const View* v, int c, bool coop_ok, int coop_row) {
+    const int n = r.n, m = r.m;
+    const uint64_t it = r.it;
+    const bool targeted = (uint64_t)r.word(c, 0, 0) < r.thr_target;
+    const int row = targeted ? (coop_ok ? coop_row : d_hot_row(v, it, c)) : (int)r.index(c, 0, 1, (uint32_t)n);
+    const bool want_dbl = r.move_set == 0 && (uint64_t)r.word(c, 0, 2) < r.thr_dbl;
+    const bool want_flip = r.w == n || (uint64_t)r.word(c, 0, 3) < r.thr_sign;
+
+    // double flip, attempt 0: first flip (2,3), second row/flip from block 3
+    const int dcol1 = flip_col_w(r, c, 2, 3, row);
+    const int drow2 = r.word(c, 3, 0) < 0x80000000u ? row : (int)r.index(c, 3, 1, (uint32_t)n);
+    const int dcol2 = flip_col_w(r, c, 3, 2, drow2);
+    const bool dbl_ok = dcol1 >= 0 && dcol2 >= 0 && !(drow2 == row && dcol2 == dcol1);
+    // plain flip
+    const int fcol = flip_col_w(r, c, 1, 0, row);
+
+    uint2 mv = make_uint2(0u, 0u);
+    if (want_dbl && dcol1 >= 0) {
+        if (dbl_ok) return pack(2, row, drow2, dcol1, dcol2, 0, 0, 0, 0);
+        mv = d_double_rest(v, it, c, row, dcol1);
+        if (mv.x) return mv;
+    }
+    if (want_flip) return fcol < 0 ? make_uint2(0u, 0u) : pack(0, row, 0, fcol, 0, 0, 0, 0, 0);
+    if (r.move_set == 1) {
+        mv = d_row_swap(v, it, c, row);
+    } else {
+        // support switch, attempt 0 (blocks 1 and 2)
+        const int mm = m > 0 ? m : 1;
+        int row2 = (int)r.index(c, 1, 1, (uint32_t)(n > 1 ? n - 1 : 1));
+        if (row2 >= row) ++row2;
+        if (row2 >= n) row2 = 0;
+        const int p1 = (int)r.index(c, 1, 2, (uint32_t)mm);
+        const int p2 = (int)r.index(c, 1, 3, (uint32_t)mm);
+        const int q1 = m > 0 ? r.mino[row * m + p1] : 0, q2 = m > 0 ? r.mino[row2 * m + p2] : 0;
+        const int c1 = r.sparse ? q1 : q2, c2 = r.sparse ? q2 : q1;
+        const int v1 = r.at(row, c1), v2 = r.at(row2, c2);
+        const bool ok = m > 0 && n > 1 && c1 != c2 && r.at(row, c2) == 0 && r.at(row2, c1) == 0 && v1 != 0 &&
+                        v2 != 0;
+        if (ok) {
+            const int nv1 = (uint64_t)r.word(c, 2, 0) < r.thr_swsign ? -v1 : v1;
+            const int nv2 = (uint64_t)r.word(c, 2, 1) < r.thr_swsign ? -v2 : v2;
+            return pack(1, row, row2, c1, c2, nv1, nv2, p1, p2);
+        }
+        mv = d_switch(v, it, c, row, 1);
+    }
+    if (mv.x) return mv;
+    return flip_move(v, it, c, 2, 2, row);
+}
+
+// A decoded move as at most two row updates: row R1 gets
+// A1*W[:,X1] + B1*W[:,Y1], row R2 (when >= 0) gets A2*W[:,X2] + B2*W[:,Y2];
+// `pair` marks the double flip over two rows whose G[r1][r2] also changes.
+struct Update {
+    int R1, X1, Y1, A1, B1;
+    int R2, X2, Y2, A2, B2;
+    int pair;
 };
 
-__device__ bool d_propose(const View& v, int c, int move_set, const Thresholds& th,
-                          bool coop_ok, int coop_row, Move& mv) {
-    const bool targeted = (uint64_t)v.word(c, 0, 0) < th.target;
-    const int row = targeted ? (coop_ok ? coop_row : d_hot_row(v, c))
-                             : (int)v.index(c, 0, 1, (uint32_t)v.n);
-    if (move_set == 1) {
-        if (v.w == v.n || (uint64_t)v.word(c, 0, 3) < th.sign) return d_flip(v, c, 1, 0, row, mv);
-        if (d_row_swap(v, c, row, mv)) return true;
-        return d_flip(v, c, 2, 2, row, mv);
+__device__ __forceinline__ Update decode(uint32_t d0, uint32_t d1, const int8_t* W, int n) {
+    const int kind = (d0 >> 1) & 3, r1 = (d0 >> 3) & 127, r2 = (d0 >> 10) & 127;
+    const int c1 = (d0 >> 17) & 127, c2 = (d0 >> 24) & 127;
+    const int nv1 = (int)(d1 & 3) - 1, nv2 = (int)((d1 >> 2) & 3) - 1;
+    const int w11 = W[c1 * n + r1], w22 = W[c2 * n + r2];
+    Update u;
+    u.R1 = r1;
+    u.R2 = -1;
+    u.X2 = 0; u.Y2 = 0; u.A2 = 0; u.B2 = 0;
+    u.pair = 0;
+    if (kind == 0) {
+        u.X1 = c1; u.Y1 = c1; u.A1 = -2 * w11; u.B1 = 0;
+    } else if (kind == 1) {
+        u.X1 = c2; u.Y1 = c1; u.A1 = nv1; u.B1 = -w11;
+        u.R2 = r2; u.X2 = c1; u.Y2 = c2; u.A2 = nv2; u.B2 = -w22;
+    } else if (kind == 2) {
+        if (r1 == r2) {
+            u.X1 = c1; u.Y1 = c2; u.A1 = -2 * w11; u.B1 = -2 * w22;
+        } else {
+            u.X1 = c1; u.Y1 = c1; u.A1 = -2 * w11; u.B1 = 0;
+            u.R2 = r2; u.X2 = c2; u.Y2 = c2; u.A2 = -2 * w22; u.B2 = 0;
+            u.pair = 1;
+        }
+    } else {
+        u.X1 = c2; u.Y1 = c1; u.A1 = nv1; u.B1 = -w11;
     }
-    if ((uint64_t)v.word(c, 0, 2) < th.dbl && d_double(v, c, row, mv)) return true;
-    if (v.w == v.n || (uint64_t)v.word(c, 0, 3) < th.sign) return d_flip(v, c, 1, 0, row, mv);
-    if (d_switch(v, c, row, th.swsign, mv)) return true;
-    return d_flip(v, c, 2, 2, row, mv);
+    return u;
 }
 
 struct Deltas {
@@ -233,198 +341,107 @@ __device__ __forceinline__ void acc(Deltas& d, int old, int nw) {
     d.dpar += (an & 1) - (ao & 1);
 }
 
+// the pair entry G[r1][r2] after a double flip over rows r1 != r2
+// (xweigh_cuda.cu:564-583)
+__device__ __forceinline__ int pair_new(const Update& u, int op, const int8_t* W, int n, int c1, int c2) {
+    return op + u.A1 * W[c1 * n + u.R2] + u.A2 * W[c2 * n + u.R1] + (c1 == c2 ? u.A1 * u.A2 : 0);
+}
+
 // evaluate_move_warp (xweigh_cuda.cu:449-599): lane-partial deltas over the
 // lane's own rows; the caller reduces them across the warp.
 template <int OPL>
-__device__ __forceinline__ Deltas eval_lane(int kind, int r1, int r2, int c1, int c2, int nv1, int nv2,
-                                            const int8_t* W, const int32_t* G, int n, int ld, int lane) {
+__device__ __forceinline__ Deltas eval_lane(const Update& u, const int8_t* W, const int32_t* G, int n, int ld,
+                                            int lane) {
     Deltas d = {0, 0, 0, 0};
-    if (kind == 0) {
-        const int ch = -2 * W[c1 * n + r1];
 #pragma unroll
-        for (int k = 0; k < OPL; ++k) {
-            const int o = lane + 32 * k;
-            if (o < n && o != r1) {
-                const int old = G[r1 * ld + o];
-                acc(d, old, old + ch * W[c1 * n + o]);
+    for (int k = 0; k < OPL; ++k) {
+        const int o = lane + 32 * k;
+        if (o < n && o != u.R1 && o != u.R2) {
+            const int o1 = G[u.R1 * ld + o];
+            acc(d, o1, o1 + u.A1 * W[u.X1 * n + o] + u.B1 * W[u.Y1 * n + o]);
+            if (u.R2 >= 0) {
+                const int o2 = G[u.R2 * ld + o];
+                acc(d, o2, o2 + u.A2 * W[u.X2 * n + o] + u.B2 * W[u.Y2 * n + o]);
             }
         }
-    } else if (kind == 1) {
-        const int v1 = W[c1 * n + r1], v2 = W[c2 * n + r2];
-#pragma unroll
-        for (int k = 0; k < OPL; ++k) {
-            const int o = lane + 32 * k;
-            if (o < n && o != r1 && o != r2) {
-                const int o1 = G[r1 * ld + o], o2 = G[r2 * ld + o];
-                const int w1 = W[c1 * n + o], w2 = W[c2 * n + o];
-                acc(d, o1, o1 + nv1 * w2 - v1 * w1);
-                acc(d, o2, o2 + nv2 * w1 - v2 * w2);
-            }
-        }
-    } else if (kind == 2) {
-        const int ch1 = -2 * W[c1 * n + r1], ch2 = -2 * W[c2 * n + r2];
-        if (r1 == r2) {
-#pragma unroll
-            for (int k = 0; k < OPL; ++k) {
-                const int o = lane + 32 * k;
-                if (o < n && o != r1) {
-                    const int old = G[r1 * ld + o];
-                    acc(d, old, old + ch1 * W[c1 * n + o] + ch2 * W[c2 * n + o]);
-                }
-            }
-        } else {
-#pragma unroll
-            for (int k = 0; k < OPL; ++k) {
-                const int o = lane + 32 * k;
-                if (o < n && o != r1 && o != r2) {
-                    const int o1 = G[r1 * ld + o], o2 = G[r2 * ld + o];
-                    acc(d, o1, o1 + ch1 * W[c1 * n + o]);
-                    acc(d, o2, o2 + ch2 * W[c2 * n + o]);
-                }
-            }
-            if (lane == 0) {
-                const int op = G[r1 * ld + r2];
-                acc(d, op, op + ch1 * W[c1 * n + r2] + ch2 * W[c2 * n + r1] + (c1 == c2 ? ch1 * ch2 : 0));
-            }
-        }
-    } else {
-        const int v = W[c1 * n + r1];
-#pragma unroll
-        for (int k = 0; k < OPL; ++k) {
-            const int o = lane + 32 * k;
-            if (o < n && o != r1) {
-                const int old = G[r1 * ld + o];
-                acc(d, old, old + nv1 * W[c2 * n + o] - v * W[c1 * n + o]);
-            }
-        }
+    }
+    if (u.pair && lane == 0) {
+        const int op = G[u.R1 * ld + u.R2];
+        acc(d, op, pair_new(u, op, W, n, u.X1, u.X2));
     }
     return d;
 }
 
-__device__ __forceinline__ void set_pair(int32_t* G, int32_t* res, int ld, int a, int o, int old, int nw, int& d) {
-    d = iabs(nw) - iabs(old);
-    G[a * ld + o] = nw;
-    G[o * ld + a] = nw;
-    res[o] += d;
-}
-
-__device__ __forceinline__ void mask_move(uint64_t* mask, int row, int from, int to) {
-    mask[2 * row + (from >> 6)] &= ~(1ull << (from & 63));
-    mask[2 * row + (to >> 6)] |= 1ull << (to & 63);
-}
-
 // commit_sign_flip / commit_support_switch / commit_double_sign_flip
-// (xweigh_cuda.cu:607-877) and the within-row swap.
+// (xweigh_cuda.cu:607-877) and the within-row swap, in the two-row form.
 template <int OPL>
-__device__ void commit(int kind, int r1, int r2, int c1, int c2, int nv1, int nv2, int p1, int p2,
-                       int ds, int8_t* W, int32_t* G, int32_t* res, uint8_t* mino, uint64_t* mask,
-                       int n, int ld, int m, int sparse, int lane) {
-    if (kind == 0) {
-        const int ch = -2 * W[c1 * n + r1];
+__device__ void commit(uint32_t d0, uint32_t d1, const Update& u, int ds, int8_t* W, int32_t* G, int32_t* res,
+                       uint8_t* mino, uint64_t* mask, int n, int ld, int m, int sparse, int lane) {
+    int s1 = 0;
 #pragma unroll
-        for (int k = 0; k < OPL; ++k) {
-            const int o = lane + 32 * k;
-            if (o < n && o != r1) {
-                const int old = G[r1 * ld + o];
-                int d;
-                set_pair(G, res, ld, r1, o, old, old + ch * W[c1 * n + o], d);
+    for (int k = 0; k < OPL; ++k) {
+        const int o = lane + 32 * k;
+        if (o < n && o != u.R1 && o != u.R2) {
+            const int o1 = G[u.R1 * ld + o];
+            const int n1 = o1 + u.A1 * W[u.X1 * n + o] + u.B1 * W[u.Y1 * n + o];
+            const int e1 = iabs(n1) - iabs(o1);
+            G[u.R1 * ld + o] = n1;
+            G[o * ld + u.R1] = n1;
+            int e = e1;
+            if (u.R2 >= 0) {
+                const int o2 = G[u.R2 * ld + o];
+                const int n2 = o2 + u.A2 * W[u.X2 * n + o] + u.B2 * W[u.Y2 * n + o];
+                G[u.R2 * ld + o] = n2;
+                G[o * ld + u.R2] = n2;
+                e += iabs(n2) - iabs(o2);
             }
+            res[o] += e;
+            s1 += e1;
         }
-        __syncwarp();
-        if (lane == 0) {
-            res[r1] += ds;
-            W[c1 * n + r1] = (int8_t)-W[c1 * n + r1];
-        }
-    } else if (kind == 1) {
-        const int v1 = W[c1 * n + r1], v2 = W[c2 * n + r2];
-        int s1 = 0;
-#pragma unroll
-        for (int k = 0; k < OPL; ++k) {
-            const int o = lane + 32 * k;
-            if (o < n && o != r1 && o != r2) {
-                const int o1 = G[r1 * ld + o], o2 = G[r2 * ld + o];
-                const int w1 = W[c1 * n + o], w2 = W[c2 * n + o];
-                int d1, d2;
-                set_pair(G, res, ld, r1, o, o1, o1 + nv1 * w2 - v1 * w1, d1);
-                set_pair(G, res, ld, r2, o, o2, o2 + nv2 * w1 - v2 * w2, d2);
-                s1 += d1;
-            }
-        }
-        const int S1 = __reduce_add_sync(FULL, s1);
-        __syncwarp();
-        if (lane == 0) {
+    }
+    const int S1 = __reduce_add_sync(FULL, s1);
+    __syncwarp();
+    if (lane == 0) {
+        const int kind = (d0 >> 1) & 3, r1 = (d0 >> 3) & 127, r2 = (d0 >> 10) & 127;
+        const int c1 = (d0 >> 17) & 127, c2 = (d0 >> 24) & 127;
+        const int nv1 = (int)(d1 & 3) - 1, nv2 = (int)((d1 >> 2) & 3) - 1;
+        const int p1 = (d1 >> 4) & 127, p2 = (d1 >> 11) & 127;
+        if (u.pair) {
+            const int op = G[r1 * ld + r2];
+            const int np = pair_new(u, op, W, n, c1, c2);
+            const int pd = iabs(np) - iabs(op);
+            G[r1 * ld + r2] = np;
+            G[r2 * ld + r1] = np;
+            res[r1] += S1 + pd;
+            res[r2] += ds - S1;
+        } else if (u.R2 >= 0) {
             res[r1] += S1;
             res[r2] += ds - S1;
+        } else {
+            res[r1] += ds;
+        }
+        if (kind == 0) {
+            W[c1 * n + r1] = (int8_t)-W[c1 * n + r1];
+        } else if (kind == 2) {
+            W[c1 * n + r1] = (int8_t)-W[c1 * n + r1];
+            W[c2 * n + r2] = (int8_t)-W[c2 * n + r2];
+        } else if (kind == 1) {
             W[c1 * n + r1] = 0;
             W[c2 * n + r2] = 0;
             W[c2 * n + r1] = (int8_t)nv1;
             W[c1 * n + r2] = (int8_t)nv2;
-            if (sparse) { mino[r1 * m + p1] = (uint8_t)c2; mino[r2 * m + p2] = (uint8_t)c1; }
-            else { mino[r1 * m + p1] = (uint8_t)c1; mino[r2 * m + p2] = (uint8_t)c2; }
-            mask_move(mask, r1, c1, c2);
-            mask_move(mask, r2, c2, c1);
-        }
-    } else if (kind == 2) {
-        const int ch1 = -2 * W[c1 * n + r1], ch2 = -2 * W[c2 * n + r2];
-        if (r1 == r2) {
-#pragma unroll
-            for (int k = 0; k < OPL; ++k) {
-                const int o = lane + 32 * k;
-                if (o < n && o != r1) {
-                    const int old = G[r1 * ld + o];
-                    int d;
-                    set_pair(G, res, ld, r1, o, old, old + ch1 * W[c1 * n + o] + ch2 * W[c2 * n + o], d);
-                }
-            }
-            __syncwarp();
-            if (lane == 0) res[r1] += ds;
+            mino[r1 * m + p1] = (uint8_t)(sparse ? c2 : c1);
+            mino[r2 * m + p2] = (uint8_t)(sparse ? c1 : c2);
+            mask[2 * r1 + (c1 >> 6)] &= ~(1ull << (c1 & 63));
+            mask[2 * r1 + (c2 >> 6)] |= 1ull << (c2 & 63);
+            mask[2 * r2 + (c2 >> 6)] &= ~(1ull << (c2 & 63));
+            mask[2 * r2 + (c1 >> 6)] |= 1ull << (c1 & 63);
         } else {
-            int s1 = 0;
-#pragma unroll
-            for (int k = 0; k < OPL; ++k) {
-                const int o = lane + 32 * k;
-                if (o < n && o != r1 && o != r2) {
-                    const int o1 = G[r1 * ld + o], o2 = G[r2 * ld + o];
-                    int d1, d2;
-                    set_pair(G, res, ld, r1, o, o1, o1 + ch1 * W[c1 * n + o], d1);
-                    set_pair(G, res, ld, r2, o, o2, o2 + ch2 * W[c2 * n + o], d2);
-                    s1 += d1;
-                }
-            }
-            const int S1 = __reduce_add_sync(FULL, s1);
-            __syncwarp();
-            if (lane == 0) {
-                const int op = G[r1 * ld + r2];
-                const int np = op + ch1 * W[c1 * n + r2] + ch2 * W[c2 * n + r1] + (c1 == c2 ? ch1 * ch2 : 0);
-                const int pd = iabs(np) - iabs(op);
-                G[r1 * ld + r2] = np;
-                G[r2 * ld + r1] = np;
-                res[r1] += S1 + pd;
-                res[r2] += ds - S1;
-            }
-        }
-        if (lane == 0) {
-            W[c1 * n + r1] = (int8_t)-W[c1 * n + r1];
-            W[c2 * n + r2] = (int8_t)-W[c2 * n + r2];
-        }
-    } else {
-        const int v = W[c1 * n + r1];
-#pragma unroll
-        for (int k = 0; k < OPL; ++k) {
-            const int o = lane + 32 * k;
-            if (o < n && o != r1) {
-                const int old = G[r1 * ld + o];
-                int d;
-                set_pair(G, res, ld, r1, o, old, old + nv1 * W[c2 * n + o] - v * W[c1 * n + o], d);
-            }
-        }
-        __syncwarp();
-        if (lane == 0) {
-            res[r1] += ds;
             W[c1 * n + r1] = 0;
             W[c2 * n + r1] = (int8_t)nv1;
             mino[r1 * m + p1] = (uint8_t)(sparse ? c2 : c1);
-            mask_move(mask, r1, c1, c2);
+            mask[2 * r1 + (c1 >> 6)] &= ~(1ull << (c1 & 63));
+            mask[2 * r1 + (c2 >> 6)] |= 1ull << (c2 & 63);
         }
     }
     __syncwarp();
@@ -462,6 +479,7 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
     uint64_t* sMask = reinterpret_cast<uint64_t*>(slot + L.off_mask);
     uint4* sDraw = reinterpret_cast<uint4*>(slot + L.off_draws);
     const uint32_t* sDw = reinterpret_cast<const uint32_t*>(sDraw);
+    View* sView = reinterpret_cast<View*>(slot + L.off_view);
 
     uint64_t it = H->it;
     uint64_t iters = a.iters;
@@ -483,6 +501,7 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
         if (o < n) {
             uint64_t lo = 0, hi = 0;
             int pos = 0;
+#pragma unroll 1
             for (int c = 0; c < n; ++c) {
                 const bool nz = sW[c * n + o] != 0;
                 if (nz) { if (c < 64) lo |= 1ull << c; else hi |= 1ull << (c - 64); }
@@ -508,8 +527,10 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
         const int o = lane + 32 * k;
         if (o < n) {
             int r_sum = 0;
+#pragma unroll 1
             for (int r = 0; r < n; ++r) {
                 int dot = 0;
+#pragma unroll 1
                 for (int c = 0; c < n; ++c) dot += sW[c * n + r] * sW[c * n + o];
                 sG[r * ld + o] = dot;
                 if (r != o) {
@@ -562,24 +583,27 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
     obj_total = obj0;
 
     // ---- job constants ----
-    const int tempering = J->tempering, move_set = J->move_set;
+    const int tempering = J->tempering;
     const int cs = J->candidate_samples, ts = J->target_samples;
     const int mpc = J->moves_per_cool, stuck = J->stuck_threshold;
     const uint32_t k0 = J->key0, k1 = J->key1, stream = H->stream;
     const uint64_t thr_greedy = J->thr_greedy;
-    Thresholds th;
-    th.target = J->thr_target; th.dbl = J->thr_double; th.sign = J->thr_sign; th.swsign = J->thr_swsign;
     const double t_min = J->t_min, cooling = J->cooling, reheat = J->reheat;
     const int bpc = 4 + (ts <= 4 ? 1 : 2);          // cached blocks per candidate
-    const int cc = 31 / bpc;                        // cached candidates
     const bool coop = ts <= 8;                      // cooperative hot-row tournament
-
-    View v;
-    v.W = sW; v.mino = sMino; v.res = sRes; v.mask = sMask; v.dw = sDw;
-    v.n = n; v.w = w; v.m = m; v.sparse = sparse; v.ts = ts; v.bpc = bpc; v.cc = cc;
-    v.stream = stream; v.k0 = k0; v.k1 = k1;
-    v.valid_lo = n >= 64 ? ~0ull : ((1ull << n) - 1ull);
-    v.valid_hi = n <= 64 ? 0ull : (n == 128 ? ~0ull : ((1ull << (n - 64)) - 1ull));
+    if (lane == 0) {
+        View v;
+        v.W = sW; v.mino = sMino; v.res = sRes; v.mask = sMask; v.dw = sDw;
+        v.valid_lo = n >= 64 ? ~0ull : ((1ull << n) - 1ull);
+        v.valid_hi = n <= 64 ? 0ull : (n == 128 ? ~0ull : ((1ull << (n - 64)) - 1ull));
+        v.thr_target = J->thr_target; v.thr_dbl = J->thr_double; v.thr_sign = J->thr_sign;
+        v.thr_swsign = J->thr_swsign;
+        v.n = n; v.w = w; v.m = m; v.sparse = sparse; v.ts = ts; v.bpc = bpc; v.cc = 31 / bpc;
+        v.move_set = J->move_set;
+        v.stream = stream; v.k0 = k0; v.k1 = k1; v.pad = 0;
+        *sView = v;
+    }
+    __syncwarp();
 
     // lane -> cached Philox block of this iteration
     uint32_t my_slot = 0;
@@ -587,14 +611,23 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
         const int q = lane - 1, c = q / bpc, b = q - c * bpc;
         my_slot = cand_slot(c, b);
     }
+    // register context of candidate `lane` for the inlined proposal path
+    Reg rg;
+    rg.W = sW; rg.mino = sMino; rg.mask = sMask;
+    rg.cw = sDw + (1 + lane * bpc) * 4;
+    rg.cached = lane < 31 / bpc;
+    rg.thr_target = J->thr_target; rg.thr_dbl = J->thr_double; rg.thr_sign = J->thr_sign;
+    rg.thr_swsign = J->thr_swsign;
+    rg.n = n; rg.w = w; rg.m = m; rg.sparse = sparse; rg.move_set = J->move_set;
+    rg.stream = stream; rg.k0 = k0; rg.k1 = k1;
 
     uint64_t done = 0;
+#pragma unroll 1
     for (; done < iters; ++done) {
         if (a.stop_on_solve) {
             if (best_s == 0) break;
             if ((done & 63) == 63 && *(volatile int32_t*)&J->solved) break;
         }
-        v.it = it;
         // A: draws
         sDraw[lane] = draw_block(my_slot, it, stream, k0, k1);
         __syncwarp();
@@ -606,10 +639,8 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
         if (coop) {
             const int c = lane >> 3, s = lane & 7;
             if (c < count && s < ts) {
-                const uint32_t word = sDw[(1 + c * bpc + 4 + (s >> 2)) * 4 + (s & 3)];
-                uint32_t row;
-                if (!lemire_ok(word, (uint32_t)n, row))
-                    row = lemire_retry(cand_slot(c, 4 + (s >> 2)), it, stream, k0, k1, s & 3, (uint32_t)n);
+                const uint32_t wd = sDw[(1 + c * bpc + 4 + (s >> 2)) * 4 + (s & 3)];
+                const uint32_t row = draw_index(wd, (uint32_t)n, cand_slot(c, 4 + (s >> 2)), it, stream, k0, k1, s & 3);
                 hot_key = (sRes[row] << 13) | ((31 - s) << 8) | (int)row;
             }
             hot_key = max(hot_key, __shfl_xor_sync(FULL, hot_key, 1));
@@ -619,28 +650,22 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
         const int coop_row = __shfl_sync(FULL, hot_key, (lane & 3) << 3) & 0xff;
 
         // D: proposals, lane c proposes candidate c
-        uint32_t d0 = 0, d1 = 0;
-        if (lane < count) {
-            Move mv;
-            if (d_propose(v, lane, move_set, th, coop && lane < 4, coop_row, mv)) {
-                d0 = pack0(mv);
-                d1 = pack1(mv);
-            }
-        }
+        uint2 desc = make_uint2(0u, 0u);
+        rg.it = it;
+        if (lane < count) desc = d_propose(rg, sView, lane, coop && lane < 4, coop_row);
         __syncwarp();
 
         // E: evaluate in candidate order, keep the first best
         bool have = false;
         uint32_t b0 = 0, b1 = 0;
         int bds = 0, bdc = 0, bprim = 0;
+#pragma unroll 1
         for (int c = 0; c < count; ++c) {
-            const uint32_t e0 = __shfl_sync(FULL, d0, c);
-            const uint32_t e1 = __shfl_sync(FULL, d1, c);
+            const uint32_t e0 = __shfl_sync(FULL, desc.x, c);
+            const uint32_t e1 = __shfl_sync(FULL, desc.y, c);
             if (!(e0 & 1u)) continue;
-            const int kind = (e0 >> 1) & 3, r1 = (e0 >> 3) & 127, r2 = (e0 >> 10) & 127;
-            const int c1 = (e0 >> 17) & 127, c2 = (e0 >> 24) & 127;
-            const int nv1 = (int)(e1 & 3) - 1, nv2 = (int)((e1 >> 2) & 3) - 1;
-            const Deltas d = eval_lane<OPL>(kind, r1, r2, c1, c2, nv1, nv2, sW, sG, n, ld, lane);
+            const Update u = decode(e0, e1, sW, n);
+            const Deltas d = eval_lane<OPL>(u, sW, sG, n, ld, lane);
             const int packed = __reduce_add_sync(FULL, d.ds * 4096 + d.dc);
             const int dc = ((packed + 2048) & 4095) - 2048;
             const int ds = (packed - dc) >> 12;
@@ -669,12 +694,8 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
 
         // G: commit
         if (accept) {
-            const int kind = (b0 >> 1) & 3, r1 = (b0 >> 3) & 127, r2 = (b0 >> 10) & 127;
-            const int c1 = (b0 >> 17) & 127, c2 = (b0 >> 24) & 127;
-            const int nv1 = (int)(b1 & 3) - 1, nv2 = (int)((b1 >> 2) & 3) - 1;
-            const int p1 = (b1 >> 4) & 127, p2 = (b1 >> 11) & 127;
-            commit<OPL>(kind, r1, r2, c1, c2, nv1, nv2, p1, p2, bds, sW, sG, sRes, sMino, sMask,
-                        n, ld, m, sparse, lane);
+            const Update u = decode(b0, b1, sW, n);
+            commit<OPL>(b0, b1, u, bds, sW, sG, sRes, sMino, sMask, n, ld, m, sparse, lane);
             score += bds;
             conflicts += bdc;
             obj_total += bprim;
@@ -735,7 +756,11 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
 }
 
 template <int OPL>
-__global__ void __launch_bounds__(128, 6) anneal_kernel(AnnealArgs a) {
+// Register budget: 256 threads x XW_ANNEAL_MIN_BLOCKS blocks per SM.
+#ifndef XW_ANNEAL_MIN_BLOCKS
+#define XW_ANNEAL_MIN_BLOCKS 2
+#endif
+__global__ void __launch_bounds__(256, XW_ANNEAL_MIN_BLOCKS) anneal_kernel(AnnealArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -752,11 +777,11 @@ __global__ void __launch_bounds__(128, 6) anneal_kernel(AnnealArgs a) {
 // One thread per tempering job: adjacent-rung sweep of
 // xweigh_anneal.hpp:1187-1221 on the device draw stream.
 __global__ void exchange_kernel(XwJob* jobs, int njobs, uint8_t* arena, const uint64_t* rec_off,
-                                const double* ladder) {
+                                const double* ladder, int stop_on_solve) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= njobs) return;
     XwJob& J = jobs[j];
-    if (!J.tempering || J.done || J.solved || J.replicas < 2 || J.replicas > XW_MAX_RUNGS) return;
+    if (!J.tempering || J.done || (stop_on_solve && J.solved) || J.replicas < 2 || J.replicas > XW_MAX_RUNGS) return;
     const int R = J.replicas;
     int owner[XW_MAX_RUNGS];
     int64_t E[XW_MAX_RUNGS];
@@ -792,48 +817,11 @@ __global__ void exchange_kernel(XwJob* jobs, int njobs, uint8_t* arena, const ui
     J.exch_round = round + 1;
 }
 
-}  // namespace
-
-uint32_t anneal_slot_bytes(int n, int m) { return slot_layout(n, m).bytes; }
-
-int anneal_opl(int n) { return n <= 32 ? 1 : n <= 64 ? 2 : 4; }
-
-const void* anneal_kernel_fn(int opl) {
-    if (opl == 1) return reinterpret_cast<const void*>(&anneal_kernel<1>);
-    if (opl == 2) return reinterpret_cast<const void*>(&anneal_kernel<2>);
-    return reinterpret_cast<const void*>(&anneal_kernel<4>);
-}
-
-cudaError_t launch_anneal(const AnnealArgs& args, int opl, int warps_per_block, int blocks,
-                          cudaStream_t stream) {
-    const size_t smem = (size_t)warps_per_block * args.slot_bytes;
-    const dim3 grid(blocks), block(32 * warps_per_block);
-    if (opl == 1) anneal_kernel<1><<<grid, block, smem, stream>>>(args);
-    else if (opl == 2) anneal_kernel<2><<<grid, block, smem, stream>>>(args);
-    else anneal_kernel<4><<<grid, block, smem, stream>>>(args);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_exchange(XwJob* jobs, int njobs, uint8_t* arena, const uint64_t* rec_off,
-                            const double* ladder, cudaStream_t stream) {
-    if (njobs <= 0) return cudaSuccess;
-    exchange_kernel<<<(njobs + 127) / 128, 128, 0, stream>>>(jobs, njobs, arena, rec_off, ladder);
-    return cudaGetLastError();
-}
-
-}  // namespace xw
-
-// ---- result collection --------------------------------------------------
-namespace xw {
-
-namespace {
-
 // One warp per job: best replica by (best score, best conflicts, replica
 // index) -- select_best_replica, xweigh_cuda.cu:1342-1354 -- summed
 // counters, and a copy of the best replica's best W into a compact buffer.
-__global__ void collect_kernel(const XwJob* jobs, int njobs, const uint8_t* arena,
-                               const uint64_t* rec_off, const uint64_t* best_out_off,
-                               JobOut* out, int8_t* best_out) {
+__global__ void collect_kernel(const XwJob* jobs, int njobs, const uint8_t* arena, const uint64_t* rec_off,
+                               const uint64_t* best_out_off, JobOut* out, int8_t* best_out) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= njobs) return;
@@ -883,12 +871,36 @@ __global__ void mark_t0_kernel(uint64_t* t0) {
 
 }  // namespace
 
-cudaError_t launch_collect(const XwJob* jobs, int njobs, const uint8_t* arena, const uint64_t* rec_off,
-                           const uint64_t* best_out_off, JobOut* out, int8_t* best_out,
-                           cudaStream_t stream) {
+uint32_t anneal_slot_bytes(int n, int m) { return slot_layout(n, m).bytes; }
+
+int anneal_opl(int n) { return n <= 32 ? 1 : n <= 64 ? 2 : 4; }
+
+const void* anneal_kernel_fn(int opl) {
+    if (opl == 1) return reinterpret_cast<const void*>(&anneal_kernel<1>);
+    if (opl == 2) return reinterpret_cast<const void*>(&anneal_kernel<2>);
+    return reinterpret_cast<const void*>(&anneal_kernel<4>);
+}
+
+cudaError_t launch_anneal(const AnnealArgs& args, int opl, int warps_per_block, int blocks, cudaStream_t stream) {
+    const size_t smem = (size_t)warps_per_block * args.slot_bytes;
+    const dim3 grid(blocks), block(32 * warps_per_block);
+    if (opl == 1) anneal_kernel<1><<<grid, block, smem, stream>>>(args);
+    else if (opl == 2) anneal_kernel<2><<<grid, block, smem, stream>>>(args);
+    else anneal_kernel<4><<<grid, block, smem, stream>>>(args);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_exchange(XwJob* jobs, int njobs, uint8_t* arena, const uint64_t* rec_off, const double* ladder,
+                            int stop_on_solve, cudaStream_t stream) {
     if (njobs <= 0) return cudaSuccess;
-    collect_kernel<<<(njobs + 3) / 4, 128, 0, stream>>>(jobs, njobs, arena, rec_off, best_out_off, out,
-                                                         best_out);
+    exchange_kernel<<<(njobs + 127) / 128, 128, 0, stream>>>(jobs, njobs, arena, rec_off, ladder, stop_on_solve);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_collect(const XwJob* jobs, int njobs, const uint8_t* arena, const uint64_t* rec_off,
+                           const uint64_t* best_out_off, JobOut* out, int8_t* best_out, cudaStream_t stream) {
+    if (njobs <= 0) return cudaSuccess;
+    collect_kernel<<<(njobs + 3) / 4, 128, 0, stream>>>(jobs, njobs, arena, rec_off, best_out_off, out, best_out);
     return cudaGetLastError();
 }
 

@@ -57,12 +57,32 @@ __device__ __forceinline__ bool lemire_ok(uint32_t v, uint32_t count, uint32_t& 
 __device__ __noinline__ uint32_t lemire_retry(uint32_t slot, uint64_t it, uint32_t stream,
                                               uint32_t k0, uint32_t k1, int j, uint32_t count) {
     uint32_t out = 0;
+#pragma unroll 1
     for (uint32_t retry = 1; retry <= 255; ++retry) {
         const uint4 b = draw_block((slot & 0x00ffffffu) | (retry << 24), it, stream, k0, k1);
         const uint32_t v = pick(b, j);
         if (lemire_ok(v, count, out) || retry == 255) return out;
     }
     return out;
+}
+
+// The rare branch of an index draw (low word below count): the threshold
+// test that needs an integer remainder, then retries.  Out of line so the
+// common path of every index draw is a multiply and a compare.
+__device__ __noinline__ uint32_t lemire_edge(uint32_t v, uint32_t slot, uint64_t it, uint32_t stream,
+                                             uint32_t k0, uint32_t k1, int j, uint32_t count) {
+    uint32_t out;
+    if (lemire_ok(v, count, out)) return out;
+    return lemire_retry(slot, it, stream, k0, k1, j, count);
+}
+
+// Index in [0,count) from word v of (slot, j): Lemire's multiply-shift with
+// the rejection handled by lemire_edge.
+__device__ __forceinline__ uint32_t draw_index(uint32_t v, uint32_t count, uint32_t slot, uint64_t it,
+                                               uint32_t stream, uint32_t k0, uint32_t k1, int j) {
+    const uint64_t prod = (uint64_t)v * count;
+    if ((uint32_t)prod >= count) return (uint32_t)(prod >> 32);
+    return lemire_edge(v, slot, it, stream, k0, k1, j, count);
 }
 
 // exp(x) for x <= 0 by Cody-Waite reduction and a degree-14 Taylor

@@ -277,6 +277,14 @@ void Batch::build(const xw_job_spec* specs, int njobs, const xw_params& p, const
             H->temperature = temps[r];
             H->reheat_temperature = temps[r];
             H->rung = r;
+            // start scores, so that results read before the first launch
+            // are meaningful; the kernel rebuilds and checks them
+            {
+                int64_t st[4];
+                xw_score(n, w, W[r].data(), st);
+                H->score = H->best_score = (int32_t)st[0];
+                H->conflicts = H->best_conflicts = (int32_t)st[1];
+            }
             if (p.objective >= 0) {
                 H->obj_kind = p.objective;
             } else {
@@ -382,21 +390,28 @@ uint64_t Batch::round_iters() const {
     return tempering ? (uint64_t)params.exchange_interval : (uint64_t)params.moves_per_launch;
 }
 
-void Batch::enqueue_rounds(uint64_t iters) {
-    const uint64_t per = round_iters();
-    const int rounds = (int)((iters + per - 1) / per);
-    if ((int)events.size() < 2 * rounds) {
-        while ((int)events.size() < 2 * rounds) {
-            cudaEvent_t e;
-            check(cudaEventCreate(&e), "cudaEventCreate");
-            events.push_back(e);
-        }
+// Events and work counters for `rounds` rounds; allocated outside any
+// stream capture.
+void Batch::reserve_rounds(int rounds) {
+    while ((int)events.size() < 2 * rounds) {
+        cudaEvent_t e;
+        check(cudaEventCreate(&e), "cudaEventCreate");
+        events.push_back(e);
     }
     if (counters_cap < rounds) {
+        check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
         if (d_counters) cudaFree(d_counters);
+        d_counters = nullptr;
         check(cudaMalloc(&d_counters, sizeof(uint32_t) * rounds), "cudaMalloc counters");
         counters_cap = rounds;
     }
+}
+
+void Batch::enqueue_rounds(uint64_t iters, bool timed) {
+    const uint64_t per = round_iters();
+    const int rounds = (int)((iters + per - 1) / per);
+    if ((int)events.size() < 2 * rounds || counters_cap < rounds)
+        throw std::logic_error("round resources not reserved");
     check(launch_mark_t0(static_cast<uint64_t*>(d_t0), stream), "launch mark_t0");
     check(cudaMemsetAsync(d_counters, 0, sizeof(uint32_t) * rounds, stream), "cudaMemsetAsync counters");
     uint64_t left = iters;
@@ -413,22 +428,24 @@ void Batch::enqueue_rounds(uint64_t iters) {
         a.stop_on_solve = params.stop_on_solve;
         a.pad = 0;
         left -= a.iters;
-        check(cudaEventRecord(events[2 * k], stream), "cudaEventRecord");
+        if (timed) check(cudaEventRecord(events[2 * k], stream), "cudaEventRecord");
         check(launch_anneal(a, opl, warps_per_block, blocks, stream), "launch anneal_kernel");
-        check(cudaEventRecord(events[2 * k + 1], stream), "cudaEventRecord");
+        if (timed) check(cudaEventRecord(events[2 * k + 1], stream), "cudaEventRecord");
         if (tempering)
             check(launch_exchange(static_cast<XwJob*>(d_jobs), (int)jobs.size(), static_cast<uint8_t*>(d_arena),
                                   static_cast<const uint64_t*>(d_rec_off), static_cast<const double*>(d_ladder),
-                                  stream),
+                                  params.stop_on_solve, stream),
                   "launch exchange_kernel");
     }
-    last_rounds = rounds;
+    last_rounds = timed ? rounds : 0;
 }
 
 void Batch::run(uint64_t iters, bool use_graph) {
     if (iters == 0) return;
+    const uint64_t per = round_iters();
+    reserve_rounds((int)((iters + per - 1) / per));
     if (!use_graph) {
-        enqueue_rounds(iters);
+        enqueue_rounds(iters, true);
         return;
     }
     if (!graph_exec || graph_iters != iters) {
@@ -439,7 +456,7 @@ void Batch::run(uint64_t iters, bool use_graph) {
         cudaGraph_t g;
         check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
         try {
-            enqueue_rounds(iters);
+            enqueue_rounds(iters, false);
         } catch (...) {
             cudaStreamEndCapture(stream, &g);
             if (g) cudaGraphDestroy(g);
@@ -451,7 +468,11 @@ void Batch::run(uint64_t iters, bool use_graph) {
         check(e, "cudaGraphInstantiate");
         graph_iters = iters;
     }
+    // events outside the graph: the time of the whole graph launch
+    check(cudaEventRecord(events[0], stream), "cudaEventRecord");
     check(cudaGraphLaunch(graph_exec, stream), "cudaGraphLaunch");
+    check(cudaEventRecord(events[1], stream), "cudaEventRecord");
+    last_rounds = 1;
 }
 
 void Batch::collect(std::vector<JobOut>& out, int8_t* best_host, bool want_best) {
@@ -739,6 +760,14 @@ int32_t xw_batch_run(xw_batch* h, uint64_t iters) {
     if (!h) return fail(XW_ERR_INVALID, "null batch");
     XW_GUARD({
         h->b->run(iters, true);
+        return XW_OK;
+    })
+}
+
+int32_t xw_batch_run_timed(xw_batch* h, uint64_t iters) {
+    if (!h) return fail(XW_ERR_INVALID, "null batch");
+    XW_GUARD({
+        h->b->run(iters, false);
         return XW_OK;
     })
 }

@@ -70,7 +70,8 @@ struct Batch {
     void configure_shape(int warps_per_block);
     void reset();
     uint64_t round_iters() const;
-    void enqueue_rounds(uint64_t iters);
+    void reserve_rounds(int rounds);
+    void enqueue_rounds(uint64_t iters, bool timed);
     void run(uint64_t iters, bool use_graph);
     void collect(std::vector<JobOut>& out, int8_t* best_host, bool want_best);
     void fill_results(const std::vector<JobOut>& out, const int8_t* best_host, xw_job_result* res) const;

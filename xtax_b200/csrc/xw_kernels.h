@@ -31,7 +31,7 @@ const void* anneal_kernel_fn(int opl);
 cudaError_t launch_anneal(const AnnealArgs& args, int opl, int warps_per_block, int blocks,
                           cudaStream_t stream);
 cudaError_t launch_exchange(XwJob* jobs, int njobs, uint8_t* arena, const uint64_t* rec_off,
-                            const double* ladder, cudaStream_t stream);
+                            const double* ladder, int stop_on_solve, cudaStream_t stream);
 
 }  // namespace xw
 
