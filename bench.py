@@ -1,0 +1,375 @@
+"""Benchmark: moves/sec of the uniform tempering population, W(26,25).
+
+Workload (one "step"): 128 independent W(26,25) searches x 32-rung
+geometric tempering ladder (T 0.1 .. 6, exchange every 10^4 iterations),
+4096 replicas, 10^9 moves (244141 iterations per replica), each replica
+starting from the reference's seeded regular random start.  Seeds are
+per instance, so every step is the same computation (the population is
+reset on the device between steps).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on rank 0.  `value` is device-timed moves/sec with the start
+states resident in HBM; `e2e` is the same metric through the C ABI's
+whole-batch call (xw_batch_solve) with host buffers, host<->device copies
+inside the timed region.  `--impl reference` times the reference's own
+CPU engine (oracle/_ref/xweigh, all host threads) on the same (n, w) and
+tempering setup.  N > 1: one process per GPU, each running its own 128
+instances (weak scaling, no collective on the data path).
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+N_ORDER, W_WEIGHT = 26, 25
+INSTANCES, RUNGS = 128, 32
+TOTAL_MOVES = 10 ** 9
+EXCHANGE = 10_000
+T_MIN, T_MAX = 0.1, 6.0
+ITERS = -(-TOTAL_MOVES // (INSTANCES * RUNGS))   # 244141 iterations per replica
+REF_XWEIGH = os.path.join(REPO, "oracle", "_ref", "xweigh")
+REF_XWEIGH_CUDA = os.path.join(REPO, "oracle", "_ref", "xweigh_cuda")
+METRIC = "moves/sec (uniform W(26,25) tempering population)"
+WORKLOAD = (f"W({N_ORDER},{W_WEIGHT}): {INSTANCES} instances x {RUNGS}-rung tempering ladder "
+            f"T {T_MIN}..{T_MAX}, exchange every {EXCHANGE} moves, {TOTAL_MOVES:.0e} moves per step")
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_info():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), \
+        int(os.environ.get("LOCAL_RANK", "0"))
+
+
+# ---------------------------------------------------------------- reference CPU
+def run_reference_cpu(seconds, threads, seed=1):
+    """The reference xweigh on `threads` host threads for `seconds`; returns
+    (moves, seconds) from its `done moves=... seconds=...` line
+    (xweigh_anneal.hpp:1263-1265)."""
+    with tempfile.TemporaryDirectory() as td:
+        out = subprocess.run(
+            [REF_XWEIGH, str(N_ORDER), str(W_WEIGHT), "-t", str(threads), "--seed", str(seed),
+             "--max-seconds", str(seconds), "--t-init", str(T_MAX), "--t-min", str(T_MIN),
+             "--exchange-interval", str(EXCHANGE), "-o", os.path.join(td, "w.csv")],
+            capture_output=True, text=True, timeout=seconds * 4 + 60)
+    m = re.search(r"done moves=(\d+) seconds=([0-9.e+-]+)", out.stdout)
+    if not m:
+        raise RuntimeError("reference xweigh gave no done line: " + out.stdout[-300:] + out.stderr[-300:])
+    return int(m.group(1)), float(m.group(2))
+
+
+def run_reference_cuda(seconds, seed=1):
+    """The reference xweigh_cuda (the plain kernel, one instance per launch)
+    on the same shape: 4096 replicas of W(26,25)."""
+    with tempfile.TemporaryDirectory() as td:
+        out = subprocess.run(
+            [REF_XWEIGH_CUDA, str(N_ORDER), str(W_WEIGHT), "--replicas", str(INSTANCES * RUNGS),
+             "--t-init", str(T_MAX), "--t-min", str(T_MIN), "--seed", str(seed), "--max-seconds", str(seconds),
+             "--restart-interval", "0", "-o", os.path.join(td, "w.csv")],
+            capture_output=True, text=True, timeout=seconds * 4 + 120)
+    m = re.search(r"done moves=(\d+) .*?seconds=([0-9.e+-]+) moves_per_sec=([0-9.e+-]+)", out.stdout)
+    if not m:
+        raise RuntimeError("reference xweigh_cuda gave no done line: " + out.stdout[-300:] + out.stderr[-300:])
+    return int(m.group(1)), float(m.group(2))
+
+
+def reference_arm(args):
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return
+    if not os.path.exists(REF_XWEIGH):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/xweigh was not built"}))
+        return
+    threads = os.cpu_count() or 1
+    sample = args.ref_seconds
+    for _ in range(args.warmup):
+        run_reference_cpu(max(1.0, sample / 4), threads)
+    moves = secs = 0
+    for k in range(args.steps):
+        mv, s = run_reference_cpu(sample, threads, seed=1 + k)
+        moves += mv
+        secs += s
+    value = moves / secs
+    line = {
+        "metric": METRIC, "value": value, "unit": "moves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": WORKLOAD, "engine": "reference xweigh CPU, parallel tempering over threads",
+                   "threads": threads, "sample_seconds_per_step": sample},
+        "cpu_baseline": {"value": value, "unit": "moves/s", "cores": threads, "kind": "reference",
+                         "sample": f"xweigh {N_ORDER} {W_WEIGHT} -t {threads} --max-seconds {sample} per step"},
+        "e2e": {"value": value, "unit": "moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.rows = []
+        if self.proc is None:
+            return
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        for line in out.splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def summary(self):
+        rows = getattr(self, "rows", [])
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+
+        def mhz(s):
+            m = re.match(r"([0-9.]+)", s)
+            return float(m.group(1)) if m else None
+
+        sm = [mhz(r[1]) for r in rows if mhz(r[1])]
+        mx = [mhz(r[2]) for r in rows if mhz(r[2])]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------- ours
+def make_jobs(rank):
+    return [{"n": N_ORDER, "w": W_WEIGHT, "seed": 1 + rank * INSTANCES + i, "replicas": RUNGS}
+            for i in range(INSTANCES)]
+
+
+def make_params():
+    import xtax_b200 as X
+    # tempering on the L1 score for every rung (no alternate objectives),
+    # reference move mix otherwise; replicas keep running after a solve so
+    # every step does the same 10^9 moves
+    return X.Params(tempering=1, exchange_interval=EXCHANGE, t_min=T_MIN, t_init=T_MAX,
+                    squared_objective_fraction=0.0, parity_objective_fraction=0.0, stop_on_solve=0)
+
+
+def algorithmic_smem_bytes(moves, cand_evals, n=N_ORDER, g=4):
+    """Shared-memory bytes a move needs at minimum: each evaluated candidate
+    reads k rows of (n-1) Gram entries (g bytes) and (n-1) W entries per
+    changed row; an accepted move writes 2k(n-1) Gram entries.  k = 1.5 for
+    this move mix (flips 1 row; switches and double flips 2 rows, a quarter
+    of the double flips on one row)."""
+    k = 1.5
+    reads = cand_evals * k * (n - 1) * (g + 1)
+    writes = moves * 0.5 * 2 * k * (n - 1) * g   # about half of the moves are accepted
+    return reads + writes
+
+
+def ours(args):
+    import torch
+    import xtax_b200 as X
+
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    p = make_params()
+    p.device = local
+    jobs = make_jobs(rank)
+    t_build = time.time()
+    batch = X.Batch(jobs, p)
+    log(f"[bench] rank {rank}: batch built in {time.time() - t_build:.1f}s shape={batch.shape()}")
+    # a dedicated stream: the library launches on it and the CUDA events
+    # below are recorded on it (the legacy default stream has handle 0,
+    # which the library would read as "use your own stream")
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    batch.set_stream(stream.cuda_stream)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    def step(timed):
+        batch.reset()
+        if timed:
+            batch.run_timed(ITERS)
+        else:
+            batch.run(ITERS)
+
+    for _ in range(args.warmup):
+        step(False)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    step_ms, launch_ms = [], []
+    moves = evals = 0
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.fill_(k & 0xff)
+            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            step(True)
+            stop.record(stream)
+            stop.synchronize()
+            step_ms.append(start.elapsed_time(stop))
+            launch_ms.extend(batch.launch_times())
+            res = batch.results()
+            moves += sum(r.moves for r, _ in res)
+            evals += sum(r.candidate_evaluations for r, _ in res)
+    torch.cuda.synchronize()
+    barrier()
+    total_ms = sum(step_ms)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([total_ms, float(moves), float(evals)], device="cuda", dtype=torch.float64)
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        total_ms, moves, evals = mx[0].item(), t[1].item(), t[2].item()
+    value = moves / (total_ms / 1e3)
+
+    # end to end: the C ABI whole-batch call with host buffers
+    starts = None
+    e2e_value = None
+    h2d, d2h = batch.transfer_bytes()
+    if args.e2e_steps > 0:
+        import numpy as np
+        starts = np.concatenate([X.random_start(N_ORDER, W_WEIGHT, (j["seed"] + r * 0x9e3779b9) & 0xffffffff)
+                                 for j in jobs for r in range(RUNGS)])
+        pinned = torch.from_numpy(starts).pin_memory()
+        host = pinned.numpy()
+        e2e_moves = 0
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            res, best = X.batch_solve(jobs, p, starts=host, iters=ITERS)
+            e2e_moves += sum(r.moves for r in res)
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([e2e_s, float(e2e_moves)], device="cuda", dtype=torch.float64)
+            mx = t.clone()
+            dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+            dist.all_reduce(t, op=dist.ReduceOp.SUM)
+            e2e_s, e2e_moves = mx[0].item(), t[1].item()
+        e2e_value = e2e_moves / e2e_s
+
+    clocks = clk.summary()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+
+    anneal_launches = [ms for ms in launch_ms if ms > 0]
+    avg_launch_ms = statistics.mean(anneal_launches)
+    per_launch_moves = moves / max(1, len(anneal_launches)) / world
+    per_launch_evals = evals / max(1, len(anneal_launches)) / world
+    alg_bytes = algorithmic_smem_bytes(per_launch_moves, per_launch_evals)
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    smem_peak = 148 * 128 * sm_mhz * 1e6 / 1e9   # GB/s, nominal: 128 B/clk/SM
+    achieved = alg_bytes / (avg_launch_ms / 1e3) / 1e9
+    prof = load_profile_traffic()
+    line = {
+        "metric": METRIC, "value": value, "unit": "moves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "replicas_per_gpu": INSTANCES * RUNGS,
+                   "iterations_per_replica": ITERS, "l2": "flushed between steps (256 MiB write)",
+                   "launch_shape": list(batch.shape()), "parallelism": f"instances x{world} GPUs"},
+        "gpu_launches": args.steps * (2 * (-(-ITERS // EXCHANGE)) + 1),
+        "roofline": {"bound": "smem", "achieved": achieved, "peak": smem_peak, "unit": "GB/s",
+                     "frac": achieved / smem_peak, "traffic": prof,
+                     "kernel": "anneal_kernel", "avg_launch_ms": avg_launch_ms,
+                     "peak_source": "nominal 128 B/clk/SM x 148 SMs x median SM clock (no measured shared-memory peak)"},
+        "clocks": clocks,
+    }
+    if e2e_value is not None:
+        line["e2e"] = {"value": e2e_value, "unit": "moves/s", "h2d_bytes_per_step": h2d,
+                       "d2h_bytes_per_step": d2h}
+    if args.cpu_seconds > 0 and os.path.exists(REF_XWEIGH):
+        threads = os.cpu_count() or 1
+        mv, s = run_reference_cpu(args.cpu_seconds, threads)
+        line["cpu_baseline"] = {"value": mv / s, "unit": "moves/s", "cores": threads, "kind": "reference",
+                                "sample": f"reference xweigh {N_ORDER} {W_WEIGHT} -t {threads} tempering, "
+                                          f"{args.cpu_seconds:g} s wall"}
+    if args.plain_seconds > 0 and os.path.exists(REF_XWEIGH_CUDA):
+        try:
+            mv, s = run_reference_cuda(args.plain_seconds)
+            line["plain_kernel"] = {"impl": "reference xweigh_cuda (sm_100a build)", "value": mv / s,
+                                    "unit": "moves/s", "replicas": INSTANCES * RUNGS,
+                                    "sample_seconds": args.plain_seconds}
+        except Exception as e:  # noqa: BLE001 - report, do not fail the bench
+            line["plain_kernel"] = {"unavailable": str(e)[:200]}
+    print(json.dumps(line), flush=True)
+
+
+def load_profile_traffic():
+    """DRAM bytes per anneal launch from the committed ncu summary, if any."""
+    path = os.path.join(REPO, "profiles", "anneal_kernel_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    except (OSError, ValueError):
+        return None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--plain-seconds", type=float, default=10.0)
+    ap.add_argument("--ref-seconds", type=float, default=10.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        log("[bench] warmup raised to 3")
+        args.warmup = 3
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -224,6 +224,10 @@ typedef struct xw_replica_state {
 int32_t xw_batch_read_replica(xw_batch* b, int32_t job, int32_t replica, xw_replica_state* st,
                               int8_t* W, int8_t* best_W, uint8_t* minority);
 
+/* Bytes the batch moves between host and device: h2d at creation (replica
+ * records, job table, offsets, ladder), d2h per xw_batch_results call. */
+int32_t xw_batch_bytes(xw_batch* b, uint64_t* h2d, uint64_t* d2h);
+
 /* Launch shape of the batch: warps per block, blocks, shared bytes per warp. */
 int32_t xw_batch_shape(xw_batch* b, int32_t* warps_per_block, int32_t* blocks, int32_t* slot_bytes);
 void xw_batch_destroy(xw_batch* b);

@@ -137,6 +137,7 @@ def lib():
             "xw_batch_read_replica": (i32, [C.c_void_p, i32, i32, P(ReplicaState), P(i8), P(i8),
                                             P(C.c_uint8)]),
             "xw_batch_shape": (i32, [C.c_void_p, P(i32), P(i32), P(i32)]),
+            "xw_batch_bytes": (i32, [C.c_void_p, P(u64), P(u64)]),
             "xw_batch_destroy": (None, [C.c_void_p]),
             "xw_batch_solve": (i32, [P(JobSpec), i32, P(_Params), P(i8), u64, P(JobResult), P(i8)]),
         }
@@ -393,6 +394,12 @@ class Batch:
         a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
         _check(lib().xw_batch_shape(self.h, C.byref(a), C.byref(b), C.byref(c)))
         return a.value, b.value, c.value
+
+    def transfer_bytes(self):
+        """(host-to-device bytes at creation, device-to-host bytes per results())"""
+        a, b = C.c_uint64(), C.c_uint64()
+        _check(lib().xw_batch_bytes(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def results(self):
         res = (JobResult * len(self.jobs))()

@@ -849,6 +849,17 @@ int32_t xw_batch_read_replica(xw_batch* h, int32_t job, int32_t replica, xw_repl
     })
 }
 
+int32_t xw_batch_bytes(xw_batch* h, uint64_t* h2d, uint64_t* d2h) {
+    if (!h) return fail(XW_ERR_INVALID, "null batch");
+    const Batch& b = *h->b;
+    if (h2d)
+        *h2d = b.arena_bytes + sizeof(XwJob) * b.jobs.size() + sizeof(uint64_t) * b.total_replicas +
+               sizeof(uint32_t) * b.total_replicas + sizeof(double) * b.ladder.size() +
+               sizeof(uint64_t) * b.jobs.size();
+    if (d2h) *d2h = sizeof(JobOut) * b.jobs.size() + b.best_bytes + sizeof(uint64_t);
+    return XW_OK;
+}
+
 int32_t xw_batch_shape(xw_batch* h, int32_t* wpb, int32_t* blocks, int32_t* slot) {
     if (!h) return fail(XW_ERR_INVALID, "null batch");
     if (wpb) *wpb = h->b->warps_per_block;
