@@ -239,6 +239,30 @@ int32_t xw_batch_solve(const xw_job_spec* jobs, int32_t njobs, const xw_params* 
                        const int8_t* starts, uint64_t iters,
                        xw_job_result* results, int8_t* best);
 
+/* ---- annealing without device allocation ------------------------------ */
+/* No counterpart in the reference: an entry point for callers that cannot
+ * call cudaMalloc -- hosts whose device memory belongs to their own pool
+ * allocator or fixed budget, and loops that cannot take the device
+ * synchronisation that cudaMalloc/cudaFree imply.  It anneals one W(n,w)
+ * search of `replicas` replicas for `iters` iterations with the batch
+ * engine's kernels (cooling, or a tempering ladder when p->tempering),
+ * keeping all scratch state in a static device array of
+ * XW_NOALLOC_SCRATCH_BYTES (4 MiB) that every GPU loading this library holds
+ * until exit; a request that needs more is rejected with XW_ERR_CAPACITY.
+ * Inputs and outputs are the caller's device buffers:
+ *   starts  replicas*n*n int8, column-major start states
+ *   best    replicas*n*n int8, each replica's best state
+ *   stats   replicas*4 int64: best score, best conflicts, score, moves
+ * p->t_init must be positive (no host calibration).  Work is enqueued on
+ * `stream` (cudaStream_t, NULL = legacy default) and the call returns
+ * without waiting.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) with that device current; make it before
+ * any stream capture.  Calls share the array: calls that overlap on the GPU
+ * race, so serialise them; each call rewrites the array from its inputs. */
+#define XW_NOALLOC_SCRATCH_BYTES (4 * 1024 * 1024)
+int32_t xw_anneal_noalloc(int32_t n, int32_t w, const xw_params* p, int32_t replicas, uint64_t iters,
+                          const int8_t* starts, int8_t* best, int64_t* stats, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

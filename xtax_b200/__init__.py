@@ -140,6 +140,8 @@ def lib():
             "xw_batch_bytes": (i32, [C.c_void_p, P(u64), P(u64)]),
             "xw_batch_destroy": (None, [C.c_void_p]),
             "xw_batch_solve": (i32, [P(JobSpec), i32, P(_Params), P(i8), u64, P(JobResult), P(i8)]),
+            "xw_anneal_noalloc": (i32, [i32, i32, P(_Params), i32, u64, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)

@@ -54,7 +54,7 @@ __device__ __forceinline__ bool lemire_ok(uint32_t v, uint32_t count, uint32_t& 
     return low >= count || low >= (0u - count) % count;
 }
 
-__device__ __noinline__ uint32_t lemire_retry(uint32_t slot, uint64_t it, uint32_t stream,
+static __device__ __noinline__ uint32_t lemire_retry(uint32_t slot, uint64_t it, uint32_t stream,
                                               uint32_t k0, uint32_t k1, int j, uint32_t count) {
     uint32_t out = 0;
 #pragma unroll 1
@@ -69,7 +69,7 @@ __device__ __noinline__ uint32_t lemire_retry(uint32_t slot, uint64_t it, uint32
 // The rare branch of an index draw (low word below count): the threshold
 // test that needs an integer remainder, then retries.  Out of line so the
 // common path of every index draw is a multiply and a compare.
-__device__ __noinline__ uint32_t lemire_edge(uint32_t v, uint32_t slot, uint64_t it, uint32_t stream,
+static __device__ __noinline__ uint32_t lemire_edge(uint32_t v, uint32_t slot, uint64_t it, uint32_t stream,
                                              uint32_t k0, uint32_t k1, int j, uint32_t count) {
     uint32_t out;
     if (lemire_ok(v, count, out)) return out;

@@ -92,6 +92,8 @@ void parallel_for(int count, F f) {
 
 namespace xw {
 
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
 std::string validate(int n, int w, const xw_params& p) {
     if (n < 1 || n > 32767) return "CUDA xweigh order is out of range";
     if (w < 1 || w > n) return "CUDA xweigh weight must be in [1, n]";

@@ -12,6 +12,7 @@
 namespace xw {
 
 std::string validate(int n, int w, const xw_params& p);
+void set_last_error(const std::string& msg);
 
 // Warps per block for the anneal kernel of a given lanes-per-row class and
 // shared-memory slot, from the autotuner's cache (xw_tune.cpp).

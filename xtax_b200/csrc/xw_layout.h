@@ -19,6 +19,7 @@
 #define XW_MAX_N 128
 #define XW_MAX_CANDIDATES 32
 #define XW_MAX_TARGET_SAMPLES 64
+#define XW_NOALLOC_SCRATCH_BYTES (4 * 1024 * 1024)
 
 #define XW_STATUS_INIT 1u      // record holds incremental state (score etc.)
 #define XW_STATUS_SOLVED 2u    // best score reached 0
