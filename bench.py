@@ -220,12 +220,14 @@ def ours(args):
     batch.set_stream(stream.cuda_stream)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
 
+    iters = args.iters
+
     def step(timed):
         batch.reset()
         if timed:
-            batch.run_timed(ITERS)
+            batch.run_timed(iters)
         else:
-            batch.run(ITERS)
+            batch.run(iters)
 
     for _ in range(args.warmup):
         step(False)
@@ -279,7 +281,7 @@ def ours(args):
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
-            res, best = X.batch_solve(jobs, p, starts=host, iters=ITERS)
+            res, best = X.batch_solve(jobs, p, starts=host, iters=iters)
             e2e_moves += sum(r.moves for r in res)
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
@@ -312,9 +314,9 @@ def ours(args):
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "replicas_per_gpu": INSTANCES * RUNGS,
-                   "iterations_per_replica": ITERS, "l2": "flushed between steps (256 MiB write)",
+                   "iterations_per_replica": iters, "l2": "flushed between steps (256 MiB write)",
                    "launch_shape": list(batch.shape()), "parallelism": f"instances x{world} GPUs"},
-        "gpu_launches": args.steps * (2 * (-(-ITERS // EXCHANGE)) + 1),
+        "gpu_launches": args.steps * (2 * (-(-iters // EXCHANGE)) + 1),
         "roofline": {"bound": "smem", "achieved": achieved, "peak": smem_peak, "unit": "GB/s",
                      "frac": achieved / smem_peak, "traffic": prof,
                      "kernel": "anneal_kernel", "avg_launch_ms": avg_launch_ms,
@@ -361,6 +363,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--plain-seconds", type=float, default=10.0)
     ap.add_argument("--ref-seconds", type=float, default=10.0)
+    ap.add_argument("--iters", type=int, default=ITERS, help="iterations per replica per step (profiling cases)")
     args = ap.parse_args()
     if args.warmup < 3:
         log("[bench] warmup raised to 3")

@@ -66,3 +66,19 @@ def test_run_annealer_drop_in_solves_small_order():
     assert O.verify(10, 9, r.best.entries) == 3
     assert any(line.startswith("done moves=") for line in r.log)
     assert any(line.startswith("[cuda] device=") for line in r.log)
+
+
+def test_cli_drop_in_solves_and_writes_csv(tmp_path):
+    import os
+    import subprocess
+    cli = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "xtax_b200", "bin", "xweigh_cuda")
+    out = tmp_path / "w.csv"
+    r = subprocess.run([cli, "12", "11", "--seed", "7", "--replicas", "512", "--max-seconds", "60", "-o", str(out)],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    lines = r.stdout.splitlines()
+    assert lines[0].startswith("[cuda] device=") and any(l.startswith("done moves=") for l in lines)
+    assert "Found W(12,11); exact verification passed" in r.stdout
+    rows = [list(map(int, l.split(","))) for l in out.read_text().splitlines()]
+    W = np.array(rows, dtype=np.int8).T.reshape(-1)   # column-major
+    assert O.verify(12, 11, W) == 3
