@@ -239,6 +239,26 @@ int32_t xw_batch_solve(const xw_job_spec* jobs, int32_t njobs, const xw_params* 
                        const int8_t* starts, uint64_t iters,
                        xw_job_result* results, int8_t* best);
 
+/* ---- batched exact rescoring and verification ------------------------- */
+/* Full recompute of G = W W^T for `count` row-major n x n int8 matrices
+ * (contiguous), the batched form of rebuild_gram_bits + verify_weighing
+ * (xweigh_anneal.hpp:429-453, 239-264).  stats receives 4 int32 per matrix:
+ * L1 score sum_{i<j}|G_ij|, conflicts #{i<j: G_ij != 0}, squared score
+ * sum_{i<j} G_ij^2, and 1 when G = wI exactly (else 0).  gram (nullable)
+ * receives each G as n*n row-major int32.  n a multiple of 32 runs on the
+ * tensor cores (tcgen05 kind::i8, int32 accumulation, exact since
+ * |G_ij| <= n); other n <= 128 on a SIMT kernel.  Host buffers. */
+int32_t xw_rescore(const int8_t* W_rowmajor, int64_t count, int32_t n, int32_t w, int32_t* stats,
+                   int32_t* gram);
+/* Same on device buffers, enqueued on `stream` (cudaStream_t); simt != 0
+ * forces the SIMT kernel.  Allocates nothing.  Check xw_rescore_status()
+ * after the stream completes. */
+int32_t xw_rescore_device(const int8_t* W_rowmajor, int64_t count, int32_t n, int32_t w, int32_t* stats,
+                          int32_t* gram, int32_t simt, void* stream);
+/* XW_OK, or XW_ERR_TIMEOUT when a rescoring pipeline wait expired since the
+ * last call (the flag is cleared).  Synchronous. */
+int32_t xw_rescore_status(void);
+
 /* ---- annealing without device allocation ------------------------------ */
 /* No counterpart in the reference: an entry point for callers that cannot
  * call cudaMalloc -- hosts whose device memory belongs to their own pool

@@ -142,6 +142,10 @@ def lib():
             "xw_batch_solve": (i32, [P(JobSpec), i32, P(_Params), P(i8), u64, P(JobResult), P(i8)]),
             "xw_anneal_noalloc": (i32, [i32, i32, P(_Params), i32, u64, C.c_void_p, C.c_void_p,
                                         C.c_void_p, C.c_void_p]),
+            "xw_rescore": (i32, [P(i8), C.c_int64, i32, i32, P(i32), P(i32)]),
+            "xw_rescore_device": (i32, [C.c_void_p, C.c_int64, i32, i32, C.c_void_p, C.c_void_p, i32,
+                                        C.c_void_p]),
+            "xw_rescore_status": (i32, []),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -327,6 +331,19 @@ def score(n, w, W):
 def verify(n, w, W):
     W = np.ascontiguousarray(W, dtype=np.int8)
     return lib().xw_verify(n, w, _i8(W))
+
+
+def rescore(W_rowmajor, n, w, gram=False):
+    """Batched exact W W^T (xw_rescore): W_rowmajor is (count, n, n) int8.
+    Returns stats (count, 4) int32 {score, conflicts, squared, exact} and,
+    with gram=True, G (count, n, n) int32."""
+    W = np.ascontiguousarray(W_rowmajor, dtype=np.int8)
+    count = W.size // (n * n)
+    stats = np.zeros((count, 4), dtype=np.int32)
+    G = np.zeros((count, n, n), dtype=np.int32) if gram else None
+    _check(lib().xw_rescore(_i8(W), count, n, w, stats.ctypes.data_as(C.POINTER(C.c_int32)),
+                            G.ctypes.data_as(C.POINTER(C.c_int32)) if gram else None))
+    return (stats, G) if gram else stats
 
 
 def impossibility_reason(n, w):

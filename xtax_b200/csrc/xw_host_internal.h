@@ -14,6 +14,10 @@ namespace xw {
 std::string validate(int n, int w, const xw_params& p);
 void set_last_error(const std::string& msg);
 
+// Enqueues the batched rescoring kernel (xw_rescore.cu).
+int32_t rescore_device(const int8_t* W, int64_t count, int n, int w, int32_t* stats, int32_t* gram,
+                       cudaStream_t stream, int* err_flag, bool force_simt);
+
 // Warps per block for the anneal kernel of a given lanes-per-row class and
 // shared-memory slot, from the autotuner's cache (xw_tune.cpp).
 int tuned_warps_per_block(int opl, uint32_t slot_bytes, int device);

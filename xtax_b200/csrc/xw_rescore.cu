@@ -1,0 +1,477 @@
+// xw_rescore.cu -- exact batched W W^T on the 5th-generation tensor cores.
+//
+// Full rescoring and verification of a batch of ternary matrices (the
+// reference does this on the CPU, one matrix at a time: rebuild_gram_bits /
+// verify_weighing, xweigh_anneal.hpp:239-264 and 429-453).  Per matrix it
+// returns the L1 score sum_{i<j}|G_ij|, the conflicts #{i<j: G_ij != 0},
+// the squared score sum_{i<j} G_ij^2 and the exact flag (G = wI), and
+// optionally G itself, with G = W W^T computed in int32 by
+// tcgen05.mma.kind::i8 -- exact, since |G_ij| <= n.
+//
+// Input: `count` row-major n x n int8 matrices, contiguous.  A tile is 128
+// rows of that array (4 matrices of n=32, 2 of n=64, 1 of n=96 or 128),
+// loaded by TMA with 128-byte swizzle into shared memory, the K (column)
+// extent zero-filled to 128.  One MMA chain computes D = A A^T (M = 128,
+// N = rows of the tile, K = 128 in four K=32 steps) into a TMEM
+// accumulator; the diagonal n x n blocks of D are the tile's Gram matrices.
+// The epilogue warps read their TMEM lane quarter (one row per thread) and
+// reduce the row statistics per matrix.  The kernel is persistent over
+// tiles with a 4-stage TMA ring, so loads of later tiles overlap the MMA and
+// the epilogue of the current one; at the benchmark's sizes it is HBM-bound
+// (n^2 bytes read per matrix, 2n^3 MACs).
+//
+// Every wait on an mbarrier has an iteration limit; on expiry the kernel
+// records an error code, waits (bounded) for its own loads still in flight,
+// releases its TMEM and returns.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "../../include/xw.h"
+#include "xw_host_internal.h"
+
+namespace xw {
+
+namespace {
+
+constexpr int kStages = 4;
+constexpr int kTileRows = 128;
+constexpr int kTileBytes = kTileRows * 128;   // 128 rows x 128 bytes (K padded to 128)
+constexpr uint32_t kTmemCols = 128;
+constexpr long long kSpinLimit = 1ll << 22;
+
+struct RescoreParams {
+    int count;          // matrices
+    int n, w;
+    int rows_per_tile;  // matrices per tile * n
+    int mpt;            // matrices per tile
+    int ntiles;
+    int4* stats;        // per matrix {score, conflicts, squared, exact}
+    int32_t* gram;      // nullable: per matrix n*n row-major
+    int* error;         // nonzero after a timed-out wait
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// bounded wait for the phase with parity `parity` to complete
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t addr = smem_addr(bar);
+    for (long long i = 0; i < kSpinLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+        ::"r"(smem_addr(dst)), "l"(map), "r"(smem_addr(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+// K-major operand with 128-byte swizzle: 8-row groups 1024 bytes apart.
+__device__ __forceinline__ uint64_t smem_desc(const void* tile) {
+    const uint64_t addr = smem_addr(tile);
+    uint64_t d = 0;
+    d |= (addr >> 4) & 0x3fffull;           // start address
+    d |= (uint64_t)1 << 16;                  // leading byte offset (unused for this layout)
+    d |= (uint64_t)(1024 >> 4) << 32;        // stride byte offset
+    d |= (uint64_t)1 << 46;                  // descriptor version for sm_100
+    d |= (uint64_t)2 << 61;                  // SWIZZLE_128B
+    return d;
+}
+
+// kind::i8, signed A and B, int32 D, both K-major, M = 128, N = n_cols
+__device__ __forceinline__ uint32_t instr_desc(int n_cols) {
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n_cols >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
+                 : "memory");
+}
+
+// 32 consecutive int32 columns of this warp's TMEM lane quarter, one row per thread
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, int (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(128, 1) rescore_tc_kernel(const __grid_constant__ CUtensorMap tmap,
+                                                             RescoreParams p) {
+    extern __shared__ uint8_t smem_raw[];
+    // tiles on a 1024-byte boundary (the 128-byte swizzle pattern repeats every 1024 bytes)
+    uint8_t* tiles = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    __shared__ __align__(8) uint64_t full_bar[kStages];
+    __shared__ __align__(8) uint64_t mma_bar;
+    __shared__ uint32_t tmem_base_sh;
+    __shared__ int abort_sh;
+    __shared__ int4 warp_part[4];
+    __shared__ int warp_diag_ok[4];
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_base_sh)),
+                     "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < kStages; ++s) mbar_init(&full_bar[s], 1);
+        mbar_init(&mma_bar, 1);
+        abort_sh = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_base_sh;
+
+    const int grid = gridDim.x;
+    // a TMA box delivers rows_per_tile rows of 128 bytes (zero fill included)
+    const uint32_t box_bytes = 128u * (uint32_t)p.rows_per_tile;
+    int issued = 0;  // loads issued by this CTA (thread 0's count)
+    if (tid == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            const int t = blockIdx.x + s * grid;
+            if (t >= p.ntiles) break;
+            mbar_expect_tx(&full_bar[s], box_bytes);
+            tma_load_2d(tiles + s * kTileBytes, &tmap, 0, t * p.rows_per_tile, &full_bar[s]);
+            ++issued;
+        }
+    }
+    const uint32_t idesc = instr_desc(p.rows_per_tile);
+    int iter = 0;
+    for (int t = blockIdx.x; t < p.ntiles; t += grid, ++iter) {
+        const int s = iter % kStages;
+        const uint32_t phase = (uint32_t)(iter / kStages) & 1u;
+        if (tid == 0 && !abort_sh) {
+            if (!mbar_wait(&full_bar[s], phase)) {
+                atomicExch(p.error, 1);
+                abort_sh = 1;
+            } else {
+                asm volatile("tcgen05.fence::after_thread_sync;");
+                const uint64_t d = smem_desc(tiles + s * kTileBytes);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) mma_i8(tmem, d + (uint64_t)(2 * k), d + (uint64_t)(2 * k), idesc, k > 0);
+                mma_commit(&mma_bar);
+            }
+        }
+        __syncthreads();
+        if (abort_sh) break;
+        if (!mbar_wait(&mma_bar, (uint32_t)iter & 1u)) {
+            atomicExch(p.error, 2);
+            abort_sh = 1;
+        }
+        __syncthreads();
+        if (abort_sh) {
+            // the MMA may still be running: give it one more bounded wait
+            // before the accumulator is released
+            if (tid == 0) mbar_wait(&mma_bar, (uint32_t)iter & 1u);
+            break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        // stage s is free again: fetch the tile kStages iterations ahead
+        if (tid == 0) {
+            const int tn = t + kStages * grid;
+            if (tn < p.ntiles) {
+                mbar_expect_tx(&full_bar[s], box_bytes);
+                tma_load_2d(tiles + s * kTileBytes, &tmap, 0, tn * p.rows_per_tile, &full_bar[s]);
+                ++issued;
+            }
+        }
+        // epilogue: warp w reads D rows 32w..32w+31 (its TMEM lane quarter)
+        const int row0 = 32 * warp;
+        const bool active = row0 < p.rows_per_tile;
+        int4 part = make_int4(0, 0, 0, 0);
+        int diag_ok = 1;
+        int b = 0;
+        if (active) {
+            const int r = row0 + lane;
+            b = row0 / p.n;                 // matrix of this warp within the tile
+            const int i = r - b * p.n;      // row within the matrix
+            const int mat = t * p.mpt + b;
+            const int col0 = b * p.n;
+            int s_abs = 0, s_nz = 0, s_sq = 0;
+            for (int c = 0; c < p.n; c += 32) {
+                int v[32];
+                tmem_ld32(tmem + ((uint32_t)row0 << 16) + (uint32_t)(col0 + c), v);
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int g = v[j];
+                    const int a = g < 0 ? -g : g;
+                    s_abs += a;
+                    s_nz += a < 1 ? a : 1;
+                    s_sq += g * g;
+                    if (c + j == i) {
+                        // diagonal: remove it from the off-diagonal sums and check G_ii = w
+                        s_abs -= a;
+                        s_nz -= a < 1 ? a : 1;
+                        s_sq -= g * g;
+                        diag_ok = g == p.w;
+                    }
+                }
+                if (p.gram && mat < p.count) {
+                    int32_t* dst = p.gram + (size_t)mat * p.n * p.n + (size_t)i * p.n + c;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) dst[j] = v[j];
+                }
+            }
+            part.x = __reduce_add_sync(0xffffffffu, s_abs);
+            part.y = __reduce_add_sync(0xffffffffu, s_nz);
+            part.z = __reduce_add_sync(0xffffffffu, s_sq);
+            diag_ok = (int)__reduce_and_sync(0xffffffffu, (unsigned)diag_ok);
+        }
+        if (lane == 0) {
+            warp_part[warp] = part;
+            warp_diag_ok[warp] = diag_ok;
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+        // one thread per matrix of the tile combines its warps
+        if (tid < p.mpt) {
+            const int mat = t * p.mpt + tid;
+            if (mat < p.count) {
+                const int wpm = (p.n + 31) / 32;   // warps per matrix
+                int4 tot = make_int4(0, 0, 0, 1);
+                for (int q = tid * wpm; q < tid * wpm + wpm && q < 4; ++q) {
+                    tot.x += warp_part[q].x;
+                    tot.y += warp_part[q].y;
+                    tot.z += warp_part[q].z;
+                    tot.w &= warp_diag_ok[q];
+                }
+                // symmetric G: the off-diagonal sums count each pair twice
+                int4 o;
+                o.x = tot.x / 2;
+                o.y = tot.y / 2;
+                o.z = tot.z / 2;
+                o.w = (tot.y == 0 && tot.w) ? 1 : 0;
+                p.stats[mat] = o;
+            }
+        }
+        __syncthreads();
+    }
+    // drain: wait (bounded) for this CTA's loads that are still in flight
+    if (tid == 0) {
+        for (int k = iter; k < issued; ++k) mbar_wait(&full_bar[k % kStages], (uint32_t)(k / kStages) & 1u);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+}
+
+// SIMT path for orders that do not fill 32-row tensor-core blocks: one warp
+// per matrix, lane o accumulates column o of G.
+__global__ void rescore_simt_kernel(const int8_t* W, int count, int n, int w, int4* stats, int32_t* gram) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= count) return;
+    const int8_t* M = W + (size_t)warp * n * n;
+    int s_abs = 0, s_nz = 0, s_sq = 0, diag_ok = 1;
+    for (int o = lane; o < n; o += 32) {
+        for (int r = 0; r < n; ++r) {
+            int dot = 0;
+            for (int c = 0; c < n; ++c) dot += M[r * n + c] * M[o * n + c];
+            if (gram) gram[(size_t)warp * n * n + (size_t)r * n + o] = dot;
+            if (r == o) {
+                diag_ok &= dot == w;
+            } else {
+                const int a = dot < 0 ? -dot : dot;
+                s_abs += a;
+                s_nz += a != 0;
+                s_sq += dot * dot;
+            }
+        }
+    }
+    s_abs = __reduce_add_sync(0xffffffffu, s_abs);
+    s_nz = __reduce_add_sync(0xffffffffu, s_nz);
+    s_sq = __reduce_add_sync(0xffffffffu, s_sq);
+    diag_ok = (int)__reduce_and_sync(0xffffffffu, (unsigned)diag_ok);
+    if (lane == 0) stats[warp] = make_int4(s_abs / 2, s_nz / 2, s_sq / 2, (s_nz == 0 && diag_ok) ? 1 : 0);
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+    static std::once_flag once;
+    static EncodeTiledFn fn = nullptr;
+    std::call_once(once, []() {
+        void* ptr = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(ptr);
+    });
+    return fn;
+}
+
+int32_t rfail(int32_t code, const std::string& msg) {
+    set_last_error(msg);
+    return code;
+}
+
+// timed-out-wait flag of the rescoring kernel (one int per device)
+static __device__ int g_rescore_error;
+
+int* error_flag_ptr() {
+    static std::mutex mu;
+    static int* ptr[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!ptr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_rescore_error) != cudaSuccess) return nullptr;
+        ptr[dev] = static_cast<int*>(p);
+    }
+    return ptr[dev];
+}
+
+}  // namespace
+
+// Enqueue the rescoring of `count` row-major n x n matrices at W (device).
+int32_t rescore_device(const int8_t* W, int64_t count, int n, int w, int32_t* stats, int32_t* gram,
+                       cudaStream_t stream, int* err_flag, bool force_simt) {
+    if (count < 0 || count > INT32_MAX / 4) return rfail(XW_ERR_INVALID, "rescore: count out of range");
+    if (n < 1 || n > XW_MAX_ORDER_CUDA) return rfail(XW_ERR_INVALID, "rescore: order must be in [1, 128]");
+    if (count == 0) return XW_OK;
+    cudaError_t e;
+    const bool tc = !force_simt && n % 32 == 0 && ((uintptr_t)W % 16) == 0;
+    if (!tc) {
+        const int blocks = (int)((count * 32 + 255) / 256);
+        rescore_simt_kernel<<<blocks, 256, 0, stream>>>(W, (int)count, n, w, reinterpret_cast<int4*>(stats), gram);
+        e = cudaGetLastError();
+        return e == cudaSuccess ? XW_OK : rfail(XW_ERR_CUDA, std::string("rescore launch: ") + cudaGetErrorString(e));
+    }
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) return rfail(XW_ERR_CUDA, "rescore: cuTensorMapEncodeTiled is unavailable");
+    RescoreParams p;
+    p.count = (int)count;
+    p.n = n;
+    p.w = w;
+    p.mpt = n <= 64 ? 128 / n : 1;
+    p.rows_per_tile = p.mpt * n;
+    p.ntiles = (int)((count + p.mpt - 1) / p.mpt);
+    p.stats = reinterpret_cast<int4*>(stats);
+    p.gram = gram;
+    p.error = err_flag;
+    CUtensorMap map;
+    const cuuint64_t dims[2] = {(cuuint64_t)n, (cuuint64_t)count * n};
+    const cuuint64_t strides[1] = {(cuuint64_t)n};
+    const cuuint32_t box[2] = {128u, (cuuint32_t)p.rows_per_tile};
+    const cuuint32_t estr[2] = {1u, 1u};
+    const CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t*>(W), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return rfail(XW_ERR_CUDA, "rescore: cuTensorMapEncodeTiled failed");
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t smem = (size_t)kStages * kTileBytes + 1024;
+    e = cudaFuncSetAttribute(rescore_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return rfail(XW_ERR_CUDA, std::string("rescore attribute: ") + cudaGetErrorString(e));
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rescore_tc_kernel, 128, smem);
+    per_sm = per_sm < 1 ? 1 : (per_sm > 3 ? 3 : per_sm);   // TMEM: 128 columns per CTA
+    const int blocks = (int)std::min<int64_t>(p.ntiles, (int64_t)per_sm * sms);
+    rescore_tc_kernel<<<blocks, 128, smem, stream>>>(map, p);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? XW_OK : rfail(XW_ERR_CUDA, std::string("rescore launch: ") + cudaGetErrorString(e));
+}
+
+}  // namespace xw
+
+using namespace xw;
+
+extern "C" int32_t xw_rescore_device(const int8_t* W, int64_t count, int32_t n, int32_t w, int32_t* stats,
+                                     int32_t* gram, int32_t simt, void* stream) {
+    if (!W || !stats) return rfail(XW_ERR_INVALID, "rescore: null argument");
+    int* flag = error_flag_ptr();
+    if (!flag) return rfail(XW_ERR_CUDA, "rescore: cannot resolve the error flag");
+    return rescore_device(W, count, n, w, stats, gram, static_cast<cudaStream_t>(stream), flag, simt != 0);
+}
+
+extern "C" int32_t xw_rescore_status(void) {
+    int* flag = error_flag_ptr();
+    if (!flag) return rfail(XW_ERR_CUDA, "rescore: cannot resolve the error flag");
+    int v = 0;
+    if (cudaMemcpy(&v, flag, sizeof v, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return rfail(XW_ERR_CUDA, "rescore: cannot read the error flag");
+    if (v == 0) return XW_OK;
+    const int zero = 0;
+    cudaMemcpy(flag, &zero, sizeof zero, cudaMemcpyHostToDevice);
+    return rfail(XW_ERR_TIMEOUT, "rescore: a pipeline wait expired (code " + std::to_string(v) + ")");
+}
+
+extern "C" int32_t xw_rescore(const int8_t* W, int64_t count, int32_t n, int32_t w, int32_t* stats, int32_t* gram) {
+    if (!W || !stats || count < 0 || n < 1 || n > XW_MAX_ORDER_CUDA) return rfail(XW_ERR_INVALID, "rescore: bad arguments");
+    if (count == 0) return XW_OK;
+    const size_t in_bytes = (size_t)count * n * n, st_bytes = (size_t)count * 16,
+                 g_bytes = gram ? (size_t)count * n * n * 4 : 0;
+    int8_t* dW = nullptr;
+    int32_t *dS = nullptr, *dG = nullptr;
+    auto cleanup = [&]() {
+        if (dW) cudaFree(dW);
+        if (dS) cudaFree(dS);
+        if (dG) cudaFree(dG);
+    };
+    if (cudaMalloc(&dW, in_bytes) != cudaSuccess || cudaMalloc(&dS, st_bytes) != cudaSuccess ||
+        (gram && cudaMalloc(&dG, g_bytes) != cudaSuccess)) {
+        cleanup();
+        return rfail(XW_ERR_CAPACITY, "rescore: device allocation failed");
+    }
+    int32_t rc = XW_OK;
+    if (cudaMemcpy(dW, W, in_bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = rfail(XW_ERR_CUDA, "rescore: copy to device failed");
+    if (rc == XW_OK) rc = xw_rescore_device(dW, count, n, w, dS, dG, 0, nullptr);
+    if (rc == XW_OK && cudaDeviceSynchronize() != cudaSuccess) rc = rfail(XW_ERR_CUDA, "rescore: kernel failed");
+    if (rc == XW_OK) rc = xw_rescore_status();
+    if (rc == XW_OK && cudaMemcpy(stats, dS, st_bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = rfail(XW_ERR_CUDA, "rescore: copy to host failed");
+    if (rc == XW_OK && gram && cudaMemcpy(gram, dG, g_bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = rfail(XW_ERR_CUDA, "rescore: copy to host failed");
+    cleanup();
+    return rc;
+}
