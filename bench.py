@@ -170,7 +170,24 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- ours
+def reduce_over_ranks(world, device, max_vals, sum_vals):
+    """(max over ranks of max_vals, sum over ranks of sum_vals): the whole-job
+    time is the slowest rank's, the work is every rank's.  Every rank calls
+    it at the same point; world 1 needs no process group."""
+    if world == 1:
+        return list(max_vals), list(sum_vals)
+    import torch
+    import torch.distributed as dist
+    mx = torch.tensor(list(max_vals), dtype=torch.float64, device=device)
+    sm = torch.tensor(list(sum_vals), dtype=torch.float64, device=device)
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    return mx.tolist(), sm.tolist()
+
+
 def make_jobs(rank):
+    """Rank r's shard: its own INSTANCES searches, seeds disjoint across ranks
+    (independent searches, so no data crosses GPUs)."""
     return [{"n": N_ORDER, "w": W_WEIGHT, "seed": 1 + rank * INSTANCES + i, "replicas": RUNGS}
             for i in range(INSTANCES)]
 
@@ -257,13 +274,7 @@ def ours(args):
     torch.cuda.synchronize()
     barrier()
     total_ms = sum(step_ms)
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([total_ms, float(moves), float(evals)], device="cuda", dtype=torch.float64)
-        mx = t.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        total_ms, moves, evals = mx[0].item(), t[1].item(), t[2].item()
+    (total_ms,), (moves, evals) = reduce_over_ranks(world, "cuda", [total_ms], [float(moves), float(evals)])
     value = moves / (total_ms / 1e3)
 
     # end to end: the C ABI whole-batch call with host buffers
@@ -285,13 +296,7 @@ def ours(args):
             e2e_moves += sum(r.moves for r in res)
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
-        if world > 1:
-            import torch.distributed as dist
-            t = torch.tensor([e2e_s, float(e2e_moves)], device="cuda", dtype=torch.float64)
-            mx = t.clone()
-            dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-            dist.all_reduce(t, op=dist.ReduceOp.SUM)
-            e2e_s, e2e_moves = mx[0].item(), t[1].item()
+        (e2e_s,), (e2e_moves,) = reduce_over_ranks(world, "cuda", [e2e_s], [float(e2e_moves)])
         e2e_value = e2e_moves / e2e_s
 
     clocks = clk.summary()
@@ -340,16 +345,227 @@ def ours(args):
                                     "sample_seconds": args.plain_seconds}
         except Exception as e:  # noqa: BLE001 - report, do not fail the bench
             line["plain_kernel"] = {"unavailable": str(e)[:200]}
+    if args.rescore:
+        line["rescore"] = rescore_bench(torch, X)
+    if args.uneven_iters > 0:
+        line["uneven"] = uneven_bench(X, args.uneven_iters)
+    if args.serve_requests > 0:
+        line["serving"] = serving_bench(X, args.serve_requests, args.serve_plain, args.serve_quantum)
     print(json.dumps(line), flush=True)
 
 
+REF_HARNESS = os.path.join(REPO, "oracle", "_ref", "ref_harness")
+
+
+def rescore_bench(torch, X):
+    """Batched exact W W^T (tcgen05 kind::i8): 65536 fixed-degree ternary
+    matrices per order n in {32, 64, 96, 128}, w = n/2, resident in HBM.
+    HBM-bound: n^2 bytes in and 16 bytes out per matrix."""
+    import ctypes as C
+    peaks = {}
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except (OSError, ValueError):
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    out = {"matrices_per_order": 65536, "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6.65 TB/s",
+           "orders": {}}
+    count = 65536
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    for n in (32, 64, 96, 128):
+        w = n // 2
+        gen = torch.Generator(device="cuda").manual_seed(n)
+        W = torch.zeros((count, n, n), dtype=torch.int8, device="cuda")
+        for c0 in range(0, count, 4096):
+            keys = torch.rand((4096, n, n), device="cuda", generator=gen)
+            idx = keys.argsort(dim=2)[:, :, :w]
+            signs = (torch.randint(0, 2, (4096, n, w), device="cuda", generator=gen) * 2 - 1).to(torch.int8)
+            W[c0:c0 + 4096].scatter_(2, idx, signs)
+            del keys, idx, signs
+        stats = torch.zeros((count, 4), dtype=torch.int32, device="cuda")
+
+        def launch():
+            rc = X.lib().xw_rescore_device(C.c_void_p(W.data_ptr()), count, n, w, C.c_void_p(stats.data_ptr()),
+                                           None, 0, C.c_void_p(stream.cuda_stream))
+            if rc != X.XW_OK:
+                raise RuntimeError(X.lib().xw_last_error().decode())
+
+        for _ in range(3):
+            launch()
+        torch.cuda.synchronize()
+        times = []
+        for _ in range(10):
+            flush.fill_(1)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            launch()
+            b.record(stream)
+            b.synchronize()
+            times.append(a.elapsed_time(b))
+        if X.lib().xw_rescore_status() != X.XW_OK:
+            raise RuntimeError("rescore pipeline wait expired")
+        ms = statistics.median(times)
+        alg_bytes = count * (n * n + 16)
+        gbs = alg_bytes / (ms / 1e3) / 1e9
+        entry = {"ms": ms, "matrices_per_sec": count / (ms / 1e3),
+                 "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                              "algorithmic_bytes": alg_bytes},
+                 "tensor_ops": 2 * n ** 3 * count}
+        if os.path.exists(REF_HARNESS):
+            threads = os.cpu_count() or 1
+            sample = 16384 if n <= 64 else 4096
+            r = subprocess.run([REF_HARNESS, "rescore_bench", str(n), str(w), str(sample), str(threads)],
+                               capture_output=True, text=True, timeout=600)
+            try:
+                ref = json.loads(r.stdout.strip().splitlines()[-1])
+                entry["cpu_baseline"] = {"value": ref["matrices_per_sec"], "unit": "matrices/s", "cores": threads,
+                                         "kind": "reference",
+                                         "sample": f"{sample} matrices: State::from_entries + verify_weighing"}
+            except (ValueError, IndexError, KeyError):
+                pass
+        out["orders"][str(n)] = entry
+        del W, stats
+    return out
+
+
+# ---------------------------------------------------------------- uneven batch (C3)
+UNEVEN = ((14, 13), (18, 17), (20, 19), (24, 23), (30, 29))
+UNEVEN_INSTANCES, UNEVEN_RUNGS = 64, 16
+
+
+def uneven_bench(X, iters):
+    """1024 replicas each of W(14,13), W(18,17), W(20,19), W(24,23) and
+    W(30,29) (64 instances x 16-rung tempering ladder per order) in one
+    persistent launch per round, at the autotuned warps per CTA, against
+    the same searches run as five launches, one order at a time."""
+    import numpy as np
+    p = X.Params(tempering=1, exchange_interval=EXCHANGE, t_min=T_MIN, t_init=T_MAX,
+                 squared_objective_fraction=0.0, parity_objective_fraction=0.0, stop_on_solve=0)
+    jobs = [{"n": n, "w": w, "seed": 7000 + 100 * i + k, "replicas": UNEVEN_RUNGS}
+            for i, (n, w) in enumerate(UNEVEN) for k in range(UNEVEN_INSTANCES)]
+    wpb, tune_ms = X.autotune(jobs, p, iters=2000)
+
+    def timed(js, steps=3):
+        b = X.Batch(js, p)
+        b.reset()
+        b.run(iters)           # warm-up (builds the CUDA graph)
+        b.synchronize()
+        ms = []
+        for _ in range(steps):
+            b.reset()
+            b.run(iters)
+            b.synchronize()
+            ms.append(sum(b.launch_times()))
+        moves = sum(r.moves for r, _ in b.results())
+        shape = b.shape()
+        b.close()
+        return moves, float(np.median(ms)), shape
+
+    moves, ms, shape = timed(jobs)
+    out = {"workload": f"{len(UNEVEN)} orders x {UNEVEN_INSTANCES} instances x {UNEVEN_RUNGS}-rung ladder "
+                       f"T {T_MIN}..{T_MAX}, exchange every {EXCHANGE}, {iters} iterations per replica",
+           "autotuned_warps_per_block": wpb, "autotune_trial_ms": tune_ms, "launch_shape": list(shape),
+           "batched": {"moves": moves, "ms": ms, "moves_per_sec": moves / (ms / 1e3)}}
+    pm = pms = 0.0
+    for (n, w) in UNEVEN:
+        m, t, _ = timed([j for j in jobs if j["n"] == n], steps=1)
+        pm += m
+        pms += t
+    out["one_order_per_launch"] = {"moves": pm, "ms": pms, "moves_per_sec": pm / (pms / 1e3)}
+    return out
+
+
+# ---------------------------------------------------------------- serving (C5)
+SERVE_ORDERS = (12, 14, 18, 20, 24, 26, 30)
+SERVE_RATE = 200.0
+SERVE_REPLICAS = 256
+SERVE_BUDGET = 10 ** 8
+
+
+def serving_stream(count, seed=5):
+    """The mixed request stream: Poisson arrivals at 200 requests/s (seeded
+    exponential gaps); 70% W(n, n-1) with n uniform in SERVE_ORDERS, 30%
+    W(n, 4) with n uniform in 16..64; request k has seed 1000 + k."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out, t = [], 0.0
+    for k in range(count):
+        t += rng.exponential(1.0 / SERVE_RATE)
+        if rng.random() < 0.7:
+            n = int(rng.choice(SERVE_ORDERS))
+            w = n - 1
+        else:
+            n, w = int(rng.integers(16, 65)), 4
+        out.append((t, n, w, 1000 + k))
+    return out
+
+
+def serve_stream(X, reqs, **cfg):
+    """Submit `reqs` at their arrival times to a server, wait for all, and
+    summarise time-to-exact (submission to first exact solution) and moves/s.
+    Requests answered by Sylvester blocks (w a power of two dividing n) are
+    counted apart and left out of both figures."""
+    import numpy as np
+    with X.Server(**cfg) as srv:
+        t0 = time.perf_counter()
+        ids = []
+        for (ta, n, w, seed) in reqs:
+            d = ta - (time.perf_counter() - t0)
+            if d > 0:
+                time.sleep(d)
+            ids.append(srv.submit(n, w, seed, replicas=SERVE_REPLICAS, max_moves=SERVE_BUDGET))
+        res = [srv.wait(i)[0] for i in ids]
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+    searched = [r for r in res if not r.sylvester]
+    solved = [r for r in searched if r.solved]
+    tte = np.array([r.time_to_solution_seconds for r in solved]) if solved else np.array([-1.0])
+    moves = sum(r.moves for r in searched)
+    failed = [r for r in res if r.state != X.REQ_DONE]
+    return {
+        "requests": len(reqs), "searched": len(searched), "sylvester": len(res) - len(searched),
+        "solved": len(solved), "censored_at_budget": len(searched) - len(solved), "failed": len(failed),
+        "all_solutions_verified": all(r.verified for r in solved),
+        "time_to_exact_s": {"p50": float(np.percentile(tte, 50)), "p99": float(np.percentile(tte, 99)),
+                            "mean": float(tte.mean())},
+        "moves": moves, "wall_s": wall, "moves_per_sec": moves / wall,
+        "device_s": st.device_seconds, "rounds": st.rounds,
+        "config": {"quantum_iters": st.quantum_iters, "schedule": ["all", "least_attained"][st.schedule],
+                   "max_active_replicas": st.max_active_replicas,
+                   "max_resident_replicas": st.max_resident_replicas},
+    }
+
+
+def serving_bench(X, count, plain_count, quantum):
+    """The serving workload: the request stream through the continuous-
+    batching server, and its first `plain_count` requests both served and
+    one request at a time (resident cap of one request: the plain
+    one-instance-per-launch mode), same kernel and budgets."""
+    reqs = serving_stream(count)
+    out = {"workload": f"{count} requests, Poisson {SERVE_RATE:g}/s; 70% W(n,n-1) n in {list(SERVE_ORDERS)}, "
+                       f"30% W(n,4) n in 16..64; {SERVE_REPLICAS} replicas and a {SERVE_BUDGET:.0e}-move budget "
+                       f"per request; time-to-exact from submission, Sylvester short-circuits excluded",
+           "served": serve_stream(X, reqs, quantum_iters=quantum)}
+    if plain_count > 0:
+        pre = reqs[:plain_count]
+        out["prefix_requests"] = len(pre)
+        out["served_prefix"] = serve_stream(X, pre, quantum_iters=quantum)
+        out["plain_prefix"] = serve_stream(X, pre, quantum_iters=quantum, schedule=X.SCHED_ALL,
+                                           max_resident_replicas=SERVE_REPLICAS)
+    return out
+
+
 def load_profile_traffic():
-    """DRAM bytes per anneal launch from the committed ncu summary, if any."""
-    path = os.path.join(REPO, "profiles", "anneal_kernel_traffic.json")
+    """DRAM bytes (read + write) per anneal launch from the committed ncu
+    summary of this workload, if any."""
+    path = os.path.join(REPO, "profiles", "anneal_kernel_w26_tempering.md")
     try:
         with open(path) as f:
-            return json.load(f).get("dram_bytes_per_launch")
-    except (OSError, ValueError):
+            m = re.search(r"traffic_bytes_per_launch\s*=\s*(\d+)", f.read())
+        return int(m.group(1)) if m else None
+    except OSError:
         return None
 
 
@@ -364,6 +580,13 @@ def main():
     ap.add_argument("--plain-seconds", type=float, default=10.0)
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--iters", type=int, default=ITERS, help="iterations per replica per step (profiling cases)")
+    ap.add_argument("--rescore", type=int, default=1, help="also time the batched tensor-core rescoring")
+    ap.add_argument("--uneven-iters", type=int, default=20000,
+                    help="iterations per replica of the uneven-orders batch (0: none)")
+    ap.add_argument("--serve-requests", type=int, default=400, help="requests of the serving stream (0: none)")
+    ap.add_argument("--serve-plain", type=int, default=60,
+                    help="prefix of the stream also run one request at a time")
+    ap.add_argument("--serve-quantum", type=int, default=1000, help="iterations per replica per server round")
     args = ap.parse_args()
     if args.warmup < 3:
         log("[bench] warmup raised to 3")

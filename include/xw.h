@@ -71,7 +71,9 @@ typedef struct xw_params {
     int32_t objective;            /* -1 reference per-replica mix, 0 L1, 1 squared, 2 parity */
     int32_t move_set;             /* 0 flip/switch/double flip, 1 flip/within-row swap */
     int32_t start_kind;           /* 0 regular random start, 1 row-only random start */
-    int32_t stop_on_solve;        /* 1: stop every replica once one solves */
+    int32_t stop_on_solve;        /* 1: stop every replica once one solves; 2: a replica stops at
+                                     its own solve and the others finish the launch, so that
+                                     results do not depend on launch timing */
     int32_t warps_per_block;      /* 0 = autotuned */
     int32_t reserved;
 } xw_params;
@@ -232,6 +234,16 @@ int32_t xw_batch_bytes(xw_batch* b, uint64_t* h2d, uint64_t* d2h);
 int32_t xw_batch_shape(xw_batch* b, int32_t* warps_per_block, int32_t* blocks, int32_t* slot_bytes);
 void xw_batch_destroy(xw_batch* b);
 
+/* Launch-shape autotuner (the tunable is warps per CTA; each replica is one
+ * warp): builds the batch, times `iters` iterations per replica at 1, 2, 4,
+ * 8 and 16 warps per CTA (those that fit shared memory), records the fastest
+ * for the batch's rows-per-lane class and shared-memory slot size in the
+ * tuning cache (XW_TUNE_CACHE, default ~/.cache/xw_tune.txt), which later
+ * batches and servers with warps_per_block = 0 use.  best_ms (nullable)
+ * receives the winner's device milliseconds. */
+int32_t xw_autotune(const xw_job_spec* jobs, int32_t njobs, const xw_params* p, uint64_t iters,
+                    int32_t* best_wpb, float* best_ms);
+
 /* Whole batched search through host buffers: upload, run until every job
  * is solved or out of budget (or `iters` per replica when nonzero), read
  * back.  The end-to-end call of the served-batch benchmark. */
@@ -258,6 +270,132 @@ int32_t xw_rescore_device(const int8_t* W_rowmajor, int64_t count, int32_t n, in
 /* XW_OK, or XW_ERR_TIMEOUT when a rescoring pipeline wait expired since the
  * last call (the flag is cleared).  Synchronous. */
 int32_t xw_rescore_status(void);
+
+/* ---- serving: continuous batching of search requests ------------------ */
+/* The reference serves one search per process: xweigh_cuda_main.cpp:281-285
+ * calls run_annealer (xweigh_cuda.cu:1419-2436), which allocates, anneals
+ * and frees one population.  A server instead keeps one device's
+ * population resident and admits requests while earlier ones run.  Each
+ * request is one W(n,w) search (an xw_job_spec with its own parameters):
+ * host worker threads build its start states and records; the engine
+ * thread admits it when its replicas fit the resident cap and its records
+ * fit the device arena (first come, first served), and every engine round
+ * advances resident requests by `quantum_iters` iterations per replica:
+ * all of them, or (the default) those with the least attained iterations,
+ * so that requests that solve early are not queued behind long searches.
+ * A request ends at the end of the round in which its first replica solved,
+ * its move budget or time limit ran out, or it was cancelled.
+ *
+ * Replicas of a served request stop at their own solve (stop_on_solve 2)
+ * and run rounds of a fixed length from the request's own start, so the
+ * first solution, its iteration, the best W and the move counts of a
+ * request are the same whether it ran alone or among other requests; only
+ * times differ.  Thread safety: any thread may submit, poll, wait, cancel
+ * and read stats concurrently. */
+#define XW_REQ_QUEUED 0    /* accepted, not yet on the device */
+#define XW_REQ_RUNNING 1   /* resident on the device */
+#define XW_REQ_DONE 2      /* solved, out of budget or out of time */
+#define XW_REQ_CANCELLED 3
+#define XW_REQ_FAILED 4    /* see status and error */
+
+typedef struct xw_server_config {
+    int32_t device;
+    int32_t quantum_iters;         /* iterations per replica per engine round (default 1000) */
+    int32_t max_requests;          /* resident requests (job slots, default 1024) */
+    int32_t max_resident_replicas; /* admission cap on resident replicas (0 = the replica id
+                                      space) */
+    int32_t max_replica_ids;       /* replica id space (default 262144) */
+    int32_t warps_per_block;       /* 0 = tuned */
+    int32_t prep_threads;          /* host threads building start states (0 = half the cores) */
+    int32_t sylvester_shortcut;    /* 1: a power-of-two w dividing n is answered by Sylvester
+                                      blocks without search (xweigh_cuda_main.cpp:270-277) */
+    uint64_t arena_bytes;          /* device bytes for resident replica records (default 1 GiB) */
+    int32_t schedule;              /* XW_SCHED_ALL: every resident request advances every round;
+                                      XW_SCHED_LEAST_ATTAINED (default): each round advances the
+                                      requests with the fewest iterations so far, oldest first,
+                                      up to max_active_replicas */
+    int32_t max_active_replicas;   /* replicas advanced per round under XW_SCHED_LEAST_ATTAINED
+                                      (0 = two waves of the device's resident warps) */
+    int32_t reserved[6];
+} xw_server_config;
+
+#define XW_SCHED_ALL 0
+#define XW_SCHED_LEAST_ATTAINED 1
+
+typedef struct xw_request {
+    int32_t n, w;
+    uint64_t seed;                 /* Philox key and start seeds, as xw_job_spec */
+    int32_t replicas;
+    int32_t reserved;
+    uint64_t max_moves;            /* total move budget, 0 = params->max_moves (0 = none) */
+    const xw_params* params;       /* nullable: xw_params_default; device, replicas,
+                                      moves_per_launch and stop_on_solve are the server's;
+                                      max_seconds limits the request's time on the device */
+    const int8_t* starts;          /* nullable: replicas*n*n column-major start states */
+} xw_request;
+
+typedef struct xw_request_result {
+    int32_t state;                 /* XW_REQ_* */
+    int32_t status;                /* XW_OK, or the failure's code */
+    int32_t n, w;
+    int32_t replicas;
+    int32_t solved;                /* a replica reached score 0 */
+    int32_t verified;              /* the returned W satisfies W W^T = wI (int64 check) */
+    int32_t sylvester;             /* answered without search */
+    int32_t best_replica;          /* the first solver, else least (score, conflicts, index) */
+    int32_t reserved;
+    int64_t score, conflicts;      /* of the returned W */
+    uint64_t moves;
+    uint64_t candidate_evaluations;
+    uint64_t iterations;           /* per replica, max over replicas */
+    uint64_t solved_iteration;     /* the first solver's solve iteration */
+    double submit_seconds;         /* server clock (seconds since creation) */
+    double admit_seconds;          /* -1 until resident */
+    double finish_seconds;         /* -1 until finished */
+    double time_to_solution_seconds; /* submit -> first exact solution (device clock), -1 if none */
+    double t_init;                 /* initial temperature used */
+    char error[192];
+} xw_request_result;
+
+typedef struct xw_server_stats {
+    uint64_t submitted, admitted, finished, solved, cancelled, failed, sylvester;
+    uint64_t queued, running;      /* now */
+    uint64_t resident_replicas;    /* now */
+    uint64_t rounds;               /* engine rounds run */
+    uint64_t moves;                /* moves of finished requests */
+    double device_seconds;         /* device time of all rounds */
+    double busy_seconds;           /* engine wall time with requests resident */
+    uint64_t arena_bytes, arena_bytes_used;
+    int32_t quantum_iters, max_resident_replicas;
+    int32_t schedule, max_active_replicas;
+} xw_server_stats;
+
+typedef struct xw_server xw_server;
+
+void xw_server_config_default(xw_server_config* c);
+/* Allocates the device arena and tables and starts the engine and worker
+ * threads. */
+int32_t xw_server_create(const xw_server_config* c, xw_server** out);
+/* Queue a request.  Fails at once (XW_ERR_INVALID with the reference's
+ * validation or impossibility message, XW_ERR_CAPACITY when it can never
+ * fit) instead of failing later. */
+int32_t xw_submit(xw_server* s, const xw_request* r, uint64_t* id);
+/* Current state of a request; best (nullable, n*n column-major) receives
+ * the returned W once the request has finished. */
+int32_t xw_poll(xw_server* s, uint64_t id, xw_request_result* res, int8_t* best_colmajor);
+/* Wait until the request finishes or timeout_seconds pass (< 0: no limit);
+ * XW_ERR_TIMEOUT when it is still unfinished. */
+int32_t xw_wait(xw_server* s, uint64_t id, double timeout_seconds, xw_request_result* res,
+                int8_t* best_colmajor);
+/* Cancel: a queued request ends at once, a resident one at the end of the
+ * current round with its best W so far.  No effect on finished requests. */
+int32_t xw_cancel(xw_server* s, uint64_t id);
+/* Forget a finished request (its result and W). */
+int32_t xw_release(xw_server* s, uint64_t id);
+int32_t xw_server_get_stats(xw_server* s, xw_server_stats* out);
+/* Stops the threads (unfinished requests end cancelled) and frees the
+ * device memory. */
+void xw_server_destroy(xw_server* s);
 
 /* ---- annealing without device allocation ------------------------------ */
 /* No counterpart in the reference: an entry point for callers that cannot

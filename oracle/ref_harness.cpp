@@ -307,6 +307,41 @@ int cmd_calibrate(int n, int w, uint32_t seed) {
     return 0;
 }
 
+// Throughput of the reference's full rescoring + exact verification
+// (State::from_entries -> rebuild_gram_and_residual, then verify_weighing)
+// over `count` random row-regular ternary matrices on `threads` threads.
+int cmd_rescore_bench(int n, int w, int count, int threads) {
+    std::vector<std::vector<int8_t>> mats((size_t)count);
+    std::mt19937 rng(12345u + (uint32_t)n);
+    for (auto& e : mats) {
+        e.assign((size_t)n * n, 0);
+        std::vector<int> cols((size_t)n);
+        for (int r = 0; r < n; ++r) {
+            for (int c = 0; c < n; ++c) cols[c] = c;
+            std::shuffle(cols.begin(), cols.end(), rng);
+            for (int k = 0; k < w; ++k) e[(size_t)cols[k] * n + r] = (rng() & 1u) ? 1 : -1;
+        }
+    }
+    std::atomic<long long> checksum{0};
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t)
+        pool.emplace_back([&, t]() {
+            long long local = 0;
+            for (int i = t; i < count; i += threads) {
+                xweigh::State s = xweigh::State::from_entries(n, w, mats[(size_t)i]);
+                local += s.score() + (s.verify_weighing() ? 1 : 0);
+            }
+            checksum += local;
+        });
+    for (auto& th : pool) th.join();
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    std::printf("{\"cmd\":\"rescore_bench\",\"n\":%d,\"w\":%d,\"count\":%d,\"threads\":%d,\"seconds\":%.6f,"
+                "\"matrices_per_sec\":%.3f,\"checksum\":%lld}\n",
+                n, w, count, threads, secs, count / secs, (long long)checksum.load());
+    return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -325,6 +360,8 @@ int main(int argc, char** argv) {
     if (cmd == "csv" && argc == 5) return cmd_csv((int)I(2), (int)I(3), argv[4]);
     if (cmd == "sylvester" && argc == 4) return cmd_sylvester((int)I(2), (int)I(3));
     if (cmd == "calibrate" && argc == 5) return cmd_calibrate((int)I(2), (int)I(3), (uint32_t)I(4));
+    if (cmd == "rescore_bench" && argc == 6)
+        return cmd_rescore_bench((int)I(2), (int)I(3), (int)I(4), (int)I(5));
     std::fprintf(stderr, "bad command\n");
     return 2;
 }

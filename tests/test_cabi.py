@@ -149,3 +149,38 @@ def test_calibration_matches_reference():
             assert t == case["t"]
         else:
             assert t > 0
+
+
+def test_ctypes_structs_match_the_c_header(tmp_path):
+    # every struct the Python side passes through the ABI has the C layout
+    import ctypes as C
+    import subprocess
+    structs = {"xw_params": X._Params, "xw_device_info": X._DeviceInfo, "xw_result": X._Result,
+               "xw_job_spec": X.JobSpec, "xw_job_result": X.JobResult, "xw_replica_state": X.ReplicaState,
+               "xw_server_config": X.ServerConfig, "xw_request": X._Request,
+               "xw_request_result": X.RequestResult, "xw_server_stats": X.ServerStats}
+    src = tmp_path / "sizes.c"
+    src.write_text('#include <stdio.h>\n#include "xw.h"\nint main(void) {\n' +
+                   "".join(f'    printf("%zu\\n", sizeof({k}));\n' for k in structs) + "    return 0;\n}\n")
+    exe = tmp_path / "sizes"
+    subprocess.run(["gcc", "-I", os.path.dirname(X.HEADER), "-o", str(exe), str(src)], check=True)
+    sizes = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert sizes == [C.sizeof(t) for t in structs.values()]
+
+
+def test_server_config_defaults():
+    import ctypes as C
+    cfg = X.ServerConfig()
+    X.lib().xw_server_config_default(C.byref(cfg))
+    assert (cfg.quantum_iters, cfg.max_requests, cfg.max_replica_ids, cfg.sylvester_shortcut) == (1000, 1024, 262144, 1)
+    assert cfg.arena_bytes == 1 << 30
+
+
+def test_server_create_rejects_bad_config_without_a_device():
+    # validation happens before any CUDA call
+    with pytest.raises(X.XwError) as e:
+        X.Server(quantum_iters=0)
+    assert e.value.code == X.XW_ERR_INVALID
+    with pytest.raises(X.XwError) as e:
+        X.Server(warps_per_block=17)
+    assert e.value.code == X.XW_ERR_INVALID

@@ -93,6 +93,49 @@ class ReplicaState(C.Structure):
                 ("error", C.c_uint32)]
 
 
+class ServerConfig(C.Structure):
+    """xw_server_config: the serving loop's device, round length and capacities."""
+    _fields_ = [("device", C.c_int32), ("quantum_iters", C.c_int32), ("max_requests", C.c_int32),
+                ("max_resident_replicas", C.c_int32), ("max_replica_ids", C.c_int32),
+                ("warps_per_block", C.c_int32), ("prep_threads", C.c_int32),
+                ("sylvester_shortcut", C.c_int32), ("arena_bytes", C.c_uint64),
+                ("schedule", C.c_int32), ("max_active_replicas", C.c_int32),
+                ("reserved", C.c_int32 * 6)]
+
+
+class _Request(C.Structure):
+    _fields_ = [("n", C.c_int32), ("w", C.c_int32), ("seed", C.c_uint64), ("replicas", C.c_int32),
+                ("reserved", C.c_int32), ("max_moves", C.c_uint64), ("params", C.POINTER(_Params)),
+                ("starts", C.POINTER(C.c_int8))]
+
+
+class RequestResult(C.Structure):
+    """xw_request_result: state, outcome and timing of one served request."""
+    _fields_ = [("state", C.c_int32), ("status", C.c_int32), ("n", C.c_int32), ("w", C.c_int32),
+                ("replicas", C.c_int32), ("solved", C.c_int32), ("verified", C.c_int32),
+                ("sylvester", C.c_int32), ("best_replica", C.c_int32), ("reserved", C.c_int32),
+                ("score", C.c_int64), ("conflicts", C.c_int64), ("moves", C.c_uint64),
+                ("candidate_evaluations", C.c_uint64), ("iterations", C.c_uint64),
+                ("solved_iteration", C.c_uint64), ("submit_seconds", C.c_double),
+                ("admit_seconds", C.c_double), ("finish_seconds", C.c_double),
+                ("time_to_solution_seconds", C.c_double), ("t_init", C.c_double),
+                ("error", C.c_char * 192)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("admitted", C.c_uint64), ("finished", C.c_uint64),
+                ("solved", C.c_uint64), ("cancelled", C.c_uint64), ("failed", C.c_uint64),
+                ("sylvester", C.c_uint64), ("queued", C.c_uint64), ("running", C.c_uint64),
+                ("resident_replicas", C.c_uint64), ("rounds", C.c_uint64), ("moves", C.c_uint64),
+                ("device_seconds", C.c_double), ("busy_seconds", C.c_double),
+                ("arena_bytes", C.c_uint64), ("arena_bytes_used", C.c_uint64),
+                ("quantum_iters", C.c_int32), ("max_resident_replicas", C.c_int32),
+                ("schedule", C.c_int32), ("max_active_replicas", C.c_int32)]
+
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_CANCELLED, REQ_FAILED = 0, 1, 2, 3, 4
+SCHED_ALL, SCHED_LEAST_ATTAINED = 0, 1
+
 LOG_FN = C.CFUNCTYPE(None, C.c_char_p, C.c_void_p)
 CHECKPOINT_FN = C.CFUNCTYPE(None, C.POINTER(C.c_int8), C.c_int32, C.c_void_p)
 
@@ -146,6 +189,16 @@ def lib():
             "xw_rescore_device": (i32, [C.c_void_p, C.c_int64, i32, i32, C.c_void_p, C.c_void_p, i32,
                                         C.c_void_p]),
             "xw_rescore_status": (i32, []),
+            "xw_autotune": (i32, [P(JobSpec), i32, P(_Params), u64, P(i32), P(C.c_float)]),
+            "xw_server_config_default": (None, [P(ServerConfig)]),
+            "xw_server_create": (i32, [P(ServerConfig), P(C.c_void_p)]),
+            "xw_submit": (i32, [C.c_void_p, P(_Request), P(u64)]),
+            "xw_poll": (i32, [C.c_void_p, u64, P(RequestResult), P(i8)]),
+            "xw_wait": (i32, [C.c_void_p, u64, C.c_double, P(RequestResult), P(i8)]),
+            "xw_cancel": (i32, [C.c_void_p, u64]),
+            "xw_release": (i32, [C.c_void_p, u64]),
+            "xw_server_get_stats": (i32, [C.c_void_p, P(ServerStats)]),
+            "xw_server_destroy": (None, [C.c_void_p]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -444,18 +497,113 @@ class Batch:
         return st, W, B, M[: n * m]
 
 
-def batch_solve(jobs, params: Params, starts=None, iters=0):
-    """xw_batch_solve: upload, run, read back through host buffers."""
+def _specs(jobs):
     specs = (JobSpec * len(jobs))()
     for i, j in enumerate(jobs):
         specs[i].n, specs[i].w, specs[i].seed, specs[i].replicas = j["n"], j["w"], j.get("seed", 1), j["replicas"]
         specs[i].max_moves = j.get("max_moves", 0)
+    return specs
+
+
+def batch_solve(jobs, params: Params, starts=None, iters=0):
+    """xw_batch_solve: upload, run, read back through host buffers."""
+    specs = _specs(jobs)
     res = (JobResult * len(jobs))()
     best = np.zeros(sum(j["n"] * j["n"] for j in jobs), dtype=np.int8)
     st = None if starts is None else np.ascontiguousarray(starts, dtype=np.int8).reshape(-1)
     _check(lib().xw_batch_solve(specs, len(jobs), C.byref(params.to_c()),
                                 _i8(st) if st is not None else None, iters, res, _i8(best)))
     return list(res), best
+
+
+class Server:
+    """A continuous-batching request loop on one device (xw_server_*).
+
+    ``submit`` queues one W(n,w) search and returns its id; ``wait`` and
+    ``poll`` return ``(RequestResult, W)`` with W the column-major int8 best
+    matrix once the request has finished (else None)."""
+
+    def __init__(self, device=0, **config):
+        cfg = ServerConfig()
+        lib().xw_server_config_default(C.byref(cfg))
+        cfg.device = device
+        for k, v in config.items():
+            setattr(cfg, k, v)
+        h = C.c_void_p()
+        _check(lib().xw_server_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+        self._orders = {}
+
+    def submit(self, n, w, seed, replicas=256, max_moves=0, params: Optional[Params] = None, starts=None):
+        r = _Request()
+        r.n, r.w, r.seed, r.replicas, r.max_moves = n, w, seed, replicas, max_moves
+        pc = params.to_c() if params is not None else None
+        r.params = C.pointer(pc) if pc is not None else None
+        st = None
+        if starts is not None:
+            st = np.ascontiguousarray(starts, dtype=np.int8).reshape(-1)
+            if st.size != replicas * n * n:
+                raise ValueError("starts must hold replicas*n*n entries")
+            r.starts = _i8(st)
+        rid = C.c_uint64()
+        _check(lib().xw_submit(self.h, C.byref(r), C.byref(rid)))
+        self._orders[rid.value] = n
+        return rid.value
+
+    def _out(self, rid, res, W):
+        return res, (W if res.state >= REQ_DONE else None)
+
+    def poll(self, rid):
+        res = RequestResult()
+        n = self._orders.get(rid, MAX_ORDER_CUDA)
+        W = np.zeros(n * n, dtype=np.int8)
+        _check(lib().xw_poll(self.h, rid, C.byref(res), _i8(W)))
+        return self._out(rid, res, W)
+
+    def wait(self, rid, timeout=-1.0):
+        res = RequestResult()
+        n = self._orders.get(rid, MAX_ORDER_CUDA)
+        W = np.zeros(n * n, dtype=np.int8)
+        _check(lib().xw_wait(self.h, rid, float(timeout), C.byref(res), _i8(W)))
+        return self._out(rid, res, W)
+
+    def cancel(self, rid):
+        _check(lib().xw_cancel(self.h, rid))
+
+    def release(self, rid):
+        _check(lib().xw_release(self.h, rid))
+        self._orders.pop(rid, None)
+
+    def stats(self):
+        st = ServerStats()
+        _check(lib().xw_server_get_stats(self.h, C.byref(st)))
+        return st
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().xw_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass
+
+
+def autotune(jobs, params: Params, iters=2000):
+    """xw_autotune: the fastest warps per CTA for this batch shape, recorded
+    in the tuning cache; returns (warps_per_block, device ms)."""
+    specs = _specs(jobs)
+    wpb, ms = C.c_int32(), C.c_float()
+    _check(lib().xw_autotune(specs, len(jobs), C.byref(params.to_c()), iters, C.byref(wpb), C.byref(ms)))
+    return wpb.value, ms.value
 
 
 def header_symbols(path=HEADER):

@@ -44,6 +44,9 @@ namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
 
+// Metropolis thresholds kept per replica for objective increases 1..kThrTable.
+constexpr uint32_t kThrTable = 64;
+
 // Replica-constant fields the proposal code reads, kept in the warp's slot.
 struct View {
     const int8_t* W;
@@ -58,7 +61,7 @@ struct View {
 };
 
 struct SlotLayout {
-    uint32_t off_g, off_res, off_mino, off_mask, off_draws, off_view, bytes;
+    uint32_t off_g, off_res, off_mino, off_mask, off_draws, off_view, off_thr, bytes;
     int ld;
 };
 
@@ -72,7 +75,8 @@ __host__ __device__ inline SlotLayout slot_layout(int n, int m) {
     L.off_mask = L.off_mino + xw_pad16((uint32_t)(n * m));
     L.off_draws = L.off_mask + xw_pad16((uint32_t)n * 16u);
     L.off_view = L.off_draws + 32u * 16u;
-    L.bytes = L.off_view + xw_pad16((uint32_t)sizeof(View));
+    L.off_thr = L.off_view + xw_pad16((uint32_t)sizeof(View));
+    L.bytes = L.off_thr + kThrTable * 8u;
     return L;
 }
 
@@ -447,6 +451,20 @@ __device__ void commit(uint32_t d0, uint32_t d1, const Update& u, int ds, int8_t
     __syncwarp();
 }
 
+// tab[d-1] = ceil(exp(-d/T) * 2^32), computed with the same division and
+// exponential as metropolis_accept, so that for a 32-bit draw u
+//   u * 2^-32 < exp(-d/T)  <=>  u < tab[d-1]
+// exactly (both sides scaled by 2^32 without rounding; u is an integer).
+// Rebuilt whenever the replica's temperature changes.
+__device__ __noinline__ void build_thresholds(uint64_t* tab, double T, int lane) {
+    const double t = T > 1.0e-12 ? T : 1.0e-12;
+    for (uint32_t d = lane + 1; d <= kThrTable; d += 32) {
+        const double e = acceptance_exp(__ddiv_rn(-(double)d, t));
+        tab[d - 1] = (uint64_t)ceil(__dmul_rn(e, 0x1p32));
+    }
+    __syncwarp();
+}
+
 __device__ __forceinline__ void copy16(void* dst, const void* src, uint32_t bytes, int lane) {
     const uint32_t chunks = xw_pad16(bytes) / 16u;
     uint4* d = reinterpret_cast<uint4*>(dst);
@@ -467,7 +485,7 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
     const uint32_t jid = H->job;
     XwJob* J = a.jobs + jid;
     if (*(volatile int32_t*)&J->done) return;
-    if (a.stop_on_solve && *(volatile int32_t*)&J->solved) return;
+    if (a.stop_on_solve == 1 && *(volatile int32_t*)&J->solved) return;
 
     const int n = J->n, w = J->w, m = J->m, sparse = J->sparse;
     const SlotLayout L = slot_layout(n, m);
@@ -480,6 +498,7 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
     uint4* sDraw = reinterpret_cast<uint4*>(slot + L.off_draws);
     const uint32_t* sDw = reinterpret_cast<const uint32_t*>(sDraw);
     View* sView = reinterpret_cast<View*>(slot + L.off_view);
+    uint64_t* sThr = reinterpret_cast<uint64_t*>(slot + L.off_thr);
 
     uint64_t it = H->it;
     uint64_t iters = a.iters;
@@ -605,6 +624,8 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
     }
     __syncwarp();
 
+    build_thresholds(sThr, T, lane);
+
     // lane -> cached Philox block of this iteration
     uint32_t my_slot = 0;
     if (lane > 0) {
@@ -624,9 +645,12 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
     uint64_t done = 0;
 #pragma unroll 1
     for (; done < iters; ++done) {
+        // 1: every replica of the job stops soon after any solve;
+        // 2: a replica stops at its own solve only, so that each replica's
+        //    trajectory is independent of how the launches are scheduled
         if (a.stop_on_solve) {
             if (best_s == 0) break;
-            if ((done & 63) == 63 && *(volatile int32_t*)&J->solved) break;
+            if (a.stop_on_solve == 1 && (done & 63) == 63 && *(volatile int32_t*)&J->solved) break;
         }
         // A: draws
         sDraw[lane] = draw_block(my_slot, it, stream, k0, k1);
@@ -690,7 +714,10 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
         ++moves;
 
         // F: Metropolis
-        const bool accept = bprim <= 0 || metropolis_accept(bprim, T, mblk.y);
+        bool accept = bprim <= 0;
+        if (!accept)
+            accept = bprim <= (int64_t)kThrTable ? (uint64_t)mblk.y < sThr[bprim - 1]
+                                                 : metropolis_accept(bprim, T, mblk.y);
 
         // G: commit
         if (accept) {
@@ -720,6 +747,7 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
             ++msi;
         }
         if (!tempering) {
+            const double T0 = T;
             if (++cool >= mpc) {
                 cool = 0;
                 T = __dmul_rn(T, cooling);
@@ -730,6 +758,7 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
                 T = __dmul_rn(reheat_T, reheat);
                 if (T < t_min) T = t_min;
             }
+            if (T != T0) build_thresholds(sThr, T, lane);
         }
         ++it;
     }
@@ -755,12 +784,12 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
     __syncwarp();
 }
 
-template <int OPL>
-// Register budget: 256 threads x XW_ANNEAL_MIN_BLOCKS blocks per SM.
-#ifndef XW_ANNEAL_MIN_BLOCKS
-#define XW_ANNEAL_MIN_BLOCKS 2
+// Register budget per thread; it sets how many replica warps an SM holds.
+#ifndef XW_ANNEAL_MAXNREG
+#define XW_ANNEAL_MAXNREG 128
 #endif
-__global__ void __launch_bounds__(256, XW_ANNEAL_MIN_BLOCKS) anneal_kernel(AnnealArgs a) {
+template <int OPL>
+__global__ void __maxnreg__(XW_ANNEAL_MAXNREG) anneal_kernel(AnnealArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -783,6 +812,12 @@ __global__ void exchange_kernel(XwJob* jobs, int njobs, uint8_t* arena, const ui
     XwJob& J = jobs[j];
     if (!J.tempering || J.done || (stop_on_solve && J.solved) || J.replicas < 2 || J.replicas > XW_MAX_RUNGS) return;
     const int R = J.replicas;
+    if (J.exchange_iters) {
+        // served jobs run launches shorter than the exchange interval: swap
+        // only at the interval's boundaries of the job's own iteration count
+        const uint64_t it0 = reinterpret_cast<const RepHeader*>(arena + rec_off[J.rep_begin])->it;
+        if (it0 == 0 || it0 % J.exchange_iters) return;
+    }
     int owner[XW_MAX_RUNGS];
     int64_t E[XW_MAX_RUNGS];
     for (int k = 0; k < R; ++k) {
@@ -820,8 +855,12 @@ __global__ void exchange_kernel(XwJob* jobs, int njobs, uint8_t* arena, const ui
 // One warp per job: best replica by (best score, best conflicts, replica
 // index) -- select_best_replica, xweigh_cuda.cu:1342-1354 -- summed
 // counters, and a copy of the best replica's best W into a compact buffer.
+// The first solver -- least (solve iteration, replica index) among replicas
+// whose best score is 0 -- does not depend on how long the job ran after
+// it; with first_solver_state its best W is the one copied out.
 __global__ void collect_kernel(const XwJob* jobs, int njobs, const uint8_t* arena, const uint64_t* rec_off,
-                               const uint64_t* best_out_off, JobOut* out, int8_t* best_out) {
+                               const uint64_t* best_out_off, JobOut* out, int8_t* best_out,
+                               int first_solver_state) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= njobs) return;
@@ -829,11 +868,16 @@ __global__ void collect_kernel(const XwJob* jobs, int njobs, const uint8_t* aren
     int64_t bs = INT64_MAX, bc = INT64_MAX;
     int br = 0x7fffffff;
     uint64_t moves = 0, evals = 0, iters = 0;
+    uint64_t fs_it = UINT64_MAX, fs_ns = 0;
+    int fs = 0x7fffffff;
     uint32_t err = 0;
     for (int r = lane; r < J.replicas; r += 32) {
         const RepHeader* H = reinterpret_cast<const RepHeader*>(arena + rec_off[J.rep_begin + r]);
         const int64_t s = H->best_score, c = H->best_conflicts;
         if (s < bs || (s == bs && (c < bc || (c == bc && r < br)))) { bs = s; bc = c; br = r; }
+        if (s == 0 && (H->solve_it < fs_it || (H->solve_it == fs_it && r < fs))) {
+            fs_it = H->solve_it; fs_ns = H->solve_ns; fs = r;
+        }
         moves += H->moves;
         evals += H->cand_evals;
         iters = iters > H->it ? iters : H->it;
@@ -848,13 +892,19 @@ __global__ void collect_kernel(const XwJob* jobs, int njobs, const uint8_t* aren
         const uint64_t i2 = __shfl_xor_sync(FULL, iters, off);
         iters = iters > i2 ? iters : i2;
         err |= __shfl_xor_sync(FULL, err, off);
+        const uint64_t fi2 = __shfl_xor_sync(FULL, fs_it, off), fn2 = __shfl_xor_sync(FULL, fs_ns, off);
+        const int f2 = __shfl_xor_sync(FULL, fs, off);
+        if (fi2 < fs_it || (fi2 == fs_it && f2 < fs)) { fs_it = fi2; fs_ns = fn2; fs = f2; }
     }
+    if (first_solver_state && fs < J.replicas) br = fs;
     if (lane == 0) {
         JobOut o;
         o.score = bs; o.conflicts = bc; o.best_replica = br;
-        o.solved = J.solved; o.err = (int32_t)err; o.pad = 0;
+        o.solved = J.solved; o.err = (int32_t)err;
+        o.first_solver = fs < J.replicas ? fs : -1;
         o.moves = moves; o.cand_evals = evals; o.iters = iters;
-        o.solved_it = J.solved_it; o.solve_ns = J.solve_ns;
+        o.solved_it = fs < J.replicas ? fs_it : 0;
+        o.solve_ns = fs < J.replicas ? fs_ns : 0;
         out[warp] = o;
     }
     if (best_out && br >= 0 && br < J.replicas) {
@@ -868,6 +918,8 @@ __global__ void collect_kernel(const XwJob* jobs, int njobs, const uint8_t* aren
 __global__ void mark_t0_kernel(uint64_t* t0) {
     if (*t0 == 0) *t0 = globaltimer();
 }
+
+__global__ void stamp_kernel(uint64_t* t) { *t = globaltimer(); }
 
 }  // namespace
 
@@ -898,9 +950,16 @@ cudaError_t launch_exchange(XwJob* jobs, int njobs, uint8_t* arena, const uint64
 }
 
 cudaError_t launch_collect(const XwJob* jobs, int njobs, const uint8_t* arena, const uint64_t* rec_off,
-                           const uint64_t* best_out_off, JobOut* out, int8_t* best_out, cudaStream_t stream) {
+                           const uint64_t* best_out_off, JobOut* out, int8_t* best_out, cudaStream_t stream,
+                           int first_solver_state) {
     if (njobs <= 0) return cudaSuccess;
-    collect_kernel<<<(njobs + 3) / 4, 128, 0, stream>>>(jobs, njobs, arena, rec_off, best_out_off, out, best_out);
+    collect_kernel<<<(njobs + 3) / 4, 128, 0, stream>>>(jobs, njobs, arena, rec_off, best_out_off, out, best_out,
+                                                        first_solver_state);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stamp(uint64_t* t, cudaStream_t stream) {
+    stamp_kernel<<<1, 1, 0, stream>>>(t);
     return cudaGetLastError();
 }
 

@@ -94,6 +94,17 @@ namespace xw {
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
+std::string strfmt(const char* f, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, f);
+    vsnprintf(buf, sizeof buf, f, ap);
+    va_end(ap);
+    return buf;
+}
+
+void check_cuda(cudaError_t e, const char* what) { check(e, what); }
+
 std::string validate(int n, int w, const xw_params& p) {
     if (n < 1 || n > 32767) return "CUDA xweigh order is out of range";
     if (w < 1 || w > n) return "CUDA xweigh weight must be in [1, n]";
@@ -133,6 +144,7 @@ std::string validate(int n, int w, const xw_params& p) {
     if (p.move_set < 0 || p.move_set > 1) return "CUDA move set must be 0 or 1";
     if (p.start_kind < 0 || p.start_kind > 1) return "CUDA start kind must be 0 or 1";
     if (p.warps_per_block < 0 || p.warps_per_block > 16) return "CUDA warps per block must be in [0, 16]";
+    if (p.stop_on_solve < 0 || p.stop_on_solve > 2) return "CUDA stop-on-solve mode must be 0, 1 or 2";
     return {};
 }
 
@@ -154,6 +166,116 @@ static size_t record_bytes(int n, int m) {
     return (b + 127) & ~size_t(127);
 }
 
+void prepare_job(const xw_job_spec& s, const xw_params& p, const int8_t* starts, uint32_t job_index, bool parallel,
+                 XwJob& J, std::vector<uint8_t>& records, std::vector<double>& temps, double& t_init) {
+    if (s.n < 1 || s.n > XW_MAX_ORDER_CUDA)
+        throw std::invalid_argument(fmt("job %u: order %d is outside [1, %d] of the device path", job_index, s.n,
+                                        XW_MAX_ORDER_CUDA));
+    if (s.w < 1 || s.w > s.n) throw std::invalid_argument(fmt("job %u: weight must be in [1, n]", job_index));
+    if (s.replicas < 1) throw std::invalid_argument(fmt("job %u: replica count must be positive", job_index));
+    const bool tempering = p.tempering != 0;
+    if (tempering && s.replicas > XW_MAX_RUNGS)
+        throw std::invalid_argument(fmt("job %u: a tempering ladder has at most %d rungs", job_index, XW_MAX_RUNGS));
+    std::memset(&J, 0, sizeof J);
+    J.n = s.n;
+    J.w = s.w;
+    J.m = std::min(s.w, s.n - s.w);
+    J.sparse = s.w <= s.n - s.w;
+    J.tempering = tempering;
+    J.move_set = p.move_set;
+    J.candidate_samples = p.candidate_samples;
+    J.target_samples = p.target_samples;
+    J.moves_per_cool = p.moves_per_cool;
+    J.stuck_threshold = p.stuck_threshold;
+    J.objective = p.objective;
+    J.replicas = s.replicas;
+    // the Philox key follows the reference's curand seed derivation
+    // (xweigh_cuda.cu:1724-1727)
+    const uint32_t base = (uint32_t)s.seed;
+    const uint64_t key = ((uint64_t)base << 32) ^ s.seed ^ 0xd1b54a32d192ed03ull;
+    J.key0 = (uint32_t)key;
+    J.key1 = (uint32_t)(key >> 32);
+    const uint32_t nn = xw_pad16((uint32_t)(s.n * s.n));
+    J.off_w = 128;
+    J.off_best = 128 + nn;
+    J.off_mino = 128 + 2 * nn;
+    J.record_bytes = (uint32_t)record_bytes(s.n, J.m);
+    J.thr_greedy = coin_threshold(p.greedy_fraction);
+    J.thr_target = coin_threshold(p.target_fraction);
+    J.thr_double = p.move_set == 0 ? coin_threshold(p.double_sign_fraction) : 0;
+    J.thr_sign = coin_threshold(p.sign_fraction);
+    J.thr_swsign = coin_threshold(p.switch_sign_fraction);
+    J.t_min = p.t_min;
+    J.cooling = p.cooling;
+    J.reheat = p.reheat;
+    const uint64_t budget = s.max_moves ? s.max_moves : p.max_moves;
+    J.budget_iters = budget ? (budget + (uint64_t)s.replicas - 1) / (uint64_t)s.replicas : 0;
+
+    const int R = J.replicas, n = J.n, w = J.w;
+    std::vector<std::vector<int8_t>> W(R);
+    auto start_of = [&](int r) -> std::vector<int8_t> {
+        if (starts) return std::vector<int8_t>(starts + (size_t)r * n * n, starts + (size_t)(r + 1) * n * n);
+        if (p.start_kind == 1) return row_start(n, w, J.key0, J.key1, (uint32_t)r);
+        return CpuState::random_start(n, w, base + (uint32_t)r * 0x9e3779b9u).entries();
+    };
+    if (parallel) {
+        parallel_for(R, [&](int r) { W[r] = start_of(r); });
+    } else {
+        for (int r = 0; r < R; ++r) W[r] = start_of(r);
+    }
+    // calibrate_temperature on replica 0 (xweigh_cuda.cu:1563-1567)
+    t_init = p.t_init;
+    if (t_init <= 0.0) {
+        CpuParams cp;
+        cp.sign_fraction = p.sign_fraction;
+        cp.target_fraction = p.target_fraction;
+        cp.target_samples = p.target_samples;
+        // the reference calibrates on replica 0's State as random_start
+        // left it (minority lists in switch order) or as read from CSV
+        const CpuState s0 = (!starts && p.start_kind == 0) ? CpuState::random_start(n, w, base)
+                                                           : CpuState::from_entries(n, w, W[0]);
+        t_init = calibrate_temperature(s0, cp, base);
+    }
+    // geometric ladder from min(t_min, t_init) to t_init (xweigh_cuda.cu:1580-1594)
+    const double bottom = std::min(p.t_min, t_init);
+    const double ratio = R > 1 ? std::pow(t_init / std::max(bottom, 1.0e-12), 1.0 / (double)(R - 1)) : 1.0;
+    temps.assign(R, 0.0);
+    double t = bottom;
+    for (int r = 0; r < R; ++r) {
+        temps[r] = t;
+        t *= ratio;
+    }
+    records.assign((size_t)R * J.record_bytes, 0);
+    for (int r = 0; r < R; ++r) {
+        uint8_t* rec = records.data() + (size_t)r * J.record_bytes;
+        RepHeader* H = reinterpret_cast<RepHeader*>(rec);
+        H->job = job_index;
+        H->stream = (uint32_t)r;
+        H->temperature = temps[r];
+        H->reheat_temperature = temps[r];
+        H->rung = r;
+        // start scores, so that results read before the first launch are
+        // meaningful; the kernel rebuilds and checks them
+        {
+            int64_t st[4];
+            xw_score(n, w, W[r].data(), st);
+            H->score = H->best_score = (int32_t)st[0];
+            H->conflicts = H->best_conflicts = (int32_t)st[1];
+        }
+        if (p.objective >= 0) {
+            H->obj_kind = p.objective;
+        } else {
+            const uint32_t h = (uint32_t)r * 0x9e3779b9u + 0x85ebca6bu;
+            const double choice = (double)h * (1.0 / 4294967296.0);
+            H->obj_kind = choice < p.squared_objective_fraction ? 1
+                : choice < p.squared_objective_fraction + p.parity_objective_fraction ? 2 : 0;
+        }
+        if (W[r].size() != (size_t)n * n) throw std::invalid_argument("start state size mismatch");
+        std::memcpy(rec + J.off_w, W[r].data(), (size_t)n * n);
+        std::memcpy(rec + J.off_best, W[r].data(), (size_t)n * n);
+    }
+}
+
 void Batch::build(const xw_job_spec* specs, int njobs, const xw_params& p, const int8_t* starts) {
     params = p;
     check(cudaSetDevice(p.device), "cudaSetDevice");
@@ -161,61 +283,31 @@ void Batch::build(const xw_job_spec* specs, int njobs, const xw_params& p, const
     if (njobs < 1) throw std::invalid_argument("batch needs at least one job");
     jobs.resize(njobs);
     rep_seed.resize(njobs);
-    size_t arena = 0;
-    uint32_t rep = 0;
-    size_t best_off = 0;
     best_offsets.resize(njobs);
+    t_init_used.assign(njobs, 0.0);
+    tempering = p.tempering != 0;
+    std::vector<uint8_t> host;
+    ladder.clear();
+    rec_off.clear();
+    uint32_t rep = 0;
+    size_t best_off = 0, start_off = 0;
     int max_opl = 1;
     slot_bytes = 0;
-    tempering = p.tempering != 0;
+    std::vector<uint8_t> records;
+    std::vector<double> temps;
     for (int j = 0; j < njobs; ++j) {
         const xw_job_spec& s = specs[j];
-        if (s.n < 1 || s.n > XW_MAX_ORDER_CUDA)
-            throw std::invalid_argument(fmt("job %d: order %d is outside [1, %d] of the device path", j, s.n,
-                                            XW_MAX_ORDER_CUDA));
-        if (s.w < 1 || s.w > s.n) throw std::invalid_argument(fmt("job %d: weight must be in [1, n]", j));
-        if (s.replicas < 1) throw std::invalid_argument(fmt("job %d: replica count must be positive", j));
-        if (tempering && s.replicas > XW_MAX_RUNGS)
-            throw std::invalid_argument(fmt("job %d: a tempering ladder has at most %d rungs", j, XW_MAX_RUNGS));
         XwJob& J = jobs[j];
-        std::memset(&J, 0, sizeof J);
-        J.n = s.n;
-        J.w = s.w;
-        J.m = std::min(s.w, s.n - s.w);
-        J.sparse = s.w <= s.n - s.w;
-        J.tempering = tempering;
-        J.move_set = p.move_set;
-        J.candidate_samples = p.candidate_samples;
-        J.target_samples = p.target_samples;
-        J.moves_per_cool = p.moves_per_cool;
-        J.stuck_threshold = p.stuck_threshold;
-        J.objective = p.objective;
-        J.replicas = s.replicas;
-        // the Philox key follows the reference's curand seed derivation
-        // (xweigh_cuda.cu:1724-1727)
-        const uint32_t base = (uint32_t)s.seed;
-        const uint64_t key = ((uint64_t)base << 32) ^ s.seed ^ 0xd1b54a32d192ed03ull;
-        J.key0 = (uint32_t)key;
-        J.key1 = (uint32_t)(key >> 32);
+        prepare_job(s, p, starts ? starts + start_off : nullptr, (uint32_t)j, true, J, records, temps,
+                    t_init_used[j]);
+        if (starts) start_off += (size_t)s.replicas * s.n * s.n;
         J.rep_begin = rep;
-        const uint32_t nn = xw_pad16((uint32_t)(s.n * s.n));
-        J.off_w = 128;
-        J.off_best = 128 + nn;
-        J.off_mino = 128 + 2 * nn;
-        J.record_bytes = (uint32_t)record_bytes(s.n, J.m);
-        J.thr_greedy = coin_threshold(p.greedy_fraction);
-        J.thr_target = coin_threshold(p.target_fraction);
-        J.thr_double = p.move_set == 0 ? coin_threshold(p.double_sign_fraction) : 0;
-        J.thr_sign = coin_threshold(p.sign_fraction);
-        J.thr_swsign = coin_threshold(p.switch_sign_fraction);
-        J.t_min = p.t_min;
-        J.cooling = p.cooling;
-        J.reheat = p.reheat;
-        const uint64_t budget = s.max_moves ? s.max_moves : p.max_moves;
-        J.budget_iters = budget ? (budget + (uint64_t)s.replicas - 1) / (uint64_t)s.replicas : 0;
-        rep_seed[j] = base;
+        J.ladder_off = ladder.size();
+        if (tempering) ladder.insert(ladder.end(), temps.begin(), temps.end());
+        rep_seed[j] = (uint32_t)s.seed;
+        for (int r = 0; r < s.replicas; ++r) rec_off.push_back(host.size() + (size_t)r * J.record_bytes);
+        host.insert(host.end(), records.begin(), records.end());
         rep += (uint32_t)s.replicas;
-        arena += (size_t)s.replicas * J.record_bytes;
         best_offsets[j] = best_off;
         best_off += (size_t)s.n * s.n;
         max_opl = std::max(max_opl, anneal_opl(s.n));
@@ -224,83 +316,7 @@ void Batch::build(const xw_job_spec* specs, int njobs, const xw_params& p, const
     total_replicas = rep;
     best_bytes = best_off;
     opl = max_opl;
-
-    // host records
-    std::vector<uint8_t> host((size_t)arena, 0);
-    rec_off.resize(total_replicas);
-    ladder.clear();
-    size_t off = 0;
-    size_t start_off = 0;
-    t_init_used.assign(njobs, 0.0);
-    for (int j = 0; j < njobs; ++j) {
-        XwJob& J = jobs[j];
-        const int R = J.replicas, n = J.n, w = J.w;
-        std::vector<std::vector<int8_t>> W(R);
-        std::vector<double> t0s(1, p.t_init);
-        auto start_of = [&](int r) -> std::vector<int8_t> {
-            if (starts) return std::vector<int8_t>(starts + start_off + (size_t)r * n * n,
-                                                   starts + start_off + (size_t)(r + 1) * n * n);
-            if (p.start_kind == 1) return row_start(n, w, J.key0, J.key1, (uint32_t)r);
-            return CpuState::random_start(n, w, rep_seed[j] + (uint32_t)r * 0x9e3779b9u).entries();
-        };
-        parallel_for(R, [&](int r) { W[r] = start_of(r); });
-        if (starts) start_off += (size_t)R * n * n;
-        // calibrate_temperature on replica 0 (xweigh_cuda.cu:1563-1567)
-        double t_init = p.t_init;
-        if (t_init <= 0.0) {
-            CpuParams cp;
-            cp.sign_fraction = p.sign_fraction;
-            cp.target_fraction = p.target_fraction;
-            cp.target_samples = p.target_samples;
-            // the reference calibrates on replica 0's State as random_start
-            // left it (minority lists in switch order) or as read from CSV
-            const CpuState s0 = (!starts && p.start_kind == 0) ? CpuState::random_start(n, w, rep_seed[j])
-                                                               : CpuState::from_entries(n, w, W[0]);
-            t_init = calibrate_temperature(s0, cp, rep_seed[j]);
-        }
-        t_init_used[j] = t_init;
-        // geometric ladder from min(t_min, t_init) to t_init (xweigh_cuda.cu:1580-1594)
-        const double bottom = std::min(p.t_min, t_init);
-        const double ratio = R > 1 ? std::pow(t_init / std::max(bottom, 1.0e-12), 1.0 / (double)(R - 1)) : 1.0;
-        std::vector<double> temps(R);
-        double t = bottom;
-        for (int r = 0; r < R; ++r) {
-            temps[r] = t;
-            t *= ratio;
-        }
-        J.ladder_off = ladder.size();
-        if (tempering) ladder.insert(ladder.end(), temps.begin(), temps.end());
-        for (int r = 0; r < R; ++r) {
-            rec_off[J.rep_begin + r] = off;
-            RepHeader* H = reinterpret_cast<RepHeader*>(host.data() + off);
-            std::memset(H, 0, sizeof *H);
-            H->job = (uint32_t)j;
-            H->stream = (uint32_t)r;
-            H->temperature = temps[r];
-            H->reheat_temperature = temps[r];
-            H->rung = r;
-            // start scores, so that results read before the first launch
-            // are meaningful; the kernel rebuilds and checks them
-            {
-                int64_t st[4];
-                xw_score(n, w, W[r].data(), st);
-                H->score = H->best_score = (int32_t)st[0];
-                H->conflicts = H->best_conflicts = (int32_t)st[1];
-            }
-            if (p.objective >= 0) {
-                H->obj_kind = p.objective;
-            } else {
-                const uint32_t h = (uint32_t)r * 0x9e3779b9u + 0x85ebca6bu;
-                const double choice = (double)h * (1.0 / 4294967296.0);
-                H->obj_kind = choice < p.squared_objective_fraction ? 1
-                    : choice < p.squared_objective_fraction + p.parity_objective_fraction ? 2 : 0;
-            }
-            if (W[r].size() != (size_t)n * n) throw std::invalid_argument("start state size mismatch");
-            std::memcpy(host.data() + off + J.off_w, W[r].data(), (size_t)n * n);
-            std::memcpy(host.data() + off + J.off_best, W[r].data(), (size_t)n * n);
-            off += J.record_bytes;
-        }
-    }
+    const size_t arena = host.size();
     if (ladder.empty()) ladder.push_back(0.0);
 
     // work items: longest replicas first (cost grows with n)
@@ -790,6 +806,50 @@ int32_t xw_batch_launch_times(xw_batch* h, float* ms, int32_t cap, int32_t* coun
         *count = b.last_rounds;
         for (int k = 0; k < b.last_rounds && k < cap; ++k)
             check(cudaEventElapsedTime(&ms[k], b.events[2 * k], b.events[2 * k + 1]), "cudaEventElapsedTime");
+        return XW_OK;
+    })
+}
+
+int32_t xw_autotune(const xw_job_spec* jobs, int32_t njobs, const xw_params* pin, uint64_t iters,
+                    int32_t* best_wpb, float* best_ms) {
+    if (!jobs || njobs < 1 || !pin || !best_wpb || iters == 0) return fail(XW_ERR_INVALID, "bad autotune arguments");
+    XW_GUARD({
+        for (int j = 0; j < njobs; ++j) {
+            const std::string err = validate(jobs[j].n, jobs[j].w, *pin);
+            if (!err.empty()) return fail(XW_ERR_INVALID, err);
+        }
+        Batch b;
+        b.build(jobs, njobs, *pin, nullptr);
+        int optin = 0;
+        check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, pin->device),
+              "cudaDeviceGetAttribute max opt-in shared memory");
+        int best = 0;
+        float best_t = 0.0f;
+        for (int wpb : {1, 2, 4, 8, 16}) {
+            if ((size_t)wpb * b.slot_bytes > (size_t)optin) break;
+            b.configure_shape(wpb);
+            if (b.warps_per_block != wpb) continue;
+            float total = 0.0f;
+            for (int rep = 0; rep < 2; ++rep) {   // the first pass warms up, the second is timed
+                b.reset();
+                b.run(iters, false);
+                check(cudaStreamSynchronize(b.stream), "cudaStreamSynchronize");
+                total = 0.0f;
+                for (int k = 0; k < b.last_rounds; ++k) {
+                    float ms = 0.0f;
+                    check(cudaEventElapsedTime(&ms, b.events[2 * k], b.events[2 * k + 1]), "cudaEventElapsedTime");
+                    total += ms;
+                }
+            }
+            if (best == 0 || total < best_t) {
+                best = wpb;
+                best_t = total;
+            }
+        }
+        if (best == 0) return fail(XW_ERR_CAPACITY, "no launch shape fits the device's shared memory");
+        record_tuned(b.opl, b.slot_bytes, best);
+        *best_wpb = best;
+        if (best_ms) *best_ms = best_t;
         return XW_OK;
     })
 }

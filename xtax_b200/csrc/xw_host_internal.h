@@ -13,6 +13,19 @@ namespace xw {
 
 std::string validate(int n, int w, const xw_params& p);
 void set_last_error(const std::string& msg);
+std::string strfmt(const char* f, ...);
+// throws std::runtime_error naming `what` when e is an error
+void check_cuda(cudaError_t e, const char* what);
+
+// One job's table entry (every field but rep_begin and ladder_off), its
+// replicas' records (replicas * J.record_bytes bytes, headers naming job
+// `job_index`), its rung temperatures and its initial temperature.  starts
+// (nullable) holds replicas*n*n column-major start states; otherwise the
+// starts follow params.start_kind.  parallel: build the starts on all host
+// threads.
+void prepare_job(const xw_job_spec& spec, const xw_params& params, const int8_t* starts, uint32_t job_index,
+                 bool parallel, XwJob& J, std::vector<uint8_t>& records, std::vector<double>& temps,
+                 double& t_init);
 
 // Enqueues the batched rescoring kernel (xw_rescore.cu).
 int32_t rescore_device(const int8_t* W, int64_t count, int n, int w, int32_t* stats, int32_t* gram,
@@ -21,6 +34,8 @@ int32_t rescore_device(const int8_t* W, int64_t count, int n, int w, int32_t* st
 // Warps per block for the anneal kernel of a given lanes-per-row class and
 // shared-memory slot, from the autotuner's cache (xw_tune.cpp).
 int tuned_warps_per_block(int opl, uint32_t slot_bytes, int device);
+// Record the fastest warps per block for that class in the tuning cache.
+void record_tuned(int opl, uint32_t slot_bytes, int wpb);
 
 struct Batch {
     xw_params params{};

@@ -39,13 +39,20 @@ namespace xw {
 
 struct JobOut {
     int64_t score, conflicts;
-    int32_t best_replica, solved, err, pad;
-    uint64_t moves, cand_evals, iters, solved_it, solve_ns;
+    int32_t best_replica, solved, err;
+    int32_t first_solver;           // least (solve iteration, index) with score 0, or -1
+    uint64_t moves, cand_evals, iters;
+    uint64_t solved_it, solve_ns;   // the first solver's solve iteration and %globaltimer
 };
 
+// One warp per job: results and (best_out nonnull) the chosen replica's best
+// W at best_out + best_out_off[job].  first_solver_state chooses the first
+// solver when there is one, else the least (score, conflicts, index).
 cudaError_t launch_collect(const XwJob* jobs, int njobs, const uint8_t* arena, const uint64_t* rec_off,
                            const uint64_t* best_out_off, JobOut* out, int8_t* best_out,
-                           cudaStream_t stream);
+                           cudaStream_t stream, int first_solver_state = 0);
 cudaError_t launch_mark_t0(uint64_t* t0, cudaStream_t stream);
+// *t = %globaltimer when the stream reaches it
+cudaError_t launch_stamp(uint64_t* t, cudaStream_t stream);
 
 }  // namespace xw

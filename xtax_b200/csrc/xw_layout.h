@@ -50,6 +50,9 @@ struct XwJob {
     uint64_t solve_ns;              // %globaltimer at the solve
     int32_t done;                   // host: job retired, skip its replicas
     int32_t pad1;
+    uint64_t exchange_iters;        // tempering: exchange only when the job's
+                                    // iteration count is a multiple of this
+                                    // (0 = after every anneal launch)
 };
 
 struct RepHeader {

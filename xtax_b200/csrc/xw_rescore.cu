@@ -137,7 +137,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, int (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-__global__ void __launch_bounds__(128, 1) rescore_tc_kernel(const __grid_constant__ CUtensorMap tmap,
+__global__ void __launch_bounds__(128, 3) rescore_tc_kernel(const __grid_constant__ CUtensorMap tmap,
                                                              RescoreParams p) {
     extern __shared__ uint8_t smem_raw[];
     // tiles on a 1024-byte boundary (the 128-byte swizzle pattern repeats every 1024 bytes)
@@ -220,42 +220,51 @@ __global__ void __launch_bounds__(128, 1) rescore_tc_kernel(const __grid_constan
             }
         }
         // epilogue: warp w reads D rows 32w..32w+31 (its TMEM lane quarter)
+        // and sums |G|, [G != 0] and G^2 over whole rows; the diagonal entry
+        // (lane j of the warp's diagonal 32x32 block) is taken out after.
         const int row0 = 32 * warp;
         const bool active = row0 < p.rows_per_tile;
         int4 part = make_int4(0, 0, 0, 0);
         int diag_ok = 1;
-        int b = 0;
         if (active) {
-            const int r = row0 + lane;
-            b = row0 / p.n;                 // matrix of this warp within the tile
-            const int i = r - b * p.n;      // row within the matrix
+            const int b = row0 / p.n;       // matrix of this warp within the tile
+            const int i0 = row0 - b * p.n;  // first row of the warp within the matrix
+            const int i = i0 + lane;
             const int mat = t * p.mpt + b;
             const int col0 = b * p.n;
-            int s_abs = 0, s_nz = 0, s_sq = 0;
+            int s_abs = 0, s_nz = 0, s_sq = 0, dg = 0;
             for (int c = 0; c < p.n; c += 32) {
                 int v[32];
                 tmem_ld32(tmem + ((uint32_t)row0 << 16) + (uint32_t)(col0 + c), v);
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const int g = v[j];
-                    const int a = g < 0 ? -g : g;
-                    s_abs += a;
-                    s_nz += a < 1 ? a : 1;
-                    s_sq += g * g;
-                    if (c + j == i) {
-                        // diagonal: remove it from the off-diagonal sums and check G_ii = w
-                        s_abs -= a;
-                        s_nz -= a < 1 ? a : 1;
-                        s_sq -= g * g;
-                        diag_ok = g == p.w;
-                    }
+                for (int j = 0; j < 32; j += 2) {
+                    const int a0 = abs(v[j]), a1 = abs(v[j + 1]);
+                    s_abs += a0 + a1;
+                    s_nz += min(a0, 1) + min(a1, 1);
+                    s_sq += v[j] * v[j] + v[j + 1] * v[j + 1];
+                }
+                if (c == i0) {
+                    int d = v[0];
+#pragma unroll
+                    for (int j = 1; j < 32; ++j) d = lane == j ? v[j] : d;
+                    dg = d;
                 }
                 if (p.gram && mat < p.count) {
                     int32_t* dst = p.gram + (size_t)mat * p.n * p.n + (size_t)i * p.n + c;
+                    if (((uintptr_t)p.gram & 15u) == 0) {   // 16-byte stores need a 16-byte aligned base
+                        int4* d4 = reinterpret_cast<int4*>(dst);
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) dst[j] = v[j];
+                        for (int j = 0; j < 32; j += 4) d4[j / 4] = make_int4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) dst[j] = v[j];
+                    }
                 }
             }
+            s_abs -= abs(dg);
+            s_nz -= min(abs(dg), 1);
+            s_sq -= dg * dg;
+            diag_ok = dg == p.w;
             part.x = __reduce_add_sync(0xffffffffu, s_abs);
             part.y = __reduce_add_sync(0xffffffffu, s_nz);
             part.z = __reduce_add_sync(0xffffffffu, s_sq);
@@ -412,10 +421,12 @@ int32_t rescore_device(const int8_t* W, int64_t count, int n, int w, int32_t* st
     const size_t smem = (size_t)kStages * kTileBytes + 1024;
     e = cudaFuncSetAttribute(rescore_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return rfail(XW_ERR_CUDA, std::string("rescore attribute: ") + cudaGetErrorString(e));
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rescore_tc_kernel, 128, smem);
-    per_sm = per_sm < 1 ? 1 : (per_sm > 3 ? 3 : per_sm);   // TMEM: 128 columns per CTA
-    const int blocks = (int)std::min<int64_t>(p.ntiles, (int64_t)per_sm * sms);
+    cudaFuncSetAttribute(rescore_tc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    // three CTAs per SM (shared memory: 3 x 66 KB; TMEM: 3 x 128 of 512
+    // columns) so that one CTA's epilogue overlaps the others' loads and
+    // MMAs; the tile loop is grid-strided, so fewer resident CTAs only
+    // serialise, never skip, tiles
+    const int blocks = (int)std::min<int64_t>(p.ntiles, (int64_t)3 * sms);
     rescore_tc_kernel<<<blocks, 128, smem, stream>>>(map, p);
     e = cudaGetLastError();
     return e == cudaSuccess ? XW_OK : rfail(XW_ERR_CUDA, std::string("rescore launch: ") + cudaGetErrorString(e));
