@@ -350,7 +350,8 @@ def ours(args):
     if args.uneven_iters > 0:
         line["uneven"] = uneven_bench(X, args.uneven_iters)
     if args.serve_requests > 0:
-        line["serving"] = serving_bench(X, args.serve_requests, args.serve_plain, args.serve_quantum)
+        line["serving"] = serving_bench(X, args.serve_requests, args.serve_plain, args.serve_quantum,
+                                        args.serve_reference, args.serve_reference_cap)
     print(json.dumps(line), flush=True)
 
 
@@ -524,7 +525,8 @@ def serve_stream(X, reqs, **cfg):
     tte = np.array([r.time_to_solution_seconds for r in solved]) if solved else np.array([-1.0])
     moves = sum(r.moves for r in searched)
     failed = [r for r in res if r.state != X.REQ_DONE]
-    return {
+    per_request = [(bool(r.sylvester), bool(r.solved), r.time_to_solution_seconds) for r in res]
+    return per_request, {
         "requests": len(reqs), "searched": len(searched), "sylvester": len(res) - len(searched),
         "solved": len(solved), "censored_at_budget": len(searched) - len(solved), "failed": len(failed),
         "all_solutions_verified": all(r.verified for r in solved),
@@ -538,7 +540,53 @@ def serve_stream(X, reqs, **cfg):
     }
 
 
-def serving_bench(X, count, plain_count, quantum):
+def serve_reference_plain(reqs, cap_seconds):
+    """The reference's plain kernel on the stream's first requests, one
+    xweigh_cuda process per request (its one-instance-per-launch mode), 256
+    replicas, at most `cap_seconds` of search each (it has no move budget).
+    Queueing is the single-server FIFO of the measured service times:
+    start_k = max(arrival_k, finish_{k-1}); time-to-exact = wait + process
+    start-up + the solve time of its `new best score=0` line.  Requests the
+    reference answers with Sylvester blocks are counted apart."""
+    import numpy as np
+    finish, tte, moves, busy, solved, syl = 0.0, [], 0, 0.0, 0, 0
+    for (ta, n, w, seed) in reqs:
+        with tempfile.TemporaryDirectory() as td:
+            t0 = time.perf_counter()
+            out = subprocess.run(
+                [REF_XWEIGH_CUDA, str(n), str(w), "--replicas", str(SERVE_REPLICAS), "--seed", str(seed),
+                 "--max-seconds", str(cap_seconds), "--restart-interval", "0", "-o", os.path.join(td, "w.csv")],
+                capture_output=True, text=True, timeout=cap_seconds * 4 + 120)
+            wall = time.perf_counter() - t0
+        start = max(ta, finish)
+        finish = start + wall
+        busy += wall
+        m = re.search(r"done moves=(\d+) .*?seconds=([0-9.e+-]+)", out.stdout)
+        search_s = float(m.group(2)) if m else 0.0
+        moves += int(m.group(1)) if m else 0
+        sol = re.search(r"\[t=([0-9.e+-]+)s\] new best score=0 ", out.stdout)
+        if sol:
+            solved += 1
+            tte.append(start - ta + (wall - search_s) + float(sol.group(1)))
+        elif "[construct] using direct sum of Sylvester blocks" in out.stdout:
+            syl += 1
+    t = np.array(tte) if tte else np.array([-1.0])
+    return {"requests": len(reqs), "sylvester": syl, "solved": solved, "cap_seconds_per_request": cap_seconds,
+            "time_to_exact_s": {"p50": float(np.percentile(t, 50)), "p99": float(np.percentile(t, 99))},
+            "moves": moves, "busy_s": busy, "moves_per_sec": moves / busy if busy > 0 else 0.0,
+            "impl": "reference xweigh_cuda (sm_100a build), one process per request"}
+
+
+def tte_summary(per_request):
+    """p50/p99 time-to-exact over the searched (not Sylvester) requests that solved."""
+    import numpy as np
+    t = np.array([x for syl, ok, x in per_request if ok and not syl] or [-1.0])
+    return {"p50": float(np.percentile(t, 50)), "p99": float(np.percentile(t, 99)),
+            "solved": int(sum(1 for syl, ok, _ in per_request if ok and not syl)),
+            "searched": int(sum(1 for syl, _, _ in per_request if not syl))}
+
+
+def serving_bench(X, count, plain_count, quantum, ref_count=0, ref_cap=3.0):
     """The serving workload: the request stream through the continuous-
     batching server, and its first `plain_count` requests both served and
     one request at a time (resident cap of one request: the plain
@@ -547,13 +595,22 @@ def serving_bench(X, count, plain_count, quantum):
     out = {"workload": f"{count} requests, Poisson {SERVE_RATE:g}/s; 70% W(n,n-1) n in {list(SERVE_ORDERS)}, "
                        f"30% W(n,4) n in 16..64; {SERVE_REPLICAS} replicas and a {SERVE_BUDGET:.0e}-move budget "
                        f"per request; time-to-exact from submission, Sylvester short-circuits excluded",
-           "served": serve_stream(X, reqs, quantum_iters=quantum)}
+           "served": serve_stream(X, reqs, quantum_iters=quantum)[1]}
+    per_pre = None
     if plain_count > 0:
         pre = reqs[:plain_count]
         out["prefix_requests"] = len(pre)
-        out["served_prefix"] = serve_stream(X, pre, quantum_iters=quantum)
+        per_pre, out["served_prefix"] = serve_stream(X, pre, quantum_iters=quantum)
         out["plain_prefix"] = serve_stream(X, pre, quantum_iters=quantum, schedule=X.SCHED_ALL,
-                                           max_resident_replicas=SERVE_REPLICAS)
+                                           max_resident_replicas=SERVE_REPLICAS)[1]
+    if ref_count > 0 and os.path.exists(REF_XWEIGH_CUDA):
+        try:
+            out["plain_reference"] = serve_reference_plain(reqs[:ref_count], ref_cap)
+            if per_pre is not None and len(per_pre) >= ref_count:
+                # the same first requests, served (from the prefix run)
+                out["served_first_requests"] = dict(tte_summary(per_pre[:ref_count]), requests=ref_count)
+        except Exception as e:  # noqa: BLE001 - report, do not fail the bench
+            out["plain_reference"] = {"unavailable": str(e)[:200]}
     return out
 
 
@@ -587,6 +644,10 @@ def main():
     ap.add_argument("--serve-plain", type=int, default=60,
                     help="prefix of the stream also run one request at a time")
     ap.add_argument("--serve-quantum", type=int, default=1000, help="iterations per replica per server round")
+    ap.add_argument("--serve-reference", type=int, default=10,
+                    help="requests of the stream also run by the reference's xweigh_cuda, one process each")
+    ap.add_argument("--serve-reference-cap", type=float, default=3.0,
+                    help="search seconds per request for the reference's xweigh_cuda")
     args = ap.parse_args()
     if args.warmup < 3:
         log("[bench] warmup raised to 3")

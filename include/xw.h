@@ -315,7 +315,7 @@ typedef struct xw_server_config {
                                       requests with the fewest iterations so far, oldest first,
                                       up to max_active_replicas */
     int32_t max_active_replicas;   /* replicas advanced per round under XW_SCHED_LEAST_ATTAINED
-                                      (0 = two waves of the device's resident warps) */
+                                      (0 = four waves of the device's resident warps) */
     int32_t reserved[6];
 } xw_server_config;
 

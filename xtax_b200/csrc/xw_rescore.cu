@@ -220,8 +220,11 @@ __global__ void __launch_bounds__(128, 3) rescore_tc_kernel(const __grid_constan
             }
         }
         // epilogue: warp w reads D rows 32w..32w+31 (its TMEM lane quarter)
-        // and sums |G|, [G != 0] and G^2 over whole rows; the diagonal entry
-        // (lane j of the warp's diagonal 32x32 block) is taken out after.
+        // and sums |G|, [G != 0] and G^2 per row; the diagonal entry (lane j
+        // of the warp's diagonal 32x32 block) is taken out after.  G is
+        // symmetric, so without a Gram output each unordered pair of
+        // off-diagonal 32x32 blocks is read once, by the warp of one of its
+        // two row blocks (offsets d = 1..nb/2 cyclically), and counted twice.
         const int row0 = 32 * warp;
         const bool active = row0 < p.rows_per_tile;
         int4 part = make_int4(0, 0, 0, 0);
@@ -232,16 +235,18 @@ __global__ void __launch_bounds__(128, 3) rescore_tc_kernel(const __grid_constan
             const int i = i0 + lane;
             const int mat = t * p.mpt + b;
             const int col0 = b * p.n;
+            const int nb = p.n / 32, rb = i0 / 32;
             int s_abs = 0, s_nz = 0, s_sq = 0, dg = 0;
-            for (int c = 0; c < p.n; c += 32) {
+            int o_abs = 0, o_nz = 0, o_sq = 0;
+            auto block = [&](int c, int& a_abs, int& a_nz, int& a_sq) {
                 int v[32];
                 tmem_ld32(tmem + ((uint32_t)row0 << 16) + (uint32_t)(col0 + c), v);
 #pragma unroll
                 for (int j = 0; j < 32; j += 2) {
                     const int a0 = abs(v[j]), a1 = abs(v[j + 1]);
-                    s_abs += a0 + a1;
-                    s_nz += min(a0, 1) + min(a1, 1);
-                    s_sq += v[j] * v[j] + v[j + 1] * v[j + 1];
+                    a_abs += a0 + a1;
+                    a_nz += min(a0, 1) + min(a1, 1);
+                    a_sq += v[j] * v[j] + v[j + 1] * v[j + 1];
                 }
                 if (c == i0) {
                     int d = v[0];
@@ -260,10 +265,19 @@ __global__ void __launch_bounds__(128, 3) rescore_tc_kernel(const __grid_constan
                         for (int j = 0; j < 32; ++j) dst[j] = v[j];
                     }
                 }
+            };
+            if (p.gram) {
+                for (int c = 0; c < p.n; c += 32) block(c, s_abs, s_nz, s_sq);
+            } else {
+                block(i0, s_abs, s_nz, s_sq);
+                for (int d = 1; 2 * d <= nb; ++d) {
+                    if (2 * d == nb && rb >= d) continue;
+                    block(((rb + d) % nb) * 32, o_abs, o_nz, o_sq);
+                }
             }
-            s_abs -= abs(dg);
-            s_nz -= min(abs(dg), 1);
-            s_sq -= dg * dg;
+            s_abs += 2 * o_abs - abs(dg);
+            s_nz += 2 * o_nz - min(abs(dg), 1);
+            s_sq += 2 * o_sq - dg * dg;
             diag_ok = dg == p.w;
             part.x = __reduce_add_sync(0xffffffffu, s_abs);
             part.y = __reduce_add_sync(0xffffffffu, s_nz);

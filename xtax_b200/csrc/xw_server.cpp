@@ -147,7 +147,9 @@ struct Server {
 
     // device state (engine thread after creation)
     cudaStream_t stream = nullptr;
+    cudaStream_t side[kClasses] = {nullptr, nullptr, nullptr};   // per-class anneal launches
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t fork = nullptr, join[kClasses] = {nullptr, nullptr, nullptr};
     XwJob* d_jobs = nullptr;
     uint8_t* d_arena = nullptr;
     uint64_t* d_rec_off = nullptr;
@@ -420,8 +422,18 @@ void Server::round(bool& any_tempering) {
     last_njobs = njobs;
     check_cuda(cudaEventRecord(ev0, stream), "cudaEventRecord");
     check_cuda(cudaMemsetAsync(d_counters, 0, sizeof(uint32_t) * kClasses, stream), "reset work counters");
+    // the classes' persistent launches run side by side on their own
+    // streams, so that one launch's tail overlaps the other's work
+    int nclass = 0;
+    for (int c = 0; c < kClasses; ++c) nclass += !items_host[c].empty();
+    if (nclass > 1) check_cuda(cudaEventRecord(fork, stream), "cudaEventRecord");
     for (int c = 0; c < kClasses; ++c) {
         if (items_host[c].empty()) continue;
+        cudaStream_t st = stream;
+        if (nclass > 1) {
+            st = side[c];
+            check_cuda(cudaStreamWaitEvent(st, fork, 0), "cudaStreamWaitEvent");
+        }
         int wpb = cfg.warps_per_block > 0 ? cfg.warps_per_block
                                           : tuned_warps_per_block(opl_of_class(c), class_slot[c], cfg.device);
         wpb = std::max(1, std::min(16, wpb));
@@ -437,8 +449,12 @@ void Server::round(bool& any_tempering) {
         a.stop_on_solve = 2;
         a.pad = 0;
         check_cuda(launch_anneal(a, opl_of_class(c), wpb, blocks_for(c, class_slot[c], wpb, items_host[c].size()),
-                                 stream),
+                                 st),
                    "launch anneal_kernel");
+        if (nclass > 1) {
+            check_cuda(cudaEventRecord(join[c], st), "cudaEventRecord");
+            check_cuda(cudaStreamWaitEvent(stream, join[c], 0), "cudaStreamWaitEvent");
+        }
     }
     any_tempering = false;
     for (int s : selected) any_tempering |= slot_req[s]->params.tempering != 0;
@@ -602,7 +618,7 @@ void Server::start() {
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, optin),
                    "cudaFuncSetAttribute max dynamic shared memory");
     if (cfg.max_active_replicas <= 0) {
-        // two waves of the resident warps at the order-32 slot: enough work
+        // four waves of the resident warps at the order-32 slot: enough work
         // per round to keep every SM busy through the round's tail
         int per_sm = 0;
         const int wpb = cfg.warps_per_block > 0 ? cfg.warps_per_block : 4;
@@ -610,7 +626,7 @@ void Server::start() {
         check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, anneal_kernel_fn(1), 32 * wpb,
                                                                  (size_t)wpb * slot),
                    "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-        cfg.max_active_replicas = std::max(256, 2 * per_sm * wpb * sms);
+        cfg.max_active_replicas = std::max(256, 4 * per_sm * wpb * sms);
     }
     if (cfg.max_resident_replicas <= 0) cfg.max_resident_replicas = cfg.max_replica_ids;
     cfg.max_resident_replicas = std::min(cfg.max_resident_replicas, cfg.max_replica_ids);
@@ -621,6 +637,11 @@ void Server::start() {
     check_cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
     check_cuda(cudaEventCreate(&ev0), "cudaEventCreate");
     check_cuda(cudaEventCreate(&ev1), "cudaEventCreate");
+    check_cuda(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "cudaEventCreate");
+    for (int c = 0; c < kClasses; ++c) {
+        check_cuda(cudaStreamCreateWithFlags(&side[c], cudaStreamNonBlocking), "cudaStreamCreate");
+        check_cuda(cudaEventCreateWithFlags(&join[c], cudaEventDisableTiming), "cudaEventCreate");
+    }
     dmalloc((void**)&d_jobs, sizeof(XwJob) * J, "cudaMalloc job table");
     dmalloc((void**)&d_arena, cfg.arena_bytes, "cudaMalloc replica arena");
     dmalloc((void**)&d_rec_off, sizeof(uint64_t) * RI, "cudaMalloc record offsets");
@@ -680,6 +701,12 @@ void Server::stop() {
     if (h_stamp) cudaFreeHost(h_stamp);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    if (fork) cudaEventDestroy(fork);
+    for (int c = 0; c < kClasses; ++c) {
+        if (side[c]) cudaStreamSynchronize(side[c]);
+        if (side[c]) cudaStreamDestroy(side[c]);
+        if (join[c]) cudaEventDestroy(join[c]);
+    }
     if (stream) cudaStreamDestroy(stream);
     stream = nullptr;
 }
