@@ -60,7 +60,7 @@ typedef struct xw_params {
     int32_t moves_per_cool;
     int32_t stuck_threshold;
     double reheat;
-    double restart_interval;      /* accepted and validated; elite restarts are not run */
+    double restart_interval;      /* seconds without improvement before an elite restart (0 = off) */
     double restart_fraction;
     int32_t restart_kick_min;
     int32_t restart_kick_max;
@@ -225,6 +225,19 @@ typedef struct xw_replica_state {
  * nullable) and the minority lists (n*min(w,n-w) bytes, nullable). */
 int32_t xw_batch_read_replica(xw_batch* b, int32_t job, int32_t replica, xw_replica_state* st,
                               int8_t* W, int8_t* best_W, uint8_t* minority);
+
+/* Exact population snapshot (checkpoint / resume): the job table and every
+ * replica record as they are on the device, with the batch's parameters,
+ * ladders and initial temperatures, written atomically (temporary file +
+ * rename).  A batch loaded from it continues bit-exactly where the saved one
+ * stood: running K iterations, saving, loading and running L more gives the
+ * state of K + L iterations in one batch.  `over` (nullable) replaces the
+ * run-time settings (device, moves_per_launch, stop_on_solve,
+ * warps_per_block, max_seconds); the file is specific to this build's struct
+ * layout and is rejected otherwise.  No counterpart in the reference, which
+ * checkpoints only the best W as CSV (write_entries_csv). */
+int32_t xw_batch_save(xw_batch* b, const char* path);
+int32_t xw_batch_load(const char* path, const xw_params* over, xw_batch** out);
 
 /* Bytes the batch moves between host and device: h2d at creation (replica
  * records, job table, offsets, ladder), d2h per xw_batch_results call. */

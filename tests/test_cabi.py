@@ -184,3 +184,12 @@ def test_server_create_rejects_bad_config_without_a_device():
     with pytest.raises(X.XwError) as e:
         X.Server(warps_per_block=17)
     assert e.value.code == X.XW_ERR_INVALID
+
+
+def test_snapshot_load_rejects_foreign_files(tmp_path):
+    import ctypes as C
+    bad = tmp_path / "bad.bin"
+    bad.write_bytes(b"not a snapshot at all" * 4)
+    h = C.c_void_p()
+    assert X.lib().xw_batch_load(str(bad).encode(), None, C.byref(h)) == X.XW_ERR_INVALID
+    assert X.lib().xw_batch_load(str(tmp_path / "missing.bin").encode(), None, C.byref(h)) == X.XW_ERR_INVALID

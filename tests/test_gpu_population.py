@@ -82,3 +82,51 @@ def test_cli_drop_in_solves_and_writes_csv(tmp_path):
     rows = [list(map(int, l.split(","))) for l in out.read_text().splitlines()]
     W = np.array(rows, dtype=np.int8).T.reshape(-1)   # column-major
     assert O.verify(12, 11, W) == 3
+
+
+def test_elite_restarts_keep_replicas_consistent():
+    # a stagnating search (hard order, short restart interval): restarted
+    # replicas are loaded back by the kernel, which rebuilds their Gram and
+    # checks the scores written for them (a mismatch fails the run)
+    p = X.Params(seed=3, replicas=64, moves_per_launch=500, max_seconds=1.5, restart_interval=0.05,
+                 restart_fraction=0.5)
+    r = X.run_annealer(30, 29, p)
+    restarts = [line for line in r.log if line.startswith("[restart] seconds=")]
+    assert restarts and r.restarted_replicas >= 32 * len(restarts) // 2
+    assert r.restarted_replicas == sum(int(l.split("replicas=")[1].split()[0]) for l in restarts)
+    done = [line for line in r.log if line.startswith("done moves=")][0]
+    assert f"restarted_replicas={r.restarted_replicas}" in done
+    assert X.score(30, 29, r.best.entries)[0] == r.best.score
+
+
+def test_snapshot_resume_is_bit_exact(tmp_path):
+    # K iterations, save, load into a new batch, L more == K + L in one batch
+    p = X.Params(tempering=1, exchange_interval=500, t_min=0.1, t_init=6.0, stop_on_solve=0,
+                 squared_objective_fraction=0.0, parity_objective_fraction=0.0)
+    jobs = [{"n": 14, "w": 13, "seed": 3, "replicas": 8}, {"n": 20, "w": 19, "seed": 4, "replicas": 8},
+            {"n": 40, "w": 4, "seed": 5, "replicas": 6}]
+    ref = X.Batch(jobs, p)
+    ref.run(2000)
+    ref.synchronize()
+    a = X.Batch(jobs, p)
+    a.run(1000)
+    a.synchronize()
+    a.save(tmp_path / "pop.bin")
+    a.close()
+    b = X.Batch.load(tmp_path / "pop.bin", jobs)
+    b.run(1000)
+    b.synchronize()
+    for j, jb in enumerate(jobs):
+        for r in range(jb["replicas"]):
+            s1, W1, B1, M1 = ref.replica(j, r)
+            s2, W2, B2, M2 = b.replica(j, r)
+            assert (s1.iterations, s1.moves, s1.score, s1.best_score, s1.temperature, s1.rung) == \
+                   (s2.iterations, s2.moves, s2.score, s2.best_score, s2.temperature, s2.rung)
+            assert (W1 == W2).all() and (B1 == B2).all() and (M1 == M2).all()
+    # reset() of a loaded batch returns to the snapshot
+    b.reset()
+    b.run(1000)
+    b.synchronize()
+    assert [r.moves for r, _ in b.results()] == [r.moves for r, _ in ref.results()]
+    ref.close()
+    b.close()

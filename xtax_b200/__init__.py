@@ -190,6 +190,8 @@ def lib():
                                         C.c_void_p]),
             "xw_rescore_status": (i32, []),
             "xw_autotune": (i32, [P(JobSpec), i32, P(_Params), u64, P(i32), P(C.c_float)]),
+            "xw_batch_save": (i32, [C.c_void_p, C.c_char_p]),
+            "xw_batch_load": (i32, [C.c_char_p, P(_Params), P(C.c_void_p)]),
             "xw_server_config_default": (None, [P(ServerConfig)]),
             "xw_server_create": (i32, [P(ServerConfig), P(C.c_void_p)]),
             "xw_submit": (i32, [C.c_void_p, P(_Request), P(u64)]),
@@ -439,6 +441,24 @@ class Batch:
 
     def __del__(self):
         self.close()
+
+    def save(self, path):
+        """xw_batch_save: exact population snapshot (atomic write)."""
+        _check(lib().xw_batch_save(self.h, os.fspath(path).encode()))
+
+    @classmethod
+    def load(cls, path, jobs, params: Optional[Params] = None):
+        """xw_batch_load: a batch that continues from a snapshot.  `jobs` are
+        the saved batch's job dicts (for result shapes); `params` (optional)
+        replaces the run-time settings."""
+        self = cls.__new__(cls)
+        self.jobs = [dict(j) for j in jobs]
+        self.params = params
+        h = C.c_void_p()
+        pc = params.to_c() if params is not None else None
+        _check(lib().xw_batch_load(os.fspath(path).encode(), C.byref(pc) if pc is not None else None, C.byref(h)))
+        self.h = h
+        return self
 
     def set_stream(self, stream_ptr):
         _check(lib().xw_batch_set_stream(self.h, C.c_void_p(stream_ptr)))

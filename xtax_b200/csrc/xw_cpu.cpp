@@ -238,6 +238,177 @@ int64_t CpuState::evaluate_score(const CpuMove& mv) const {
     return d;
 }
 
+void CpuState::commit(const CpuMove& mv) {
+    auto ab = [](int v) { return (int64_t)(v < 0 ? -v : v); };
+    int64_t ds = 0, dc = 0;
+    if (mv.kind == 0) {
+        const int r = mv.row1, c = mv.col1;
+        const int ch = -2 * at(r, c);
+        for (int o = 0; o < n_; ++o) {
+            if (o == r) continue;
+            const int old = gram_[(size_t)r * n_ + o];
+            const int nw = old + ch * at(o, c);
+            const int64_t d = ab(nw) - ab(old);
+            gram_[(size_t)r * n_ + o] = nw;
+            gram_[(size_t)o * n_ + r] = nw;
+            residual_[r] += d;
+            residual_[o] += d;
+            ds += d;
+            dc += (int64_t)(nw != 0) - (int64_t)(old != 0);
+        }
+        at(r, c) = (int8_t)-at(r, c);
+    } else {
+        const int r1 = mv.row1, r2 = mv.row2, c1 = mv.col1, c2 = mv.col2;
+        const int8_t v1 = at(r1, c1), v2 = at(r2, c2);
+        for (int o = 0; o < n_; ++o) {
+            if (o == r1 || o == r2) continue;
+            const int o1 = gram_[(size_t)r1 * n_ + o], o2 = gram_[(size_t)r2 * n_ + o];
+            const int n1 = o1 + v1 * (at(o, c2) - at(o, c1));
+            const int n2 = o2 + v2 * (at(o, c1) - at(o, c2));
+            const int64_t d1 = ab(n1) - ab(o1), d2 = ab(n2) - ab(o2);
+            gram_[(size_t)r1 * n_ + o] = n1;
+            gram_[(size_t)o * n_ + r1] = n1;
+            gram_[(size_t)r2 * n_ + o] = n2;
+            gram_[(size_t)o * n_ + r2] = n2;
+            residual_[r1] += d1;
+            residual_[r2] += d2;
+            residual_[o] += d1 + d2;
+            ds += d1 + d2;
+            dc += (int64_t)(n1 != 0) - (int64_t)(o1 != 0) + (int64_t)(n2 != 0) - (int64_t)(o2 != 0);
+        }
+        at(r1, c1) = 0;
+        at(r2, c2) = 0;
+        at(r1, c2) = v1;
+        at(r2, c1) = v2;
+        mino(r1, mv.pos1) = (uint16_t)(sparse_ ? c2 : c1);
+        mino(r2, mv.pos2) = (uint16_t)(sparse_ ? c1 : c2);
+    }
+    score_ += ds;
+    conflicts_ += dc;
+}
+
+std::vector<EscapeMove> escape_moves(const CpuState& e, size_t limit) {
+    const int n = e.order();
+    const bool sparse = e.sparse_side();
+    auto at = [&](int r, int c) { return (int)e.entries()[(size_t)c * n + r]; };
+    // minority position of (row, column) on the sparse side, in column order
+    std::vector<int> mpos((size_t)n * n, -1);
+    for (int r = 0; r < n; ++r) {
+        int pos = 0;
+        for (int c = 0; c < n; ++c)
+            if ((at(r, c) != 0) == sparse) mpos[(size_t)r * n + c] = pos++;
+    }
+    const auto less = [](const EscapeMove& a, const EscapeMove& b) {
+        if (a.score_delta != b.score_delta) return a.score_delta < b.score_delta;
+        return a.conflict_delta < b.conflict_delta;
+    };
+    std::vector<EscapeMove> out;
+    for (int r1 = 0; r1 < n; ++r1)
+        for (int r2 = r1 + 1; r2 < n; ++r2)
+            for (int c1 = 0; c1 < n; ++c1) {
+                const int ov1 = at(r1, c1);
+                if (ov1 == 0 || at(r2, c1) != 0) continue;
+                for (int c2 = 0; c2 < n; ++c2) {
+                    const int ov2 = at(r2, c2);
+                    if (ov2 == 0 || at(r1, c2) != 0) continue;
+                    for (int nv1 : {-1, 1})
+                        for (int nv2 : {-1, 1}) {
+                            int64_t ds = 0, dc = 0;
+                            for (int o = 0; o < n; ++o) {
+                                if (o == r1 || o == r2) continue;
+                                const int o1 = e.gram_at(r1, o), o2 = e.gram_at(r2, o);
+                                const int n1 = o1 + nv1 * at(o, c2) - ov1 * at(o, c1);
+                                const int n2 = o2 + nv2 * at(o, c1) - ov2 * at(o, c2);
+                                ds += std::abs(n1) - std::abs(o1) + std::abs(n2) - std::abs(o2);
+                                dc += (n1 != 0) - (o1 != 0) + (n2 != 0) - (o2 != 0);
+                            }
+                            EscapeMove m;
+                            m.support.kind = 1;
+                            m.support.row1 = r1;
+                            m.support.row2 = r2;
+                            m.support.col1 = c1;
+                            m.support.col2 = c2;
+                            m.support.pos1 = mpos[(size_t)r1 * n + (sparse ? c1 : c2)];
+                            m.support.pos2 = mpos[(size_t)r2 * n + (sparse ? c2 : c1)];
+                            m.flip_first = nv1 != ov1;
+                            m.flip_second = nv2 != ov2;
+                            m.score_delta = ds;
+                            m.conflict_delta = dc;
+                            out.push_back(m);
+                            if (out.size() > limit * 2) {
+                                std::nth_element(out.begin(), out.begin() + (std::ptrdiff_t)limit, out.end(), less);
+                                out.resize(limit);
+                            }
+                        }
+                }
+            }
+    std::sort(out.begin(), out.end(), less);
+    if (out.size() > limit) out.resize(limit);
+    return out;
+}
+
+CpuState kick_elite(const CpuState& elite, const std::vector<EscapeMove>& escapes, size_t index, size_t selected,
+                    uint64_t restart_round, int replica, uint32_t base_seed, int kick_steps, const CpuParams& p) {
+    const int n = elite.order(), w = elite.weight();
+    CpuState k = elite;
+    std::mt19937 rng(base_seed ^ (uint32_t)(restart_round * 0x9e3779b97f4a7c15ull) ^
+                     ((uint32_t)replica * 0x85ebca6bu));
+    if (!escapes.empty()) {
+        const size_t pool = std::min(escapes.size(), std::max<size_t>(selected * 4, 1));
+        const EscapeMove& esc = escapes[(index + (size_t)restart_round * selected) % pool];
+        k.commit(esc.support);
+        if (esc.flip_first) {
+            CpuMove f;
+            f.kind = 0;
+            f.row1 = esc.support.row1;
+            f.col1 = esc.support.col2;
+            k.commit(f);
+        }
+        if (esc.flip_second) {
+            CpuMove f;
+            f.kind = 0;
+            f.row1 = esc.support.row2;
+            f.col1 = esc.support.col1;
+            k.commit(f);
+        }
+    }
+    const int mode = (int)((index + restart_round) % 3);
+    int random_steps = kick_steps;
+    if (mode == 0) {
+        random_steps = 0;
+    } else if (mode == 1 && kick_steps > 0 && w >= 3) {
+        const int row_kicks = std::clamp(1 + kick_steps / std::max(1, w), 1, 4);
+        const int max_flips = std::max(2, w / 2);
+        for (int rk = 0; rk < row_kicks; ++rk) {
+            const int row = std::uniform_int_distribution<int>(0, n - 1)(rng);
+            std::vector<int> cols;
+            cols.reserve((size_t)w);
+            for (int c = 0; c < n; ++c)
+                if (k.entries()[(size_t)c * n + row] != 0) cols.push_back(c);
+            std::shuffle(cols.begin(), cols.end(), rng);
+            const int flips = std::uniform_int_distribution<int>(2, max_flips)(rng);
+            for (int f = 0; f < flips; ++f) {
+                CpuMove mv;
+                mv.kind = 0;
+                mv.row1 = row;
+                mv.col1 = cols[(size_t)f];
+                k.commit(mv);
+            }
+        }
+        random_steps = kick_steps / 4;
+    }
+    CpuParams kp = p;
+    if (mode == 2) kp.sign_fraction = 0.0;
+    int applied = 0;
+    for (int a = 0; a < random_steps * 8 && applied < random_steps; ++a) {
+        CpuMove mv;
+        if (!k.propose(rng, kp, false, mv)) continue;
+        k.commit(mv);
+        ++applied;
+    }
+    return k;
+}
+
 double calibrate_temperature(const CpuState& s, const CpuParams& p, uint32_t seed) {
     if (p.t_init > 0.0) return p.t_init;
     std::mt19937 rng(seed ^ 0xa511e9b3u);

@@ -49,6 +49,14 @@ public:
 
     bool propose(std::mt19937& rng, const CpuParams& p, bool targeted, CpuMove& mv) const;
     int64_t evaluate_score(const CpuMove& mv) const;
+    // commit_sign_flip / commit_support_switch (anneal.hpp:598-666): apply
+    // the move, update the Gram, residuals, minority list, score, conflicts
+    void commit(const CpuMove& mv);
+
+    int minority_count() const { return m_; }
+    bool sparse_side() const { return sparse_; }
+    const std::vector<uint16_t>& minority() const { return minority_; }
+    int gram_at(int a, int b) const { return gram_[(size_t)a * n_ + b]; }
 
 private:
     int n_ = 0, w_ = 0, m_ = 0;
@@ -70,6 +78,25 @@ private:
     bool propose_flip(std::mt19937& rng, int row, CpuMove& mv) const;
     bool propose_switch(std::mt19937& rng, int row, CpuMove& mv) const;
 };
+
+// Elite restart of a stagnant population (xweigh_cuda.cu:1817-2289, the
+// host half of run_annealer): the best support switches out of the elite
+// state (with optional sign changes), ranked by (score delta, conflict
+// delta) and truncated to `limit` as the reference does ...
+struct EscapeMove {
+    CpuMove support;
+    bool flip_first = false, flip_second = false;
+    int64_t score_delta = 0, conflict_delta = 0;
+};
+std::vector<EscapeMove> escape_moves(const CpuState& elite, size_t limit);
+
+// ... and the kicked copy of the elite for restarted replica `replica`, the
+// `index`-th of `selected` this round: one escape move from the pool, then a
+// row kick, a run of random moves, or neither (by (index + round) % 3),
+// drawn from mt19937(base_seed ^ round * 0x9e3779b97f4a7c15 ^ replica *
+// 0x85ebca6b) as the reference seeds it.
+CpuState kick_elite(const CpuState& elite, const std::vector<EscapeMove>& escapes, size_t index, size_t selected,
+                    uint64_t restart_round, int replica, uint32_t base_seed, int kick_steps, const CpuParams& p);
 
 // calibrate_temperature (anneal.hpp:881-899)
 double calibrate_temperature(const CpuState& s, const CpuParams& p, uint32_t seed);

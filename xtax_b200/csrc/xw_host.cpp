@@ -290,9 +290,7 @@ void Batch::build(const xw_job_spec* specs, int njobs, const xw_params& p, const
     ladder.clear();
     rec_off.clear();
     uint32_t rep = 0;
-    size_t best_off = 0, start_off = 0;
-    int max_opl = 1;
-    slot_bytes = 0;
+    size_t start_off = 0;
     std::vector<uint8_t> records;
     std::vector<double> temps;
     for (int j = 0; j < njobs; ++j) {
@@ -308,27 +306,46 @@ void Batch::build(const xw_job_spec* specs, int njobs, const xw_params& p, const
         for (int r = 0; r < s.replicas; ++r) rec_off.push_back(host.size() + (size_t)r * J.record_bytes);
         host.insert(host.end(), records.begin(), records.end());
         rep += (uint32_t)s.replicas;
-        best_offsets[j] = best_off;
-        best_off += (size_t)s.n * s.n;
-        max_opl = std::max(max_opl, anneal_opl(s.n));
-        slot_bytes = std::max(slot_bytes, anneal_slot_bytes(s.n, J.m));
     }
-    total_replicas = rep;
-    best_bytes = best_off;
-    opl = max_opl;
-    const size_t arena = host.size();
     if (ladder.empty()) ladder.push_back(0.0);
+    derive_layout();
+    upload(host);
+}
 
+// Work list, result offsets, launch class and shared-memory slot from the
+// job table.
+void Batch::derive_layout() {
+    const int njobs = (int)jobs.size();
+    total_replicas = 0;
+    best_offsets.assign(njobs, 0);
+    size_t best_off = 0;
+    opl = 1;
+    slot_bytes = 0;
+    for (int j = 0; j < njobs; ++j) {
+        const XwJob& J = jobs[j];
+        total_replicas += (uint32_t)J.replicas;
+        best_offsets[j] = best_off;
+        best_off += (size_t)J.n * J.n;
+        opl = std::max(opl, anneal_opl(J.n));
+        slot_bytes = std::max(slot_bytes, anneal_slot_bytes(J.n, J.m));
+    }
+    best_bytes = best_off;
     // work items: longest replicas first (cost grows with n)
     items.resize(total_replicas);
-    for (uint32_t i = 0; i < total_replicas; ++i) items[i] = i;
     std::vector<int> job_of(total_replicas);
     for (int j = 0; j < njobs; ++j)
         for (int r = 0; r < jobs[j].replicas; ++r) job_of[jobs[j].rep_begin + r] = j;
+    for (uint32_t i = 0; i < total_replicas; ++i) items[i] = i;
     std::stable_sort(items.begin(), items.end(), [&](uint32_t a, uint32_t b) {
         return jobs[job_of[a]].n > jobs[job_of[b]].n;
     });
+}
 
+// Device buffers for the batch; the records in `host` become the state that
+// reset() restores.
+void Batch::upload(const std::vector<uint8_t>& host) {
+    const int njobs = (int)jobs.size();
+    const size_t arena = host.size();
     arena_bytes = arena;
     auto dmalloc = [&](void** ptr, size_t bytes, const char* what) {
         check(cudaMalloc(ptr, std::max<size_t>(bytes, 16)), what);
@@ -366,7 +383,108 @@ void Batch::build(const xw_job_spec* specs, int njobs, const xw_params& p, const
           "upload result offsets");
     reset();
     check(cudaStreamSynchronize(stream), "cudaStreamSynchronize upload");
-    configure_shape(p.warps_per_block);
+    configure_shape(params.warps_per_block);
+}
+
+// Population snapshot: the job table and every replica record as they are on
+// the device now, with the batch's parameters, ladder and initial
+// temperatures.  Layout (native byte order, this build's struct sizes):
+//   "XWPOP001" | u32 sizeof(XwJob), sizeof(RepHeader), sizeof(xw_params), njobs
+//   | u64 replicas, arena bytes, ladder entries | xw_params | XwJob[njobs]
+//   | u64 record offsets[replicas] | f64 ladder[] | f64 t_init[njobs] | arena
+// written to a temporary file and renamed into place.
+static const char kSnapMagic[8] = {'X', 'W', 'P', 'O', 'P', '0', '0', '1'};
+
+void Batch::save(const std::string& path) {
+    std::vector<XwJob> dj(jobs.size());
+    std::vector<uint8_t> arena(arena_bytes);
+    check(cudaMemcpyAsync(dj.data(), d_jobs, sizeof(XwJob) * dj.size(), cudaMemcpyDeviceToHost, stream),
+          "read job table");
+    check(cudaMemcpyAsync(arena.data(), d_arena, arena_bytes, cudaMemcpyDeviceToHost, stream), "read records");
+    check(cudaStreamSynchronize(stream), "cudaStreamSynchronize snapshot");
+    const std::string tmp = path + ".tmp";
+    FILE* f = std::fopen(tmp.c_str(), "wb");
+    if (!f) throw std::runtime_error("cannot write snapshot " + tmp);
+    bool ok = true;
+    auto put = [&](const void* p, size_t n) { ok = ok && std::fwrite(p, 1, n, f) == n; };
+    const uint32_t sizes[4] = {(uint32_t)sizeof(XwJob), (uint32_t)sizeof(RepHeader), (uint32_t)sizeof(xw_params),
+                               (uint32_t)jobs.size()};
+    const uint64_t counts[3] = {total_replicas, arena_bytes, ladder.size()};
+    put(kSnapMagic, 8);
+    put(sizes, sizeof sizes);
+    put(counts, sizeof counts);
+    put(&params, sizeof params);
+    put(dj.data(), sizeof(XwJob) * dj.size());
+    put(rec_off.data(), sizeof(uint64_t) * rec_off.size());
+    put(ladder.data(), sizeof(double) * ladder.size());
+    put(t_init_used.data(), sizeof(double) * t_init_used.size());
+    put(arena.data(), arena.size());
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok || std::rename(tmp.c_str(), path.c_str()) != 0) {
+        std::remove(tmp.c_str());
+        throw std::runtime_error("cannot write snapshot " + path);
+    }
+}
+
+void Batch::load(const std::string& path, const xw_params* over) {
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) throw std::invalid_argument("cannot open snapshot " + path);
+    bool ok = true;
+    auto get = [&](void* p, size_t n) { ok = ok && std::fread(p, 1, n, f) == n; };
+    char magic[8];
+    uint32_t sizes[4];
+    uint64_t counts[3];
+    get(magic, 8);
+    get(sizes, sizeof sizes);
+    get(counts, sizeof counts);
+    if (!ok || std::memcmp(magic, kSnapMagic, 8) != 0 || sizes[0] != sizeof(XwJob) ||
+        sizes[1] != sizeof(RepHeader) || sizes[2] != sizeof(xw_params) || sizes[3] == 0 ||
+        counts[0] > (1ull << 32) || counts[2] > (1ull << 32)) {
+        std::fclose(f);
+        throw std::invalid_argument("not a population snapshot of this build: " + path);
+    }
+    get(&params, sizeof params);
+    jobs.resize(sizes[3]);
+    get(jobs.data(), sizeof(XwJob) * jobs.size());
+    rec_off.resize(counts[0]);
+    get(rec_off.data(), sizeof(uint64_t) * rec_off.size());
+    ladder.resize(counts[2]);
+    get(ladder.data(), sizeof(double) * ladder.size());
+    t_init_used.resize(jobs.size());
+    get(t_init_used.data(), sizeof(double) * t_init_used.size());
+    std::vector<uint8_t> host(counts[1]);
+    get(host.data(), host.size());
+    std::fclose(f);
+    if (!ok) throw std::invalid_argument("truncated population snapshot: " + path);
+    // the saved records must lie inside the arena and name their own job
+    uint64_t total = 0;
+    for (size_t j = 0; j < jobs.size(); ++j) {
+        const XwJob& J = jobs[j];
+        if (J.n < 1 || J.n > XW_MAX_ORDER_CUDA || J.replicas < 1 || (uint64_t)J.rep_begin + J.replicas > counts[0])
+            throw std::invalid_argument("corrupt population snapshot: " + path);
+        for (int r = 0; r < J.replicas; ++r) {
+            const uint64_t off = rec_off[J.rep_begin + r];
+            if (off + J.record_bytes > host.size() ||
+                reinterpret_cast<const RepHeader*>(host.data() + off)->job != (uint32_t)j)
+                throw std::invalid_argument("corrupt population snapshot: " + path);
+        }
+        total += (uint64_t)J.replicas;
+    }
+    if (total != counts[0]) throw std::invalid_argument("corrupt population snapshot: " + path);
+    if (over) {
+        // run-time settings may change on resume; the search itself may not
+        params.device = over->device;
+        params.moves_per_launch = over->moves_per_launch;
+        params.stop_on_solve = over->stop_on_solve;
+        params.warps_per_block = over->warps_per_block;
+        params.max_seconds = over->max_seconds;
+    }
+    tempering = params.tempering != 0;
+    rep_seed.assign(jobs.size(), 0);
+    check(cudaSetDevice(params.device), "cudaSetDevice");
+    check(cudaGetDeviceProperties(&props, params.device), "cudaGetDeviceProperties");
+    derive_layout();
+    upload(host);
 }
 
 void Batch::configure_shape(int wpb) {
@@ -533,6 +651,78 @@ void Batch::fill_results(const std::vector<JobOut>& out, const int8_t* best_host
             }
         }
     }
+}
+
+// Elite restart of job j (xweigh_cuda.cu:1817-2289): restart_count replicas,
+// taken from a rotating cursor and skipping the elite, are replaced by kicked
+// copies of the elite's best state; each gets the kicked state's score, the
+// better of it and the global best as its best, and the reheat temperature.
+// The job's records make one round trip through host memory.  Returns the
+// number of replicas restarted; `line` receives the reference's log line.
+int restart_population(Batch& b, int j, const std::vector<int8_t>& elite_best, int64_t gbest, int64_t gconf,
+                       RestartState& rs, double elapsed, std::string& line) {
+    const xw_params& p = b.params;
+    XwJob& J = b.jobs[j];
+    const int R = J.replicas, n = J.n, w = J.w;
+    if (p.restart_interval <= 0.0 || R < 2 || J.tempering) return 0;
+    const int available = R - 1;
+    const int count = std::clamp((int)std::ceil(p.restart_fraction * available), 1, available);
+    const CpuState elite = CpuState::from_entries(n, w, elite_best);
+    const size_t limit = std::max<size_t>((size_t)count * 4, 1);
+    const std::vector<EscapeMove> escapes = escape_moves(elite, limit);
+    std::vector<int> selected;
+    size_t scanned = 0;
+    while ((int)selected.size() < count && scanned < (size_t)R * 2) {
+        const int r = (int)((rs.cursor + scanned) % (size_t)R);
+        ++scanned;
+        if (r == rs.elite) continue;
+        selected.push_back(r);
+    }
+    rs.cursor = (rs.cursor + scanned) % (size_t)R;
+
+    const size_t rb = J.record_bytes, base = b.rec_off[J.rep_begin];
+    std::vector<uint8_t> host((size_t)R * rb);
+    uint8_t* dev = static_cast<uint8_t*>(b.d_arena) + base;
+    check(cudaMemcpyAsync(host.data(), dev, host.size(), cudaMemcpyDeviceToHost, b.stream), "read restart records");
+    check(cudaStreamSynchronize(b.stream), "cudaStreamSynchronize");
+    CpuParams cp;
+    cp.sign_fraction = p.sign_fraction;
+    cp.target_fraction = p.target_fraction;
+    cp.target_samples = p.target_samples;
+    const int m = J.m;
+    const uint32_t base_seed = (uint32_t)p.seed;
+    parallel_for((int)selected.size(), [&](int idx) {
+        const int r = selected[(size_t)idx];
+        const int kick = selected.size() > 1
+            ? p.restart_kick_min + (int)((size_t)idx * (size_t)(p.restart_kick_max - p.restart_kick_min) /
+                                         (selected.size() - 1))
+            : p.restart_kick_min;
+        const CpuState k = kick_elite(elite, escapes, (size_t)idx, selected.size(), rs.round, r, base_seed, kick, cp);
+        uint8_t* rec = host.data() + (size_t)r * rb;
+        RepHeader* H = reinterpret_cast<RepHeader*>(rec);
+        std::memcpy(rec + J.off_w, k.entries().data(), (size_t)n * n);
+        for (int i = 0; i < n * m; ++i) rec[J.off_mino + i] = (uint8_t)k.minority()[(size_t)i];
+        const bool kick_better = k.score() < gbest || (k.score() == gbest && k.conflicts() < gconf);
+        std::memcpy(rec + J.off_best, kick_better ? k.entries().data() : elite_best.data(), (size_t)n * n);
+        H->score = (int32_t)k.score();
+        H->conflicts = (int32_t)k.conflicts();
+        H->best_score = (int32_t)(kick_better ? k.score() : gbest);
+        H->best_conflicts = (int32_t)(kick_better ? k.conflicts() : gconf);
+        int64_t st[4];
+        xw_score(n, w, k.entries().data(), st);
+        H->obj_total = H->obj_kind == 1 ? st[2] : H->obj_kind == 2 ? st[3] : st[0];
+        H->temperature = std::max(p.t_min, H->reheat_temperature * p.reheat);
+        H->msi = 0;
+        H->cool_ctr = 0;
+    });
+    check(cudaMemcpyAsync(dev, host.data(), host.size(), cudaMemcpyHostToDevice, b.stream), "write restart records");
+    check(cudaStreamSynchronize(b.stream), "cudaStreamSynchronize");
+    ++rs.round;
+    rs.restarted += selected.size();
+    line = fmt("[restart] seconds=%g elite_score=%lld replicas=%zu kicks=%d..%d min_escape_delta=%lld", elapsed,
+               (long long)gbest, selected.size(), p.restart_kick_min, p.restart_kick_max,
+               (long long)(escapes.empty() ? 0 : escapes.front().score_delta));
+    return (int)selected.size();
 }
 
 }  // namespace xw
@@ -744,6 +934,29 @@ int32_t xw_batch_create(const xw_job_spec* jobs, int32_t njobs, const xw_params*
         auto h = std::make_unique<xw_batch>();
         h->b = std::make_unique<Batch>();
         h->b->build(jobs, njobs, *p, starts);
+        *out = h.release();
+        return XW_OK;
+    })
+}
+
+int32_t xw_batch_save(xw_batch* h, const char* path) {
+    if (!h || !path) return fail(XW_ERR_INVALID, "null argument");
+    XW_GUARD({
+        h->b->save(path);
+        return XW_OK;
+    })
+}
+
+int32_t xw_batch_load(const char* path, const xw_params* over, xw_batch** out) {
+    if (!path || !out) return fail(XW_ERR_INVALID, "null argument");
+    if (over) {
+        const std::string e = validate(1, 1, *over);
+        if (!e.empty()) return fail(XW_ERR_INVALID, e);
+    }
+    XW_GUARD({
+        auto h = std::make_unique<xw_batch>();
+        h->b = std::make_unique<Batch>();
+        h->b->load(path, over);
         *out = h.release();
         return XW_OK;
     })
@@ -1034,7 +1247,8 @@ int32_t xw_run(int32_t n, int32_t w, const xw_params* pin, const int8_t* start, 
         int64_t gbest = res[0].score, gconf = res[0].conflicts;
         int best_rep = res[0].best_replica;
         const auto t0 = std::chrono::steady_clock::now();
-        double last_save = -1e300, last_progress = 0.0;
+        double last_save = -1e300, last_progress = 0.0, last_improvement = 0.0, last_restart = 0.0;
+        RestartState rs;
         bool pending = true;
         double solve_s = -1.0;
         const uint64_t budget = b.jobs[0].budget_iters;
@@ -1058,6 +1272,14 @@ int32_t xw_run(int32_t n, int32_t w, const xw_params* pin, const int8_t* start, 
                 say(fmt("[t=%gs] new best score=%lld conflicts=%lld (replica %d)", now, (long long)gbest,
                         (long long)gconf, best_rep));
                 if (gbest == 0) solve_s = now;
+                last_improvement = now;
+            }
+            if (gbest != 0 && p.restart_interval > 0.0 && now - last_improvement >= p.restart_interval &&
+                now - last_restart >= p.restart_interval) {
+                rs.elite = best_rep;
+                std::string line;
+                if (restart_population(b, 0, best, gbest, gconf, rs, now, line) > 0) say(line);
+                last_restart = now;
             }
             if (pending && now - last_save >= p.save_interval) {
                 if (checkpoint) checkpoint(best.data(), n, user);
@@ -1077,9 +1299,10 @@ int32_t xw_run(int32_t n, int32_t w, const xw_params* pin, const int8_t* start, 
             throw std::runtime_error("CUDA final best snapshot score mismatch");
         const uint64_t moves = res[0].moves, evals = res[0].cand_evals;
         say(fmt("done moves=%llu candidate_evaluations=%llu seconds=%g moves_per_sec=%g "
-                "candidate_evaluations_per_sec=%g restarted_replicas=0",
+                "candidate_evaluations_per_sec=%g restarted_replicas=%llu",
                 (unsigned long long)moves, (unsigned long long)evals, search_s,
-                search_s > 0 ? moves / search_s : 0.0, search_s > 0 ? evals / search_s : 0.0));
+                search_s > 0 ? moves / search_s : 0.0, search_s > 0 ? evals / search_s : 0.0,
+                (unsigned long long)rs.restarted));
         out->score = res[0].score;
         out->conflicts = res[0].conflicts;
         out->replicas = replicas;
@@ -1088,7 +1311,7 @@ int32_t xw_run(int32_t n, int32_t w, const xw_params* pin, const int8_t* start, 
         out->best_replica = res[0].best_replica;
         out->moves = moves;
         out->candidate_evaluations = evals;
-        out->restarted_replicas = 0;
+        out->restarted_replicas = rs.restarted;
         out->iterations = res[0].iters;
         out->initialization_seconds = init_s;
         out->search_seconds = search_s;

@@ -87,6 +87,12 @@ struct Batch {
     ~Batch();
 
     void build(const xw_job_spec* specs, int njobs, const xw_params& p, const int8_t* starts);
+    void derive_layout();
+    void upload(const std::vector<uint8_t>& host);
+    void save(const std::string& path);
+    // rebuild from a snapshot; `over` (nullable) replaces the run-time
+    // settings (device, launch length, stop mode, shape, time limit)
+    void load(const std::string& path, const xw_params* over);
     void configure_shape(int warps_per_block);
     void reset();
     uint64_t round_iters() const;
@@ -96,5 +102,19 @@ struct Batch {
     void collect(std::vector<JobOut>& out, int8_t* best_host, bool want_best);
     void fill_results(const std::vector<JobOut>& out, const int8_t* best_host, xw_job_result* res) const;
 };
+
+// Elite-restart bookkeeping of one job (the reference's restart_cursor,
+// restart_round and restarted_replicas, xweigh_cuda.cu:1812-1814).
+struct RestartState {
+    size_t cursor = 0;
+    uint64_t round = 0;
+    uint64_t restarted = 0;
+    int elite = 0;
+};
+
+// Elite restart of job j's replicas (xweigh_cuda.cu:1817-2289); returns how
+// many replicas were restarted and the reference's log line.
+int restart_population(Batch& b, int j, const std::vector<int8_t>& elite_best, int64_t gbest, int64_t gconf,
+                       RestartState& rs, double elapsed, std::string& line);
 
 }  // namespace xw
