@@ -69,6 +69,13 @@ CASES = [
                            objective=1, sign_fraction=0.3)),
     (16, 4, 4, 1500, dict(t_init=2.0, moves_per_launch=500, move_set=1, start_kind=1, objective=0)),
     (30, 29, 3, 1200, dict(t_init=6.0, moves_per_launch=600, objective=2)),
+    # edge cases: the largest order (four rows per lane), w = n (no zeros:
+    # flips only), w = 1 (one nonzero per row), an odd order
+    (128, 64, 2, 120, dict(t_init=8.0, moves_per_launch=60)),
+    (128, 127, 2, 120, dict(t_init=8.0, moves_per_launch=120)),
+    (8, 8, 4, 1500, dict(t_init=3.0, moves_per_launch=500)),
+    (9, 1, 3, 800, dict(t_init=1.0, moves_per_launch=400)),
+    (21, 16, 3, 900, dict(t_init=5.0, moves_per_launch=300)),
 ]
 
 

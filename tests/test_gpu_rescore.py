@@ -84,3 +84,25 @@ def test_rescore_at_benchmark_size(n):
     for m in rng.choice(count, 64, replace=False):
         ref, _, _ = oracle_stats(Wh[m], n, w)
         assert sh[m].tolist() == ref, m
+
+
+@pytest.mark.parametrize("n", [1, 5, 12, 26, 63, 100, 127])
+def test_simt_rescore_for_orders_off_the_tensor_core_grid(n):
+    # orders that are not multiples of 32 take the SIMT kernel
+    count, w = 17, max(1, n // 3)
+    W = random_fixed_degree(count, n, w, seed=500 + n)
+    stats, G = X.rescore(W, n, w, gram=True)
+    for m in range(count):
+        ref, Gref, _ = oracle_stats(W[m], n, w)
+        assert stats[m].tolist() == ref, (m, stats[m], ref)
+        assert (G[m] == Gref).all(), m
+
+
+def test_rescore_empty_batch_and_bad_arguments():
+    import ctypes as C
+    stats = np.zeros((1, 4), dtype=np.int32)
+    W = np.zeros((1, 32, 32), dtype=np.int8)
+    assert X.lib().xw_rescore(W.ctypes.data_as(C.POINTER(C.c_int8)), 0, 32, 16,
+                              stats.ctypes.data_as(C.POINTER(C.c_int32)), None) == X.XW_OK
+    assert X.lib().xw_rescore(W.ctypes.data_as(C.POINTER(C.c_int8)), 1, 129, 16,
+                              stats.ctypes.data_as(C.POINTER(C.c_int32)), None) == X.XW_ERR_INVALID
