@@ -32,7 +32,7 @@ extern "C" {
 #define XW_ERR_TIMEOUT 6   /* a wait ended before the request finished */
 #define XW_ERR_IO 7        /* file read or write failed */
 
-#define XW_MAX_ORDER_CUDA 128       /* largest n the device path anneals */
+#define XW_MAX_ORDER_CUDA 256       /* largest n the device path anneals */
 #define XW_MAX_CANDIDATE_SAMPLES 32 /* xweigh_cuda.hpp:11 */
 #define XW_MAX_TARGET_SAMPLES 64    /* xweigh_cuda.hpp:12 */
 

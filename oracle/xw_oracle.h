@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define XWO_MAX_N 128
+#define XWO_MAX_N 256
 
 /* ---- random streams ---------------------------------------------------- */
 void xwo_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);

@@ -76,6 +76,11 @@ CASES = [
     (8, 8, 4, 1500, dict(t_init=3.0, moves_per_launch=500)),
     (9, 1, 3, 800, dict(t_init=1.0, moves_per_launch=400)),
     (21, 16, 3, 900, dict(t_init=5.0, moves_per_launch=300)),
+    # orders above 128: eight rows per lane, int16 Gram, 256-bit row masks
+    (160, 159, 2, 60, dict(t_init=8.0, moves_per_launch=30)),
+    (200, 20, 2, 60, dict(t_init=6.0, moves_per_launch=60)),
+    (256, 255, 1, 40, dict(t_init=8.0, moves_per_launch=20)),
+    (256, 4, 2, 50, dict(t_init=2.0, moves_per_launch=50, move_set=1, start_kind=1)),
 ]
 
 
@@ -138,5 +143,25 @@ def test_mixed_orders_in_one_launch_match_oracle():
         for r in range(jb["replicas"]):
             rep = O.Replica(job, r, start_of(jb["n"], jb["w"], jb["seed"], r, p), temps[j][r], r)
             rep.run(1800, stop_on_solve=False)
+            compare(batch, j, r, rep)
+    batch.close()
+
+
+def test_small_orders_in_an_eight_rows_per_lane_launch_match_oracle():
+    # a batch with an order above 128 runs every replica with the wide
+    # kernel (int16 Gram, 256-bit masks), small orders included
+    p = X.Params(stop_on_solve=0, t_init=5.0, moves_per_launch=100)
+    jobs = [{"n": 150, "w": 149, "seed": 21, "replicas": 1}, {"n": 26, "w": 25, "seed": 22, "replicas": 2},
+            {"n": 40, "w": 4, "seed": 23, "replicas": 2}]
+    batch = X.Batch(jobs, p)
+    temps = [[batch.replica(j, r)[0].reheat_temperature for r in range(jb["replicas"])]
+             for j, jb in enumerate(jobs)]
+    batch.run(200)
+    batch.synchronize()
+    for j, jb in enumerate(jobs):
+        job = oracle_job(jb["n"], jb["w"], jb["seed"], p)
+        for r in range(jb["replicas"]):
+            rep = O.Replica(job, r, start_of(jb["n"], jb["w"], jb["seed"], r, p), temps[j][r], r)
+            rep.run(200, stop_on_solve=False)
             compare(batch, j, r, rep)
     batch.close()

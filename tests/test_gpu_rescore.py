@@ -86,7 +86,7 @@ def test_rescore_at_benchmark_size(n):
         assert sh[m].tolist() == ref, m
 
 
-@pytest.mark.parametrize("n", [1, 5, 12, 26, 63, 100, 127])
+@pytest.mark.parametrize("n", [1, 5, 12, 26, 63, 100, 127, 160, 256])
 def test_simt_rescore_for_orders_off_the_tensor_core_grid(n):
     # orders that are not multiples of 32 take the SIMT kernel
     count, w = 17, max(1, n // 3)
@@ -104,5 +104,5 @@ def test_rescore_empty_batch_and_bad_arguments():
     W = np.zeros((1, 32, 32), dtype=np.int8)
     assert X.lib().xw_rescore(W.ctypes.data_as(C.POINTER(C.c_int8)), 0, 32, 16,
                               stats.ctypes.data_as(C.POINTER(C.c_int32)), None) == X.XW_OK
-    assert X.lib().xw_rescore(W.ctypes.data_as(C.POINTER(C.c_int8)), 1, 129, 16,
+    assert X.lib().xw_rescore(W.ctypes.data_as(C.POINTER(C.c_int8)), 1, 257, 16,
                               stats.ctypes.data_as(C.POINTER(C.c_int32)), None) == X.XW_ERR_INVALID

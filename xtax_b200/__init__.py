@@ -24,7 +24,7 @@ HEADER = os.path.join(os.path.dirname(_HERE), "include", "xw.h")
 
 XW_OK, XW_ERR_INVALID, XW_ERR_CUDA, XW_ERR_CAPACITY, XW_ERR_INTERNAL = 0, 1, 2, 3, 4
 XW_ERR_NOT_FOUND, XW_ERR_TIMEOUT, XW_ERR_IO = 5, 6, 7
-MAX_ORDER_CUDA = 128
+MAX_ORDER_CUDA = 256
 MAX_CANDIDATE_SAMPLES = 32
 MAX_TARGET_SAMPLES = 64
 

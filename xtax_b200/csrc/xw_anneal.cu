@@ -35,6 +35,8 @@
 // different orders and weights share one launch.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "xw_device.cuh"
 #include "xw_kernels.h"
 
@@ -52,9 +54,9 @@ struct View {
     const int8_t* W;
     const uint8_t* mino;
     const int32_t* res;
-    const uint64_t* mask;      // 2 words per row: nonzero support
+    const uint64_t* mask;      // MW words per row: nonzero support
     const uint32_t* dw;        // cached draw words of this iteration
-    uint64_t valid_lo, valid_hi;
+    uint64_t valid[4];         // columns < n
     uint64_t thr_target, thr_dbl, thr_sign, thr_swsign;
     int n, w, m, sparse, ts, bpc, cc, move_set;
     uint32_t stream, k0, k1, pad;
@@ -65,15 +67,20 @@ struct SlotLayout {
     int ld;
 };
 
-__host__ __device__ inline SlotLayout slot_layout(int n, int m) {
+// The eight-rows-per-lane kernel (orders above 128) keeps G as int16
+// (|G_ij| <= w <= 256, as the reference does) and 256-bit row masks, so that
+// W(256,255) still fits one CTA's shared memory; `wide` selects that layout
+// for every replica of such a launch, whatever its own order.
+__host__ __device__ inline SlotLayout slot_layout(int n, int m, bool wide) {
     SlotLayout L;
     L.ld = n | 1;
     const uint32_t nn = (uint32_t)(n * n);
+    const uint32_t gsz = wide ? 2u : 4u, mw = wide ? 4u : 2u;
     L.off_g = xw_pad16(nn);
-    L.off_res = L.off_g + xw_pad16((uint32_t)(n * L.ld) * 4u);
+    L.off_res = L.off_g + xw_pad16((uint32_t)(n * L.ld) * gsz);
     L.off_mino = L.off_res + xw_pad16((uint32_t)n * 4u);
     L.off_mask = L.off_mino + xw_pad16((uint32_t)(n * m));
-    L.off_draws = L.off_mask + xw_pad16((uint32_t)n * 16u);
+    L.off_draws = L.off_mask + xw_pad16((uint32_t)n * 8u * mw);
     L.off_view = L.off_draws + 32u * 16u;
     L.off_thr = L.off_view + xw_pad16((uint32_t)sizeof(View));
     L.bytes = L.off_thr + kThrTable * 8u;
@@ -91,6 +98,31 @@ __device__ __forceinline__ int cyclic_first(uint64_t lo, uint64_t hi, int start)
     if (lo) return __ffsll((long long)lo) - 1;
     if (hi) return 64 + __ffsll((long long)hi) - 1;
     return -1;
+}
+
+__device__ __forceinline__ int cyclic_first(const uint64_t (&m)[2], int start) {
+    return cyclic_first(m[0], m[1], start);
+}
+
+// the same over a 256-bit row mask
+__device__ __forceinline__ int cyclic_first(const uint64_t (&m)[4], int start) {
+    const int ws = start >> 6;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (k < ws) continue;
+        const uint64_t x = k == ws ? (m[k] & (~0ull << (start & 63))) : m[k];
+        if (x) return 64 * k + __ffsll((long long)x) - 1;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (m[k]) return 64 * k + __ffsll((long long)m[k]) - 1;
+    return -1;
+}
+
+template <int MW>
+__device__ __forceinline__ void row_mask(const uint64_t* mask, int row, uint64_t (&m)[MW]) {
+#pragma unroll
+    for (int k = 0; k < MW; ++k) m[k] = mask[MW * row + k];
 }
 
 // Draw words outside the cached blocks (rare: attempts past the first,
@@ -135,25 +167,28 @@ struct Reg {
     __device__ __forceinline__ int at(int r, int c) const { return W[c * n + r]; }
 };
 
-// Move descriptor, two words:
-//   d0 = valid | kind<<1 | r1<<3 | r2<<10 | c1<<17 | c2<<24
-//   d1 = (v1+1) | (v2+1)<<2 | p1<<4 | p2<<11
+// Move descriptor, two words (8-bit rows, columns and minority positions):
+//   d0 = valid | kind<<1 | r1<<3 | r2<<11 | c1<<19
+//   d1 = c2 | (v1+1)<<8 | (v2+1)<<10 | p1<<12 | p2<<20
 // kinds: 0 sign flip (r1,c1); 1 support switch with new values v1 at
 // (r1,c2) and v2 at (r2,c1); 2 double flip (r1,c1),(r2,c2); 3 within-row
 // swap: the nonzero at (r1,c1) moves to (r1,c2) with value v1.
 __device__ __forceinline__ uint2 pack(int kind, int r1, int r2, int c1, int c2, int v1, int v2, int p1, int p2) {
-    return make_uint2(1u | ((uint32_t)kind << 1) | ((uint32_t)r1 << 3) | ((uint32_t)r2 << 10) |
-                          ((uint32_t)c1 << 17) | ((uint32_t)c2 << 24),
-                      (uint32_t)(v1 + 1) | ((uint32_t)(v2 + 1) << 2) | ((uint32_t)p1 << 4) | ((uint32_t)p2 << 11));
+    return make_uint2(1u | ((uint32_t)kind << 1) | ((uint32_t)r1 << 3) | ((uint32_t)r2 << 11) | ((uint32_t)c1 << 19),
+                      (uint32_t)c2 | ((uint32_t)(v1 + 1) << 8) | ((uint32_t)(v2 + 1) << 10) | ((uint32_t)p1 << 12) |
+                          ((uint32_t)p2 << 20));
 }
 
 // propose_sign_flip (xweigh_cuda.cu:302-325): a nonzero column of `row`,
 // from the minority list when the row is sparse, else the first nonzero at
 // or after a random column; -1 when the row has none.
+template <int MW>
 __device__ __noinline__ int d_flip_col(const View* v, uint64_t it, int c, int b, int j, int row) {
     if (v->sparse && v->m > 0) return v->mino[row * v->m + (int)index(v, it, c, b, j, (uint32_t)v->m)];
     const int start = (int)index(v, it, c, b, j, (uint32_t)v->n);
-    return cyclic_first(v->mask[2 * row], v->mask[2 * row + 1], start);
+    uint64_t mk[MW];
+    row_mask<MW>(v->mask, row, mk);
+    return cyclic_first(mk, start);
 }
 
 // hot_row (xweigh_cuda.cu:291-300), serial form
@@ -169,12 +204,13 @@ __device__ __noinline__ int d_hot_row(const View* v, uint64_t it, int c) {
 
 // propose_double_sign_flip (xweigh_cuda.cu:389-421), second-flip attempts
 // 1..15 (attempt 0 is evaluated inline by d_propose)
+template <int MW>
 __device__ __noinline__ uint2 d_double_rest(const View* v, uint64_t it, int c, int row1, int col1) {
 #pragma unroll 1
     for (int a = 1; a < 16; ++a) {
         const int b = 20 + (a - 1);
         const int row2 = word(v, it, c, b, 0) < 0x80000000u ? row1 : (int)index(v, it, c, b, 1, (uint32_t)v->n);
-        const int col2 = d_flip_col(v, it, c, b, 2, row2);
+        const int col2 = d_flip_col<MW>(v, it, c, b, 2, row2);
         if (col2 < 0 || (row2 == row1 && col2 == col1)) continue;
         return pack(2, row1, row2, col1, col2, 0, 0, 0, 0);
     }
@@ -208,34 +244,43 @@ __device__ __noinline__ uint2 d_switch(const View* v, uint64_t it, int c, int ro
 }
 
 // within-row swap: a nonzero of the row moves to one of its zeros
+template <int MW>
 __device__ __noinline__ uint2 d_row_swap(const View* v, uint64_t it, int c, int row) {
     if (v->m == 0) return make_uint2(0u, 0u);
-    const uint64_t nz_lo = v->mask[2 * row], nz_hi = v->mask[2 * row + 1];
+    uint64_t nz[MW];
+    row_mask<MW>(v->mask, row, nz);
     int c1, c2, pos;
     if (v->sparse) {
         pos = (int)index(v, it, c, 1, 1, (uint32_t)v->m);
         c1 = v->mino[row * v->m + pos];
-        c2 = cyclic_first(~nz_lo & v->valid_lo, ~nz_hi & v->valid_hi, (int)index(v, it, c, 1, 2, (uint32_t)v->n));
+        uint64_t zero[MW];
+#pragma unroll
+        for (int k = 0; k < MW; ++k) zero[k] = ~nz[k] & v->valid[k];
+        c2 = cyclic_first(zero, (int)index(v, it, c, 1, 2, (uint32_t)v->n));
     } else {
         pos = (int)index(v, it, c, 1, 2, (uint32_t)v->m);
         c2 = v->mino[row * v->m + pos];
-        c1 = cyclic_first(nz_lo, nz_hi, (int)index(v, it, c, 1, 1, (uint32_t)v->n));
+        c1 = cyclic_first(nz, (int)index(v, it, c, 1, 1, (uint32_t)v->n));
     }
     if (c1 < 0 || c2 < 0) return make_uint2(0u, 0u);
     return pack(3, row, 0, c1, c2, word(v, it, c, 1, 3) < 0x80000000u ? 1 : -1, 0, pos, 0);
 }
 
+template <int MW>
 __device__ __forceinline__ uint2 flip_move(const View* v, uint64_t it, int c, int b, int j, int row) {
-    const int col = d_flip_col(v, it, c, b, j, row);
+    const int col = d_flip_col<MW>(v, it, c, b, j, row);
     return col < 0 ? make_uint2(0u, 0u) : pack(0, row, 0, col, 0, 0, 0, 0, 0);
 }
 
 // flip column from a draw word without the out-of-line call: minority pick
 // for a sparse row, else the cyclic first nonzero from a random column
+template <int MW>
 __device__ __forceinline__ int flip_col_w(const Reg& r, int c, int b, int j, int row) {
     if (r.sparse && r.m > 0) return r.mino[row * r.m + (int)r.index(c, b, j, (uint32_t)r.m)];
     const int start = (int)r.index(c, b, j, (uint32_t)r.n);
-    return cyclic_first(r.mask[2 * row], r.mask[2 * row + 1], start);
+    uint64_t mk[MW];
+    row_mask<MW>(r.mask, row, mk);
+    return cyclic_first(mk, start);
 }
 
 // propose_move (xweigh_cuda.cu:423-447).  The first attempt of every move
@@ -246,6 +291,7 @@ __device__ __forceinline__ int flip_col_w(const Reg& r, int c, int b, int j, int
 // legal) branch into out-of-line code.  Move set 1 replaces the switch by
 // the within-row swap and has no double flips.  The result equals the
 // sequential reference order of draws and tests.
+template <int MW>
 __device__ __forceinline__ uint2 d_propose(const Reg& r, const View* v, int c, bool coop_ok, int coop_row) {
     const int n = r.n, m = r.m;
     const uint64_t it = r.it;
@@ -255,22 +301,22 @@ __device__ __forceinline__ uint2 d_propose(const Reg& r, const View* v, int c, b
     const bool want_flip = r.w == n || (uint64_t)r.word(c, 0, 3) < r.thr_sign;
 
     // double flip, attempt 0: first flip (2,3), second row/flip from block 3
-    const int dcol1 = flip_col_w(r, c, 2, 3, row);
+    const int dcol1 = flip_col_w<MW>(r, c, 2, 3, row);
     const int drow2 = r.word(c, 3, 0) < 0x80000000u ? row : (int)r.index(c, 3, 1, (uint32_t)n);
-    const int dcol2 = flip_col_w(r, c, 3, 2, drow2);
+    const int dcol2 = flip_col_w<MW>(r, c, 3, 2, drow2);
     const bool dbl_ok = dcol1 >= 0 && dcol2 >= 0 && !(drow2 == row && dcol2 == dcol1);
     // plain flip
-    const int fcol = flip_col_w(r, c, 1, 0, row);
+    const int fcol = flip_col_w<MW>(r, c, 1, 0, row);
 
     uint2 mv = make_uint2(0u, 0u);
     if (want_dbl && dcol1 >= 0) {
         if (dbl_ok) return pack(2, row, drow2, dcol1, dcol2, 0, 0, 0, 0);
-        mv = d_double_rest(v, it, c, row, dcol1);
+        mv = d_double_rest<MW>(v, it, c, row, dcol1);
         if (mv.x) return mv;
     }
     if (want_flip) return fcol < 0 ? make_uint2(0u, 0u) : pack(0, row, 0, fcol, 0, 0, 0, 0, 0);
     if (r.move_set == 1) {
-        mv = d_row_swap(v, it, c, row);
+        mv = d_row_swap<MW>(v, it, c, row);
     } else {
         // support switch, attempt 0 (blocks 1 and 2)
         const int mm = m > 0 ? m : 1;
@@ -292,7 +338,7 @@ __device__ __forceinline__ uint2 d_propose(const Reg& r, const View* v, int c, b
         mv = d_switch(v, it, c, row, 1);
     }
     if (mv.x) return mv;
-    return flip_move(v, it, c, 2, 2, row);
+    return flip_move<MW>(v, it, c, 2, 2, row);
 }
 
 // A decoded move as at most two row updates: row R1 gets
@@ -305,9 +351,9 @@ struct Update {
 };
 
 __device__ __forceinline__ Update decode(uint32_t d0, uint32_t d1, const int8_t* W, int n) {
-    const int kind = (d0 >> 1) & 3, r1 = (d0 >> 3) & 127, r2 = (d0 >> 10) & 127;
-    const int c1 = (d0 >> 17) & 127, c2 = (d0 >> 24) & 127;
-    const int nv1 = (int)(d1 & 3) - 1, nv2 = (int)((d1 >> 2) & 3) - 1;
+    const int kind = (d0 >> 1) & 3, r1 = (d0 >> 3) & 255, r2 = (d0 >> 11) & 255;
+    const int c1 = (d0 >> 19) & 255, c2 = d1 & 255;
+    const int nv1 = (int)((d1 >> 8) & 3) - 1, nv2 = (int)((d1 >> 10) & 3) - 1;
     const int w11 = W[c1 * n + r1], w22 = W[c2 * n + r2];
     Update u;
     u.R1 = r1;
@@ -353,8 +399,8 @@ __device__ __forceinline__ int pair_new(const Update& u, int op, const int8_t* W
 
 // evaluate_move_warp (xweigh_cuda.cu:449-599): lane-partial deltas over the
 // lane's own rows; the caller reduces them across the warp.
-template <int OPL>
-__device__ __forceinline__ Deltas eval_lane(const Update& u, const int8_t* W, const int32_t* G, int n, int ld,
+template <int OPL, typename GT>
+__device__ __forceinline__ Deltas eval_lane(const Update& u, const int8_t* W, const GT* G, int n, int ld,
                                             int lane) {
     Deltas d = {0, 0, 0, 0};
 #pragma unroll
@@ -378,8 +424,8 @@ __device__ __forceinline__ Deltas eval_lane(const Update& u, const int8_t* W, co
 
 // commit_sign_flip / commit_support_switch / commit_double_sign_flip
 // (xweigh_cuda.cu:607-877) and the within-row swap, in the two-row form.
-template <int OPL>
-__device__ void commit(uint32_t d0, uint32_t d1, const Update& u, int ds, int8_t* W, int32_t* G, int32_t* res,
+template <int OPL, int MW, typename GT>
+__device__ void commit(uint32_t d0, uint32_t d1, const Update& u, int ds, int8_t* W, GT* G, int32_t* res,
                        uint8_t* mino, uint64_t* mask, int n, int ld, int m, int sparse, int lane) {
     int s1 = 0;
 #pragma unroll
@@ -389,14 +435,14 @@ __device__ void commit(uint32_t d0, uint32_t d1, const Update& u, int ds, int8_t
             const int o1 = G[u.R1 * ld + o];
             const int n1 = o1 + u.A1 * W[u.X1 * n + o] + u.B1 * W[u.Y1 * n + o];
             const int e1 = iabs(n1) - iabs(o1);
-            G[u.R1 * ld + o] = n1;
-            G[o * ld + u.R1] = n1;
+            G[u.R1 * ld + o] = (GT)n1;
+            G[o * ld + u.R1] = (GT)n1;
             int e = e1;
             if (u.R2 >= 0) {
                 const int o2 = G[u.R2 * ld + o];
                 const int n2 = o2 + u.A2 * W[u.X2 * n + o] + u.B2 * W[u.Y2 * n + o];
-                G[u.R2 * ld + o] = n2;
-                G[o * ld + u.R2] = n2;
+                G[u.R2 * ld + o] = (GT)n2;
+                G[o * ld + u.R2] = (GT)n2;
                 e += iabs(n2) - iabs(o2);
             }
             res[o] += e;
@@ -406,16 +452,16 @@ __device__ void commit(uint32_t d0, uint32_t d1, const Update& u, int ds, int8_t
     const int S1 = __reduce_add_sync(FULL, s1);
     __syncwarp();
     if (lane == 0) {
-        const int kind = (d0 >> 1) & 3, r1 = (d0 >> 3) & 127, r2 = (d0 >> 10) & 127;
-        const int c1 = (d0 >> 17) & 127, c2 = (d0 >> 24) & 127;
-        const int nv1 = (int)(d1 & 3) - 1, nv2 = (int)((d1 >> 2) & 3) - 1;
-        const int p1 = (d1 >> 4) & 127, p2 = (d1 >> 11) & 127;
+        const int kind = (d0 >> 1) & 3, r1 = (d0 >> 3) & 255, r2 = (d0 >> 11) & 255;
+        const int c1 = (d0 >> 19) & 255, c2 = d1 & 255;
+        const int nv1 = (int)((d1 >> 8) & 3) - 1, nv2 = (int)((d1 >> 10) & 3) - 1;
+        const int p1 = (d1 >> 12) & 255, p2 = (d1 >> 20) & 255;
         if (u.pair) {
             const int op = G[r1 * ld + r2];
             const int np = pair_new(u, op, W, n, c1, c2);
             const int pd = iabs(np) - iabs(op);
-            G[r1 * ld + r2] = np;
-            G[r2 * ld + r1] = np;
+            G[r1 * ld + r2] = (GT)np;
+            G[r2 * ld + r1] = (GT)np;
             res[r1] += S1 + pd;
             res[r2] += ds - S1;
         } else if (u.R2 >= 0) {
@@ -436,16 +482,16 @@ __device__ void commit(uint32_t d0, uint32_t d1, const Update& u, int ds, int8_t
             W[c1 * n + r2] = (int8_t)nv2;
             mino[r1 * m + p1] = (uint8_t)(sparse ? c2 : c1);
             mino[r2 * m + p2] = (uint8_t)(sparse ? c1 : c2);
-            mask[2 * r1 + (c1 >> 6)] &= ~(1ull << (c1 & 63));
-            mask[2 * r1 + (c2 >> 6)] |= 1ull << (c2 & 63);
-            mask[2 * r2 + (c2 >> 6)] &= ~(1ull << (c2 & 63));
-            mask[2 * r2 + (c1 >> 6)] |= 1ull << (c1 & 63);
+            mask[MW * r1 + (c1 >> 6)] &= ~(1ull << (c1 & 63));
+            mask[MW * r1 + (c2 >> 6)] |= 1ull << (c2 & 63);
+            mask[MW * r2 + (c2 >> 6)] &= ~(1ull << (c2 & 63));
+            mask[MW * r2 + (c1 >> 6)] |= 1ull << (c1 & 63);
         } else {
             W[c1 * n + r1] = 0;
             W[c2 * n + r1] = (int8_t)nv1;
             mino[r1 * m + p1] = (uint8_t)(sparse ? c2 : c1);
-            mask[2 * r1 + (c1 >> 6)] &= ~(1ull << (c1 & 63));
-            mask[2 * r1 + (c2 >> 6)] |= 1ull << (c2 & 63);
+            mask[MW * r1 + (c1 >> 6)] &= ~(1ull << (c1 & 63));
+            mask[MW * r1 + (c2 >> 6)] |= 1ull << (c2 & 63);
         }
     }
     __syncwarp();
@@ -487,11 +533,14 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
     if (*(volatile int32_t*)&J->done) return;
     if (a.stop_on_solve == 1 && *(volatile int32_t*)&J->solved) return;
 
+    // eight rows per lane: int16 Gram and 256-bit row masks (slot_layout)
+    constexpr int MW = OPL > 4 ? 4 : 2;
+    using GT = typename std::conditional<(OPL > 4), int16_t, int32_t>::type;
     const int n = J->n, w = J->w, m = J->m, sparse = J->sparse;
-    const SlotLayout L = slot_layout(n, m);
+    const SlotLayout L = slot_layout(n, m, OPL > 4);
     const int ld = L.ld;
     int8_t* sW = reinterpret_cast<int8_t*>(slot);
-    int32_t* sG = reinterpret_cast<int32_t*>(slot + L.off_g);
+    GT* sG = reinterpret_cast<GT*>(slot + L.off_g);
     int32_t* sRes = reinterpret_cast<int32_t*>(slot + L.off_res);
     uint8_t* sMino = slot + L.off_mino;
     uint64_t* sMask = reinterpret_cast<uint64_t*>(slot + L.off_mask);
@@ -518,20 +567,23 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
     for (int k = 0; k < OPL; ++k) {
         const int o = lane + 32 * k;
         if (o < n) {
-            uint64_t lo = 0, hi = 0;
-            int pos = 0;
+            int pos = 0, weight = 0;
+#pragma unroll
+            for (int q = 0; q < MW; ++q) {
+                uint64_t word = 0;
 #pragma unroll 1
-            for (int c = 0; c < n; ++c) {
-                const bool nz = sW[c * n + o] != 0;
-                if (nz) { if (c < 64) lo |= 1ull << c; else hi |= 1ull << (c - 64); }
-                if (m > 0 && !(status0 & XW_STATUS_INIT) && nz == (sparse != 0)) {
-                    if (pos < m) sMino[o * m + pos] = (uint8_t)c;
-                    ++pos;
+                for (int c = 64 * q; c < n && c < 64 * q + 64; ++c) {
+                    const bool nz = sW[c * n + o] != 0;
+                    if (nz) word |= 1ull << (c & 63);
+                    if (m > 0 && !(status0 & XW_STATUS_INIT) && nz == (sparse != 0)) {
+                        if (pos < m) sMino[o * m + pos] = (uint8_t)c;
+                        ++pos;
+                    }
                 }
+                sMask[MW * o + q] = word;
+                weight += __popcll(word);
             }
-            sMask[2 * o] = lo;
-            sMask[2 * o + 1] = hi;
-            if (__popcll(lo) + __popcll(hi) != w) bad_rows = 1;
+            if (weight != w) bad_rows = 1;
             if (m > 0 && !(status0 & XW_STATUS_INIT) && pos != m) bad_rows = 1;
         }
     }
@@ -540,7 +592,8 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
         return;
     }
     __syncwarp();
-    int p_score = 0, p_conf = 0, p_sq = 0, p_par = 0;
+    int p_score = 0, p_conf = 0, p_par = 0;
+    long long p_sq = 0;
 #pragma unroll
     for (int k = 0; k < OPL; ++k) {
         const int o = lane + 32 * k;
@@ -551,12 +604,12 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
                 int dot = 0;
 #pragma unroll 1
                 for (int c = 0; c < n; ++c) dot += sW[c * n + r] * sW[c * n + o];
-                sG[r * ld + o] = dot;
+                sG[r * ld + o] = (GT)dot;
                 if (r != o) {
                     const int ad = iabs(dot);
                     r_sum += ad;
                     p_conf += dot != 0;
-                    p_sq += dot * dot;
+                    p_sq += (long long)(dot * dot);
                     p_par += ad & 1;
                 }
             }
@@ -566,7 +619,9 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
     }
     const int score0 = __reduce_add_sync(FULL, p_score) / 2;
     const int conf0 = __reduce_add_sync(FULL, p_conf) / 2;
-    const int sq0 = __reduce_add_sync(FULL, p_sq) / 2;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) p_sq += __shfl_xor_sync(FULL, p_sq, off);
+    const long long sq0 = p_sq / 2;
     const int par0 = __reduce_add_sync(FULL, p_par) / 2;
     __syncwarp();
 
@@ -613,8 +668,11 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
     if (lane == 0) {
         View v;
         v.W = sW; v.mino = sMino; v.res = sRes; v.mask = sMask; v.dw = sDw;
-        v.valid_lo = n >= 64 ? ~0ull : ((1ull << n) - 1ull);
-        v.valid_hi = n <= 64 ? 0ull : (n == 128 ? ~0ull : ((1ull << (n - 64)) - 1ull));
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int lo = 64 * q;
+            v.valid[q] = n >= lo + 64 ? ~0ull : n <= lo ? 0ull : ((1ull << (n - lo)) - 1ull);
+        }
         v.thr_target = J->thr_target; v.thr_dbl = J->thr_double; v.thr_sign = J->thr_sign;
         v.thr_swsign = J->thr_swsign;
         v.n = n; v.w = w; v.m = m; v.sparse = sparse; v.ts = ts; v.bpc = bpc; v.cc = 31 / bpc;
@@ -676,7 +734,7 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
         // D: proposals, lane c proposes candidate c
         uint2 desc = make_uint2(0u, 0u);
         rg.it = it;
-        if (lane < count) desc = d_propose(rg, sView, lane, coop && lane < 4, coop_row);
+        if (lane < count) desc = d_propose<MW>(rg, sView, lane, coop && lane < 4, coop_row);
         __syncwarp();
 
         // E: evaluate in candidate order, keep the first best
@@ -689,7 +747,7 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
             const uint32_t e1 = __shfl_sync(FULL, desc.y, c);
             if (!(e0 & 1u)) continue;
             const Update u = decode(e0, e1, sW, n);
-            const Deltas d = eval_lane<OPL>(u, sW, sG, n, ld, lane);
+            const Deltas d = eval_lane<OPL, GT>(u, sW, sG, n, ld, lane);
             const int packed = __reduce_add_sync(FULL, d.ds * 4096 + d.dc);
             const int dc = ((packed + 2048) & 4095) - 2048;
             const int ds = (packed - dc) >> 12;
@@ -722,7 +780,7 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
         // G: commit
         if (accept) {
             const Update u = decode(b0, b1, sW, n);
-            commit<OPL>(b0, b1, u, bds, sW, sG, sRes, sMino, sMask, n, ld, m, sparse, lane);
+            commit<OPL, MW, GT>(b0, b1, u, bds, sW, sG, sRes, sMino, sMask, n, ld, m, sparse, lane);
             score += bds;
             conflicts += bdc;
             obj_total += bprim;
@@ -923,14 +981,15 @@ __global__ void stamp_kernel(uint64_t* t) { *t = globaltimer(); }
 
 }  // namespace
 
-uint32_t anneal_slot_bytes(int n, int m) { return slot_layout(n, m).bytes; }
+uint32_t anneal_slot_bytes(int n, int m, int opl) { return slot_layout(n, m, opl > 4).bytes; }
 
-int anneal_opl(int n) { return n <= 32 ? 1 : n <= 64 ? 2 : 4; }
+int anneal_opl(int n) { return n <= 32 ? 1 : n <= 64 ? 2 : n <= 128 ? 4 : 8; }
 
 const void* anneal_kernel_fn(int opl) {
     if (opl == 1) return reinterpret_cast<const void*>(&anneal_kernel<1>);
     if (opl == 2) return reinterpret_cast<const void*>(&anneal_kernel<2>);
-    return reinterpret_cast<const void*>(&anneal_kernel<4>);
+    if (opl == 4) return reinterpret_cast<const void*>(&anneal_kernel<4>);
+    return reinterpret_cast<const void*>(&anneal_kernel<8>);
 }
 
 cudaError_t launch_anneal(const AnnealArgs& args, int opl, int warps_per_block, int blocks, cudaStream_t stream) {
@@ -938,7 +997,8 @@ cudaError_t launch_anneal(const AnnealArgs& args, int opl, int warps_per_block, 
     const dim3 grid(blocks), block(32 * warps_per_block);
     if (opl == 1) anneal_kernel<1><<<grid, block, smem, stream>>>(args);
     else if (opl == 2) anneal_kernel<2><<<grid, block, smem, stream>>>(args);
-    else anneal_kernel<4><<<grid, block, smem, stream>>>(args);
+    else if (opl == 4) anneal_kernel<4><<<grid, block, smem, stream>>>(args);
+    else anneal_kernel<8><<<grid, block, smem, stream>>>(args);
     return cudaGetLastError();
 }
 

@@ -327,8 +327,9 @@ void Batch::derive_layout() {
         best_offsets[j] = best_off;
         best_off += (size_t)J.n * J.n;
         opl = std::max(opl, anneal_opl(J.n));
-        slot_bytes = std::max(slot_bytes, anneal_slot_bytes(J.n, J.m));
     }
+    // one launch runs every replica with the widest class's kernel and layout
+    for (int j = 0; j < njobs; ++j) slot_bytes = std::max(slot_bytes, anneal_slot_bytes(jobs[j].n, jobs[j].m, opl));
     best_bytes = best_off;
     // work items: longest replicas first (cost grows with n)
     items.resize(total_replicas);
@@ -1197,7 +1198,7 @@ int32_t xw_run(int32_t n, int32_t w, const xw_params* pin, const int8_t* start, 
     int32_t rc = xw_query_device(p.device, &out->device);
     if (rc != XW_OK) return rc;
     if (n > XW_MAX_ORDER_CUDA) {
-        const double need = anneal_slot_bytes(std::min(n, 4096), std::min(w, n - w)) / 1024.0;
+        const double need = anneal_slot_bytes(std::min(n, 4096), std::min(w, n - w), 8) / 1024.0;
         return fail(XW_ERR_CAPACITY,
                     fmt("CUDA replica requires %.2f KiB of shared memory, but device %d permits %.2f KiB per "
                         "opt-in block",
@@ -1214,7 +1215,7 @@ int32_t xw_run(int32_t n, int32_t w, const xw_params* pin, const int8_t* start, 
         spec.seed = p.seed;
         int replicas = p.replicas;
         const int m = std::min(w, n - w);
-        const uint32_t slot = anneal_slot_bytes(n, m);
+        const uint32_t slot = anneal_slot_bytes(n, m, anneal_opl(n));
         if (replicas == 0) {
             // one resident wave: warp slots per SM times SMs
             const int wpb = p.warps_per_block > 0 ? p.warps_per_block : 4;

@@ -24,8 +24,10 @@ struct AnnealArgs {
 };
 
 // shared-memory bytes one warp needs for a replica of order n, minority m
-uint32_t anneal_slot_bytes(int n, int m);
-// lanes' rows per lane: 1 for n <= 32, 2 for n <= 64, 4 for n <= 128
+// shared-memory bytes one warp needs for a replica of order n, minority m,
+// in a launch of the `opl` rows-per-lane kernel
+uint32_t anneal_slot_bytes(int n, int m, int opl);
+// lanes' rows per lane: 1 for n <= 32, 2 for n <= 64, 4 for n <= 128, 8 for n <= 256
 int anneal_opl(int n);
 const void* anneal_kernel_fn(int opl);
 cudaError_t launch_anneal(const AnnealArgs& args, int opl, int warps_per_block, int blocks,

@@ -16,7 +16,7 @@
 
 #include <stdint.h>
 
-#define XW_MAX_N 128
+#define XW_MAX_N 256
 #define XW_MAX_CANDIDATES 32
 #define XW_MAX_TARGET_SAMPLES 64
 #define XW_NOALLOC_SCRATCH_BYTES (4 * 1024 * 1024)

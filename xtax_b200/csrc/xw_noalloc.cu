@@ -155,7 +155,7 @@ extern "C" int32_t xw_anneal_noalloc(int32_t n, int32_t w, const xw_params* p, i
         if (!e.empty()) return nfail(XW_ERR_INVALID, e);
     }
     if (n > XW_MAX_ORDER_CUDA)
-        return nfail(XW_ERR_CAPACITY, "xw_anneal_noalloc: order above the device path's maximum of 128");
+        return nfail(XW_ERR_CAPACITY, "xw_anneal_noalloc: order above the device path's maximum of 256");
     if (replicas < 1) return nfail(XW_ERR_INVALID, "xw_anneal_noalloc: replica count must be positive");
     if (iters < 1) return nfail(XW_ERR_INVALID, "xw_anneal_noalloc: iterations must be positive");
     if (!(p->t_init > 0.0))
@@ -183,7 +183,7 @@ extern "C" int32_t xw_anneal_noalloc(int32_t n, int32_t w, const xw_params* p, i
     if (dev < 0 || dev >= kMaxDevices) return nfail(XW_ERR_INVALID, "xw_anneal_noalloc: device ordinal too large");
 
     const int opl = anneal_opl(n);
-    const uint32_t slot = anneal_slot_bytes(n, m);
+    const uint32_t slot = anneal_slot_bytes(n, m, opl);
     const int wpb = p->warps_per_block > 0 ? p->warps_per_block : 4;
     const void* fn = anneal_kernel_fn(opl);
     unsigned char* scratch = nullptr;

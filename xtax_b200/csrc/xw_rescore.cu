@@ -399,10 +399,11 @@ int* error_flag_ptr() {
 int32_t rescore_device(const int8_t* W, int64_t count, int n, int w, int32_t* stats, int32_t* gram,
                        cudaStream_t stream, int* err_flag, bool force_simt) {
     if (count < 0 || count > INT32_MAX / 4) return rfail(XW_ERR_INVALID, "rescore: count out of range");
-    if (n < 1 || n > XW_MAX_ORDER_CUDA) return rfail(XW_ERR_INVALID, "rescore: order must be in [1, 128]");
+    if (n < 1 || n > XW_MAX_ORDER_CUDA) return rfail(XW_ERR_INVALID, "rescore: order must be in [1, 256]");
     if (count == 0) return XW_OK;
     cudaError_t e;
-    const bool tc = !force_simt && n % 32 == 0 && ((uintptr_t)W % 16) == 0;
+    // tensor cores for n in {32, 64, 96, 128}: a tile row is one 128-byte TMA row
+    const bool tc = !force_simt && n % 32 == 0 && n <= 128 && ((uintptr_t)W % 16) == 0;
     if (!tc) {
         const int blocks = (int)((count * 32 + 255) / 256);
         rescore_simt_kernel<<<blocks, 256, 0, stream>>>(W, (int)count, n, w, reinterpret_cast<int4*>(stats), gram);

@@ -49,11 +49,11 @@
 namespace xw {
 namespace {
 
-constexpr int kClasses = 3;                      // lanes per row 1, 2, 4
+constexpr int kClasses = 4;                      // rows per lane 1, 2, 4, 8
 constexpr size_t kBestStride = (size_t)XW_MAX_N * XW_MAX_N;
 
-int class_of(int n) { return n <= 32 ? 0 : n <= 64 ? 1 : 2; }
-int opl_of_class(int c) { return c == 0 ? 1 : c == 1 ? 2 : 4; }
+int class_of(int n) { return n <= 32 ? 0 : n <= 64 ? 1 : n <= 128 ? 2 : 3; }
+int opl_of_class(int c) { return 1 << c; }
 
 // First-fit allocator of [0, capacity) ranges with coalescing on release.
 struct RangeAlloc {
@@ -147,9 +147,9 @@ struct Server {
 
     // device state (engine thread after creation)
     cudaStream_t stream = nullptr;
-    cudaStream_t side[kClasses] = {nullptr, nullptr, nullptr};   // per-class anneal launches
+    cudaStream_t side[kClasses] = {};                // per-class anneal launches
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    cudaEvent_t fork = nullptr, join[kClasses] = {nullptr, nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join[kClasses] = {};
     XwJob* d_jobs = nullptr;
     uint8_t* d_arena = nullptr;
     uint64_t* d_rec_off = nullptr;
@@ -170,7 +170,7 @@ struct Server {
     uint64_t resident = 0;
     bool items_dirty = true;
     std::vector<uint32_t> items_host[kClasses];
-    uint32_t class_slot[kClasses] = {0, 0, 0};
+    uint32_t class_slot[kClasses] = {};
     std::map<std::pair<int, uint32_t>, int> per_sm_cache;
     int last_njobs = 0;
 
@@ -388,7 +388,7 @@ void Server::rebuild_items() {
         const ReqPtr& q = slot_req[s];
         const int c = class_of(q->spec.n);
         for (int r = 0; r < q->spec.replicas; ++r) items_host[c].push_back((uint32_t)(q->rep_begin + r));
-        class_slot[c] = std::max(class_slot[c], anneal_slot_bytes(q->spec.n, q->job.m));
+        class_slot[c] = std::max(class_slot[c], anneal_slot_bytes(q->spec.n, q->job.m, opl_of_class(c)));
     }
     for (int c = 0; c < kClasses; ++c)
         if (!items_host[c].empty())
@@ -622,7 +622,7 @@ void Server::start() {
         // per round to keep every SM busy through the round's tail
         int per_sm = 0;
         const int wpb = cfg.warps_per_block > 0 ? cfg.warps_per_block : 4;
-        const uint32_t slot = anneal_slot_bytes(32, 16);
+        const uint32_t slot = anneal_slot_bytes(32, 16, 1);
         check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, anneal_kernel_fn(1), 32 * wpb,
                                                                  (size_t)wpb * slot),
                    "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
