@@ -313,7 +313,8 @@ def ours(args):
     sm_mhz = clocks.get("sm_mhz") or 1965.0
     smem_peak = 148 * 128 * sm_mhz * 1e6 / 1e9   # GB/s, nominal: 128 B/clk/SM
     achieved = alg_bytes / (avg_launch_ms / 1e3) / 1e9
-    prof = load_profile_traffic()
+    prof = load_profile_figure("traffic_bytes_per_launch")
+    issue = load_profile_figure("issue_active_pct")
     line = {
         "metric": METRIC, "value": value, "unit": "moves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -323,7 +324,8 @@ def ours(args):
                    "launch_shape": list(batch.shape()), "parallelism": f"instances x{world} GPUs"},
         "gpu_launches": args.steps * (2 * (-(-iters // EXCHANGE)) + 1),
         "roofline": {"bound": "smem", "achieved": achieved, "peak": smem_peak, "unit": "GB/s",
-                     "frac": achieved / smem_peak, "traffic": prof,
+                     "frac": achieved / smem_peak, "traffic": int(prof) if prof else None,
+                     "issue_active_pct_ncu": issue,
                      "kernel": "anneal_kernel", "avg_launch_ms": avg_launch_ms,
                      "peak_source": "nominal 128 B/clk/SM x 148 SMs x median SM clock (no measured shared-memory peak)"},
         "clocks": clocks,
@@ -614,14 +616,15 @@ def serving_bench(X, count, plain_count, quantum, ref_count=0, ref_cap=3.0):
     return out
 
 
-def load_profile_traffic():
-    """DRAM bytes (read + write) per anneal launch from the committed ncu
-    summary of this workload, if any."""
+def load_profile_figure(name):
+    """A figure (`name = value`) of the committed ncu summary of this
+    workload's anneal kernel, if any: DRAM bytes (read + write) per launch,
+    issue-slot utilisation."""
     path = os.path.join(REPO, "profiles", "anneal_kernel_w26_tempering.md")
     try:
         with open(path) as f:
-            m = re.search(r"traffic_bytes_per_launch\s*=\s*(\d+)", f.read())
-        return int(m.group(1)) if m else None
+            m = re.search(name + r"\s*=\s*([0-9.]+)", f.read())
+        return float(m.group(1)) if m else None
     except OSError:
         return None
 
