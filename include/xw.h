@@ -284,6 +284,22 @@ int32_t xw_rescore_device(const int8_t* W_rowmajor, int64_t count, int32_t n, in
  * last call (the flag is cleared).  Synchronous. */
 int32_t xw_rescore_status(void);
 
+/* ---- elite restarts --------------------------------------------------- */
+/* The escape-move scan of an elite restart (xweigh_cuda.cu:1870-2057), on
+ * the device: every support switch out of W (rows r1 < r2, a column c1
+ * nonzero in r1 and zero in r2, a column c2 nonzero in r2 and zero in r1,
+ * new signs new1 at (r1,c2) and new2 at (r2,c1)) with its exact change of
+ * the L1 score and of the conflicts; `out` receives the `limit` best by
+ * (score delta, conflict delta), ties in scan order (r1, r2, c1, c2, new1,
+ * new2), and *count how many (fewer when there are fewer switches).
+ * xw_run's restarts use it.  W: n*n column-major, rows of weight w. */
+typedef struct xw_escape_move {
+    int32_t row1, row2, col1, col2, new1, new2;
+    int64_t score_delta, conflict_delta;
+} xw_escape_move;
+int32_t xw_escape_scan(int32_t n, int32_t w, const int8_t* W_colmajor, int32_t limit, xw_escape_move* out,
+                       int32_t* count);
+
 /* ---- serving: continuous batching of search requests ------------------ */
 /* The reference serves one search per process: xweigh_cuda_main.cpp:281-285
  * calls run_annealer (xweigh_cuda.cu:1419-2436), which allocates, anneals

@@ -130,3 +130,46 @@ def test_snapshot_resume_is_bit_exact(tmp_path):
     assert [r.moves for r, _ in b.results()] == [r.moves for r, _ in ref.results()]
     ref.close()
     b.close()
+
+
+def escape_brute_force(n, w, W):
+    """Every support switch out of W in scan order (r1 < r2, c1, c2, new1,
+    new2 ascending) with its exact deltas, from a full int64 recompute of the
+    two changed Gram rows."""
+    M = W.reshape(n, n).T.astype(np.int64)          # row-major
+    G = M @ M.T
+    out = []
+    for r1 in range(n):
+        for r2 in range(r1 + 1, n):
+            for c1 in range(n):
+                if M[r1, c1] == 0 or M[r2, c1] != 0:
+                    continue
+                for c2 in range(n):
+                    if M[r2, c2] == 0 or M[r1, c2] != 0:
+                        continue
+                    for nv1 in (-1, 1):
+                        for nv2 in (-1, 1):
+                            N = M.copy()
+                            N[r1, c1] = 0
+                            N[r2, c2] = 0
+                            N[r1, c2] = nv1
+                            N[r2, c1] = nv2
+                            ds = dc = 0
+                            for o in range(n):
+                                if o in (r1, r2):
+                                    continue
+                                for r in (r1, r2):
+                                    old, new = G[r, o], N[r] @ N[o]
+                                    ds += int(abs(new)) - int(abs(old))
+                                    dc += int(new != 0) - int(old != 0)
+                            out.append((r1, r2, c1, c2, nv1, nv2, int(ds), int(dc)))
+    return out
+
+
+@pytest.mark.parametrize("n,w,limit", [(8, 7, 12), (10, 5, 40), (12, 3, 1000), (9, 4, 7), (12, 11, 5)])
+def test_device_escape_scan_matches_brute_force(n, w, limit):
+    W = O.random_start(n, w, 100 + n * w)
+    got = X.escape_scan(n, w, W, limit)
+    ref = escape_brute_force(n, w, W)
+    ref = sorted(enumerate(ref), key=lambda t: (t[1][6], t[1][7], t[0]))[:limit]
+    assert got == [r for _, r in ref]

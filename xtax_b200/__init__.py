@@ -136,6 +136,13 @@ class ServerStats(C.Structure):
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_CANCELLED, REQ_FAILED = 0, 1, 2, 3, 4
 SCHED_ALL, SCHED_LEAST_ATTAINED = 0, 1
 
+class EscapeMove(C.Structure):
+    """xw_escape_move: a support switch out of an elite state with its deltas."""
+    _fields_ = [("row1", C.c_int32), ("row2", C.c_int32), ("col1", C.c_int32), ("col2", C.c_int32),
+                ("new1", C.c_int32), ("new2", C.c_int32), ("score_delta", C.c_int64),
+                ("conflict_delta", C.c_int64)]
+
+
 LOG_FN = C.CFUNCTYPE(None, C.c_char_p, C.c_void_p)
 CHECKPOINT_FN = C.CFUNCTYPE(None, C.POINTER(C.c_int8), C.c_int32, C.c_void_p)
 
@@ -192,6 +199,7 @@ def lib():
             "xw_autotune": (i32, [P(JobSpec), i32, P(_Params), u64, P(i32), P(C.c_float)]),
             "xw_batch_save": (i32, [C.c_void_p, C.c_char_p]),
             "xw_batch_load": (i32, [C.c_char_p, P(_Params), P(C.c_void_p)]),
+            "xw_escape_scan": (i32, [i32, i32, P(i8), i32, P(EscapeMove), P(i32)]),
             "xw_server_config_default": (None, [P(ServerConfig)]),
             "xw_server_create": (i32, [P(ServerConfig), P(C.c_void_p)]),
             "xw_submit": (i32, [C.c_void_p, P(_Request), P(u64)]),
@@ -624,6 +632,17 @@ def autotune(jobs, params: Params, iters=2000):
     wpb, ms = C.c_int32(), C.c_float()
     _check(lib().xw_autotune(specs, len(jobs), C.byref(params.to_c()), iters, C.byref(wpb), C.byref(ms)))
     return wpb.value, ms.value
+
+
+def escape_scan(n, w, W_colmajor, limit):
+    """xw_escape_scan: the `limit` best support switches out of W, as tuples
+    (row1, row2, col1, col2, new1, new2, score_delta, conflict_delta)."""
+    W = np.ascontiguousarray(W_colmajor, dtype=np.int8).reshape(-1)
+    out = (EscapeMove * max(limit, 1))()
+    cnt = C.c_int32()
+    _check(lib().xw_escape_scan(n, w, _i8(W), limit, out, C.byref(cnt)))
+    return [(m.row1, m.row2, m.col1, m.col2, m.new1, m.new2, m.score_delta, m.conflict_delta)
+            for m in out[:cnt.value]]
 
 
 def header_symbols(path=HEADER):

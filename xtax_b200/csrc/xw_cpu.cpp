@@ -287,7 +287,7 @@ void CpuState::commit(const CpuMove& mv) {
     conflicts_ += dc;
 }
 
-std::vector<EscapeMove> escape_moves(const CpuState& e, size_t limit) {
+std::vector<EscapeMove> escape_moves_from(const CpuState& e, const std::vector<ScanResult>& scan) {
     const int n = e.order();
     const bool sparse = e.sparse_side();
     auto at = [&](int r, int c) { return (int)e.entries()[(size_t)c * n + r]; };
@@ -298,52 +298,23 @@ std::vector<EscapeMove> escape_moves(const CpuState& e, size_t limit) {
         for (int c = 0; c < n; ++c)
             if ((at(r, c) != 0) == sparse) mpos[(size_t)r * n + c] = pos++;
     }
-    const auto less = [](const EscapeMove& a, const EscapeMove& b) {
-        if (a.score_delta != b.score_delta) return a.score_delta < b.score_delta;
-        return a.conflict_delta < b.conflict_delta;
-    };
     std::vector<EscapeMove> out;
-    for (int r1 = 0; r1 < n; ++r1)
-        for (int r2 = r1 + 1; r2 < n; ++r2)
-            for (int c1 = 0; c1 < n; ++c1) {
-                const int ov1 = at(r1, c1);
-                if (ov1 == 0 || at(r2, c1) != 0) continue;
-                for (int c2 = 0; c2 < n; ++c2) {
-                    const int ov2 = at(r2, c2);
-                    if (ov2 == 0 || at(r1, c2) != 0) continue;
-                    for (int nv1 : {-1, 1})
-                        for (int nv2 : {-1, 1}) {
-                            int64_t ds = 0, dc = 0;
-                            for (int o = 0; o < n; ++o) {
-                                if (o == r1 || o == r2) continue;
-                                const int o1 = e.gram_at(r1, o), o2 = e.gram_at(r2, o);
-                                const int n1 = o1 + nv1 * at(o, c2) - ov1 * at(o, c1);
-                                const int n2 = o2 + nv2 * at(o, c1) - ov2 * at(o, c2);
-                                ds += std::abs(n1) - std::abs(o1) + std::abs(n2) - std::abs(o2);
-                                dc += (n1 != 0) - (o1 != 0) + (n2 != 0) - (o2 != 0);
-                            }
-                            EscapeMove m;
-                            m.support.kind = 1;
-                            m.support.row1 = r1;
-                            m.support.row2 = r2;
-                            m.support.col1 = c1;
-                            m.support.col2 = c2;
-                            m.support.pos1 = mpos[(size_t)r1 * n + (sparse ? c1 : c2)];
-                            m.support.pos2 = mpos[(size_t)r2 * n + (sparse ? c2 : c1)];
-                            m.flip_first = nv1 != ov1;
-                            m.flip_second = nv2 != ov2;
-                            m.score_delta = ds;
-                            m.conflict_delta = dc;
-                            out.push_back(m);
-                            if (out.size() > limit * 2) {
-                                std::nth_element(out.begin(), out.begin() + (std::ptrdiff_t)limit, out.end(), less);
-                                out.resize(limit);
-                            }
-                        }
-                }
-            }
-    std::sort(out.begin(), out.end(), less);
-    if (out.size() > limit) out.resize(limit);
+    out.reserve(scan.size());
+    for (const ScanResult& x : scan) {
+        EscapeMove m;
+        m.support.kind = 1;
+        m.support.row1 = x.row1;
+        m.support.row2 = x.row2;
+        m.support.col1 = x.col1;
+        m.support.col2 = x.col2;
+        m.support.pos1 = mpos[(size_t)x.row1 * n + (sparse ? x.col1 : x.col2)];
+        m.support.pos2 = mpos[(size_t)x.row2 * n + (sparse ? x.col2 : x.col1)];
+        m.flip_first = x.new1 != at(x.row1, x.col1);
+        m.flip_second = x.new2 != at(x.row2, x.col2);
+        m.score_delta = x.score_delta;
+        m.conflict_delta = x.conflict_delta;
+        out.push_back(m);
+    }
     return out;
 }
 

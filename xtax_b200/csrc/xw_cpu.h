@@ -80,15 +80,23 @@ private:
 };
 
 // Elite restart of a stagnant population (xweigh_cuda.cu:1817-2289, the
-// host half of run_annealer): the best support switches out of the elite
-// state (with optional sign changes), ranked by (score delta, conflict
-// delta) and truncated to `limit` as the reference does ...
+// host half of run_annealer).  A scanned support switch out of the elite
+// (rows r1 < r2, c1 moving from r1 to r2's zero... see xw_restart.cu) with
+// its new signs and exact deltas ...
+struct ScanResult {
+    int row1, row2, col1, col2, new1, new2;
+    int64_t score_delta, conflict_delta;
+};
+
+// ... as the reference's escape move: the value-preserving switch plus the
+// sign flips that give the new signs, with the minority positions of the
+// elite's lists
 struct EscapeMove {
     CpuMove support;
     bool flip_first = false, flip_second = false;
     int64_t score_delta = 0, conflict_delta = 0;
 };
-std::vector<EscapeMove> escape_moves(const CpuState& elite, size_t limit);
+std::vector<EscapeMove> escape_moves_from(const CpuState& elite, const std::vector<ScanResult>& scan);
 
 // ... and the kicked copy of the elite for restarted replica `replica`, the
 // `index`-th of `selected` this round: one escape move from the pool, then a

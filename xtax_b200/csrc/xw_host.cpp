@@ -670,7 +670,10 @@ int restart_population(Batch& b, int j, const std::vector<int8_t>& elite_best, i
     const int count = std::clamp((int)std::ceil(p.restart_fraction * available), 1, available);
     const CpuState elite = CpuState::from_entries(n, w, elite_best);
     const size_t limit = std::max<size_t>((size_t)count * 4, 1);
-    const std::vector<EscapeMove> escapes = escape_moves(elite, limit);
+    std::vector<int32_t> eg((size_t)n * n);
+    for (int a = 0; a < n; ++a)
+        for (int c = 0; c < n; ++c) eg[(size_t)a * n + c] = elite.gram_at(a, c);
+    const std::vector<EscapeMove> escapes = escape_moves_from(elite, escape_scan(n, elite_best.data(), eg.data(), limit));
     std::vector<int> selected;
     size_t scanned = 0;
     while ((int)selected.size() < count && scanned < (size_t)R * 2) {

@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "../../include/xw.h"
+#include "xw_cpu.h"
 #include "xw_kernels.h"
 
 namespace xw {
@@ -102,6 +103,11 @@ struct Batch {
     void collect(std::vector<JobOut>& out, int8_t* best_host, bool want_best);
     void fill_results(const std::vector<JobOut>& out, const int8_t* best_host, xw_job_result* res) const;
 };
+
+// The escape-move scan of an elite restart on the device (xw_restart.cu): the
+// `limit` best support switches out of the column-major W (G its Gram,
+// row-major) by (score delta, conflict delta, scan order).
+std::vector<ScanResult> escape_scan(int n, const int8_t* W, const int32_t* G, size_t limit);
 
 // Elite-restart bookkeeping of one job (the reference's restart_cursor,
 // restart_round and restarted_replicas, xweigh_cuda.cu:1812-1814).
