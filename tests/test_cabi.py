@@ -158,7 +158,8 @@ def test_ctypes_structs_match_the_c_header(tmp_path):
     structs = {"xw_params": X._Params, "xw_device_info": X._DeviceInfo, "xw_result": X._Result,
                "xw_job_spec": X.JobSpec, "xw_job_result": X.JobResult, "xw_replica_state": X.ReplicaState,
                "xw_server_config": X.ServerConfig, "xw_request": X._Request,
-               "xw_request_result": X.RequestResult, "xw_server_stats": X.ServerStats}
+               "xw_request_result": X.RequestResult, "xw_server_stats": X.ServerStats,
+               "xw_escape_move": X.EscapeMove}
     src = tmp_path / "sizes.c"
     src.write_text('#include <stdio.h>\n#include "xw.h"\nint main(void) {\n' +
                    "".join(f'    printf("%zu\\n", sizeof({k}));\n' for k in structs) + "    return 0;\n}\n")
