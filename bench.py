@@ -349,6 +349,8 @@ def ours(args):
             line["plain_kernel"] = {"unavailable": str(e)[:200]}
     if args.rescore:
         line["rescore"] = rescore_bench(torch, X)
+    if args.c1:
+        line["single_replica"] = c1_bench(X, args.c1_ref_seconds)
     if args.uneven_iters > 0:
         line["uneven"] = uneven_bench(X, args.uneven_iters)
     if args.serve_requests > 0:
@@ -430,6 +432,62 @@ def rescore_bench(torch, X):
                 pass
         out["orders"][str(n)] = entry
         del W, stats
+    return out
+
+
+# ---------------------------------------------------------------- single replicas (C1)
+C1_SEEDS = 32
+C1_MOVES = 10 ** 6
+
+
+def c1_bench(X, ref_seconds):
+    """W(12,11), one replica per search, 32 seeds: row-only fixed-degree
+    starts, the squared objective, sign flips and within-row swaps, geometric
+    cooling 4 -> 0.05 over 1e6 moves (500 moves per step), no reheat; each
+    search stops at its solve or its 1e6 moves.  All 32 run in one launch per
+    round.  Beside it, the reference's CPU xweigh, one thread, on the same
+    order and schedule (its own move set and L1 objective: the closest run the
+    reference offers)."""
+    import numpy as np
+    cooling = (0.05 / 4.0) ** (1.0 / 2000.0)
+    p = X.Params(t_init=4.0, t_min=0.05, cooling=cooling, moves_per_cool=500, stuck_threshold=2_000_000_000,
+                 objective=1, move_set=1, start_kind=1, stop_on_solve=2, moves_per_launch=100_000,
+                 max_moves=C1_MOVES)
+    jobs = [{"n": 12, "w": 11, "seed": k, "replicas": 1} for k in range(1, C1_SEEDS + 1)]
+    b = X.Batch(jobs, p)
+    b.run_timed(C1_MOVES)
+    b.synchronize()
+    ms = sum(b.launch_times())
+    res = b.results()
+    b.close()
+    moves = sum(r.moves for r, _ in res)
+    solved = [r for r, _ in res if r.solved]
+    out = {"workload": f"W(12,11) x {C1_SEEDS} seeds, 1 replica each, squared objective, flips + within-row "
+                       f"swaps, cooling 4 -> 0.05 over {C1_MOVES:.0e} moves",
+           "device": {"moves": moves, "ms": ms, "moves_per_sec": moves / (ms / 1e3),
+                      "solved": len(solved), "searches": C1_SEEDS,
+                      "median_solve_iteration": float(np.median([r.solved_iteration for r in solved]))
+                      if solved else None}}
+    if ref_seconds > 0 and os.path.exists(REF_XWEIGH):
+        mv = secs = 0.0
+        ok = runs = 0
+        t_end = time.perf_counter() + ref_seconds
+        seed = 1
+        while time.perf_counter() < t_end:
+            with tempfile.TemporaryDirectory() as td:
+                r = subprocess.run([REF_XWEIGH, "12", "11", "-t", "1", "--seed", str(seed), "--t-init", "4",
+                                    "--t-min", "0.05", "--cooling", repr(cooling), "--moves-per-cool", "500",
+                                    "--stuck-threshold", "2000000000", "--max-seconds", "2",
+                                    "-o", os.path.join(td, "w.csv")], capture_output=True, text=True, timeout=60)
+            m = re.search(r"done moves=(\d+) seconds=([0-9.e+-]+)", r.stdout)
+            if m:
+                mv += int(m.group(1))
+                secs += float(m.group(2))
+                runs += 1
+                ok += "exact verification passed" in r.stdout
+            seed += 1
+        out["reference_cpu_1thread"] = {"moves_per_sec": mv / secs if secs else None, "runs": runs, "solved": ok,
+                                        "max_seconds_per_run": 2}
     return out
 
 
@@ -641,6 +699,9 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--iters", type=int, default=ITERS, help="iterations per replica per step (profiling cases)")
     ap.add_argument("--rescore", type=int, default=1, help="also time the batched tensor-core rescoring")
+    ap.add_argument("--c1", type=int, default=1, help="also time single-replica W(12,11) searches")
+    ap.add_argument("--c1-ref-seconds", type=float, default=8.0,
+                    help="wall seconds of single-thread reference runs beside them")
     ap.add_argument("--uneven-iters", type=int, default=20000,
                     help="iterations per replica of the uneven-orders batch (0: none)")
     ap.add_argument("--serve-requests", type=int, default=400, help="requests of the serving stream (0: none)")
