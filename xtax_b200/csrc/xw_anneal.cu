@@ -291,13 +291,13 @@ __device__ __forceinline__ int flip_col_w(const Reg& r, int c, int b, int j, int
 // legal) branch into out-of-line code.  Move set 1 replaces the switch by
 // the within-row swap and has no double flips.  The result equals the
 // sequential reference order of draws and tests.
-template <int MW>
+template <int MW, bool GEN>
 __device__ __forceinline__ uint2 d_propose(const Reg& r, const View* v, int c, bool coop_ok, int coop_row) {
     const int n = r.n, m = r.m;
     const uint64_t it = r.it;
     const bool targeted = (uint64_t)r.word(c, 0, 0) < r.thr_target;
     const int row = targeted ? (coop_ok ? coop_row : d_hot_row(v, it, c)) : (int)r.index(c, 0, 1, (uint32_t)n);
-    const bool want_dbl = r.move_set == 0 && (uint64_t)r.word(c, 0, 2) < r.thr_dbl;
+    const bool want_dbl = (!GEN || r.move_set == 0) && (uint64_t)r.word(c, 0, 2) < r.thr_dbl;
     const bool want_flip = r.w == n || (uint64_t)r.word(c, 0, 3) < r.thr_sign;
 
     // double flip, attempt 0: first flip (2,3), second row/flip from block 3
@@ -315,7 +315,7 @@ __device__ __forceinline__ uint2 d_propose(const Reg& r, const View* v, int c, b
         if (mv.x) return mv;
     }
     if (want_flip) return fcol < 0 ? make_uint2(0u, 0u) : pack(0, row, 0, fcol, 0, 0, 0, 0, 0);
-    if (r.move_set == 1) {
+    if (GEN && r.move_set == 1) {
         mv = d_row_swap<MW>(v, it, c, row);
     } else {
         // support switch, attempt 0 (blocks 1 and 2)
@@ -383,12 +383,17 @@ struct Deltas {
     int ds, dc, dsq, dpar;
 };
 
+// GEN: the general kernel, whose replicas may use the squared or parity
+// objective; the lean one tracks the L1 score and conflicts only
+template <bool GEN>
 __device__ __forceinline__ void acc(Deltas& d, int old, int nw) {
     const int ao = iabs(old), an = iabs(nw);
     d.ds += an - ao;
     d.dc += (nw != 0) - (old != 0);
-    d.dsq += nw * nw - old * old;
-    d.dpar += (an & 1) - (ao & 1);
+    if (GEN) {
+        d.dsq += nw * nw - old * old;
+        d.dpar += (an & 1) - (ao & 1);
+    }
 }
 
 // the pair entry G[r1][r2] after a double flip over rows r1 != r2
@@ -399,7 +404,7 @@ __device__ __forceinline__ int pair_new(const Update& u, int op, const int8_t* W
 
 // evaluate_move_warp (xweigh_cuda.cu:449-599): lane-partial deltas over the
 // lane's own rows; the caller reduces them across the warp.
-template <int OPL, typename GT>
+template <int OPL, typename GT, bool GEN>
 __device__ __forceinline__ Deltas eval_lane(const Update& u, const int8_t* W, const GT* G, int n, int ld,
                                             int lane) {
     Deltas d = {0, 0, 0, 0};
@@ -408,23 +413,23 @@ __device__ __forceinline__ Deltas eval_lane(const Update& u, const int8_t* W, co
         const int o = lane + 32 * k;
         if (o < n && o != u.R1 && o != u.R2) {
             const int o1 = G[u.R1 * ld + o];
-            acc(d, o1, o1 + u.A1 * W[u.X1 * n + o] + u.B1 * W[u.Y1 * n + o]);
+            acc<GEN>(d, o1, o1 + u.A1 * W[u.X1 * n + o] + u.B1 * W[u.Y1 * n + o]);
             if (u.R2 >= 0) {
                 const int o2 = G[u.R2 * ld + o];
-                acc(d, o2, o2 + u.A2 * W[u.X2 * n + o] + u.B2 * W[u.Y2 * n + o]);
+                acc<GEN>(d, o2, o2 + u.A2 * W[u.X2 * n + o] + u.B2 * W[u.Y2 * n + o]);
             }
         }
     }
     if (u.pair && lane == 0) {
         const int op = G[u.R1 * ld + u.R2];
-        acc(d, op, pair_new(u, op, W, n, u.X1, u.X2));
+        acc<GEN>(d, op, pair_new(u, op, W, n, u.X1, u.X2));
     }
     return d;
 }
 
 // commit_sign_flip / commit_support_switch / commit_double_sign_flip
 // (xweigh_cuda.cu:607-877) and the within-row swap, in the two-row form.
-template <int OPL, int MW, typename GT>
+template <int OPL, int MW, typename GT, bool GEN>
 __device__ void commit(uint32_t d0, uint32_t d1, const Update& u, int ds, int8_t* W, GT* G, int32_t* res,
                        uint8_t* mino, uint64_t* mask, int n, int ld, int m, int sparse, int lane) {
     int s1 = 0;
@@ -486,7 +491,7 @@ __device__ void commit(uint32_t d0, uint32_t d1, const Update& u, int ds, int8_t
             mask[MW * r1 + (c2 >> 6)] |= 1ull << (c2 & 63);
             mask[MW * r2 + (c2 >> 6)] &= ~(1ull << (c2 & 63));
             mask[MW * r2 + (c1 >> 6)] |= 1ull << (c1 & 63);
-        } else {
+        } else if (GEN) {
             W[c1 * n + r1] = 0;
             W[c2 * n + r1] = (int8_t)nv1;
             mino[r1 * m + p1] = (uint8_t)(sparse ? c2 : c1);
@@ -524,7 +529,7 @@ __device__ __forceinline__ uint64_t globaltimer() {
     return t;
 }
 
-template <int OPL>
+template <int OPL, bool GEN>
 __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int lane) {
     uint8_t* rec = a.arena + a.rec_off[rid];
     RepHeader* H = reinterpret_cast<RepHeader*>(rec);
@@ -625,7 +630,12 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
     const int par0 = __reduce_add_sync(FULL, p_par) / 2;
     __syncwarp();
 
-    const int obj_kind = H->obj_kind;
+    const int obj_kind = GEN ? H->obj_kind : 0;
+    if (!GEN && (H->obj_kind != 0 || J->move_set != 0)) {
+        // the lean kernel was launched for a replica that needs the general one
+        if (lane == 0) H->err |= XW_ERR_KERNEL;
+        return;
+    }
     const int64_t obj0 = obj_kind == 1 ? sq0 : obj_kind == 2 ? par0 : score0;
     int score, conflicts, best_s, best_c, msi, cool;
     int64_t obj_total;
@@ -734,7 +744,7 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
         // D: proposals, lane c proposes candidate c
         uint2 desc = make_uint2(0u, 0u);
         rg.it = it;
-        if (lane < count) desc = d_propose<MW>(rg, sView, lane, coop && lane < 4, coop_row);
+        if (lane < count) desc = d_propose<MW, GEN>(rg, sView, lane, coop && lane < 4, coop_row);
         __syncwarp();
 
         // E: evaluate in candidate order, keep the first best
@@ -747,13 +757,15 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
             const uint32_t e1 = __shfl_sync(FULL, desc.y, c);
             if (!(e0 & 1u)) continue;
             const Update u = decode(e0, e1, sW, n);
-            const Deltas d = eval_lane<OPL, GT>(u, sW, sG, n, ld, lane);
+            const Deltas d = eval_lane<OPL, GT, GEN>(u, sW, sG, n, ld, lane);
             const int packed = __reduce_add_sync(FULL, d.ds * 4096 + d.dc);
             const int dc = ((packed + 2048) & 4095) - 2048;
             const int ds = (packed - dc) >> 12;
             int prim = ds;
-            if (obj_kind == 1) prim = __reduce_add_sync(FULL, d.dsq);
-            else if (obj_kind == 2) prim = __reduce_add_sync(FULL, d.dpar);
+            if (GEN) {
+                if (obj_kind == 1) prim = __reduce_add_sync(FULL, d.dsq);
+                else if (obj_kind == 2) prim = __reduce_add_sync(FULL, d.dpar);
+            }
             ++cand_evals;
             bool better = !have;
             if (!better) {
@@ -780,7 +792,7 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
         // G: commit
         if (accept) {
             const Update u = decode(b0, b1, sW, n);
-            commit<OPL, MW, GT>(b0, b1, u, bds, sW, sG, sRes, sMino, sMask, n, ld, m, sparse, lane);
+            commit<OPL, MW, GT, GEN>(b0, b1, u, bds, sW, sG, sRes, sMino, sMask, n, ld, m, sparse, lane);
             score += bds;
             conflicts += bdc;
             obj_total += bprim;
@@ -846,7 +858,7 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
 #ifndef XW_ANNEAL_MAXNREG
 #define XW_ANNEAL_MAXNREG 128
 #endif
-template <int OPL>
+template <int OPL, bool GEN>
 __global__ void __maxnreg__(XW_ANNEAL_MAXNREG) anneal_kernel(AnnealArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int lane = threadIdx.x & 31;
@@ -857,7 +869,7 @@ __global__ void __maxnreg__(XW_ANNEAL_MAXNREG) anneal_kernel(AnnealArgs a) {
         if (lane == 0) item = atomicAdd(a.counter, 1u);
         item = __shfl_sync(FULL, item, 0);
         if (item >= a.n_items) break;
-        run_replica<OPL>(a, a.items[item], slot, lane);
+        run_replica<OPL, GEN>(a, a.items[item], slot, lane);
     }
 }
 
@@ -985,21 +997,25 @@ uint32_t anneal_slot_bytes(int n, int m, int opl) { return slot_layout(n, m, opl
 
 int anneal_opl(int n) { return n <= 32 ? 1 : n <= 64 ? 2 : n <= 128 ? 4 : 8; }
 
-const void* anneal_kernel_fn(int opl) {
-    if (opl == 1) return reinterpret_cast<const void*>(&anneal_kernel<1>);
-    if (opl == 2) return reinterpret_cast<const void*>(&anneal_kernel<2>);
-    if (opl == 4) return reinterpret_cast<const void*>(&anneal_kernel<4>);
-    return reinterpret_cast<const void*>(&anneal_kernel<8>);
+const void* anneal_kernel_fn(int opl, bool general) {
+    if (general) {
+        if (opl == 1) return reinterpret_cast<const void*>(&anneal_kernel<1, true>);
+        if (opl == 2) return reinterpret_cast<const void*>(&anneal_kernel<2, true>);
+        if (opl == 4) return reinterpret_cast<const void*>(&anneal_kernel<4, true>);
+        return reinterpret_cast<const void*>(&anneal_kernel<8, true>);
+    }
+    if (opl == 1) return reinterpret_cast<const void*>(&anneal_kernel<1, false>);
+    if (opl == 2) return reinterpret_cast<const void*>(&anneal_kernel<2, false>);
+    if (opl == 4) return reinterpret_cast<const void*>(&anneal_kernel<4, false>);
+    return reinterpret_cast<const void*>(&anneal_kernel<8, false>);
 }
 
-cudaError_t launch_anneal(const AnnealArgs& args, int opl, int warps_per_block, int blocks, cudaStream_t stream) {
+cudaError_t launch_anneal(const AnnealArgs& args, int opl, bool general, int warps_per_block, int blocks,
+                          cudaStream_t stream) {
     const size_t smem = (size_t)warps_per_block * args.slot_bytes;
     const dim3 grid(blocks), block(32 * warps_per_block);
-    if (opl == 1) anneal_kernel<1><<<grid, block, smem, stream>>>(args);
-    else if (opl == 2) anneal_kernel<2><<<grid, block, smem, stream>>>(args);
-    else if (opl == 4) anneal_kernel<4><<<grid, block, smem, stream>>>(args);
-    else anneal_kernel<8><<<grid, block, smem, stream>>>(args);
-    return cudaGetLastError();
+    void* kargs[] = {const_cast<AnnealArgs*>(&args)};
+    return cudaLaunchKernel(anneal_kernel_fn(opl, general), grid, block, kargs, smem, stream);
 }
 
 cudaError_t launch_exchange(XwJob* jobs, int njobs, uint8_t* arena, const uint64_t* rec_off, const double* ladder,

@@ -62,8 +62,8 @@ uint64_t coin_threshold(double p) {
 }
 
 template <typename F>
-void parallel_for(int count, F f) {
-    const int threads = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(), count / 16 + 1));
+void parallel_for(int count, F f, int grain = 16) {
+    const int threads = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(), count / grain + 1));
     if (threads <= 1) {
         for (int i = 0; i < count; ++i) f(i);
         return;
@@ -93,6 +93,12 @@ void parallel_for(int count, F f) {
 namespace xw {
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+bool needs_general_kernel(const xw_params& p) {
+    if (p.move_set != 0) return true;
+    if (p.objective == 1 || p.objective == 2) return true;
+    return p.objective == -1 && (p.squared_objective_fraction > 0.0 || p.parity_objective_fraction > 0.0);
+}
 
 std::string strfmt(const char* f, ...) {
     char buf[1024];
@@ -188,6 +194,7 @@ void prepare_job(const xw_job_spec& s, const xw_params& p, const int8_t* starts,
     J.moves_per_cool = p.moves_per_cool;
     J.stuck_threshold = p.stuck_threshold;
     J.objective = p.objective;
+    J.general = needs_general_kernel(p) ? 1 : 0;
     J.replicas = s.replicas;
     // the Philox key follows the reference's curand seed derivation
     // (xweigh_cuda.cu:1724-1727)
@@ -290,21 +297,32 @@ void Batch::build(const xw_job_spec* specs, int njobs, const xw_params& p, const
     ladder.clear();
     rec_off.clear();
     uint32_t rep = 0;
-    size_t start_off = 0;
-    std::vector<uint8_t> records;
-    std::vector<double> temps;
+    // jobs are built in parallel across jobs when there are enough of them,
+    // else each job builds its replicas' starts in parallel
+    std::vector<size_t> start_at((size_t)njobs, 0);
+    for (int j = 1; j < njobs; ++j)
+        start_at[j] = start_at[j - 1] + (size_t)specs[j - 1].replicas * specs[j - 1].n * specs[j - 1].n;
+    std::vector<std::vector<uint8_t>> records((size_t)njobs);
+    std::vector<std::vector<double>> temps((size_t)njobs);
+    const bool across = njobs >= (int)std::max(2u, std::thread::hardware_concurrency());
+    auto build_job = [&](int j) {
+        prepare_job(specs[j], p, starts ? starts + start_at[j] : nullptr, (uint32_t)j, !across, jobs[j], records[j],
+                    temps[j], t_init_used[j]);
+    };
+    if (across) {
+        parallel_for(njobs, build_job, 1);
+    } else {
+        for (int j = 0; j < njobs; ++j) build_job(j);
+    }
     for (int j = 0; j < njobs; ++j) {
         const xw_job_spec& s = specs[j];
         XwJob& J = jobs[j];
-        prepare_job(s, p, starts ? starts + start_off : nullptr, (uint32_t)j, true, J, records, temps,
-                    t_init_used[j]);
-        if (starts) start_off += (size_t)s.replicas * s.n * s.n;
         J.rep_begin = rep;
         J.ladder_off = ladder.size();
-        if (tempering) ladder.insert(ladder.end(), temps.begin(), temps.end());
+        if (tempering) ladder.insert(ladder.end(), temps[j].begin(), temps[j].end());
         rep_seed[j] = (uint32_t)s.seed;
         for (int r = 0; r < s.replicas; ++r) rec_off.push_back(host.size() + (size_t)r * J.record_bytes);
-        host.insert(host.end(), records.begin(), records.end());
+        host.insert(host.end(), records[j].begin(), records[j].end());
         rep += (uint32_t)s.replicas;
     }
     if (ladder.empty()) ladder.push_back(0.0);
@@ -320,6 +338,7 @@ void Batch::derive_layout() {
     best_offsets.assign(njobs, 0);
     size_t best_off = 0;
     opl = 1;
+    general = false;
     slot_bytes = 0;
     for (int j = 0; j < njobs; ++j) {
         const XwJob& J = jobs[j];
@@ -327,6 +346,7 @@ void Batch::derive_layout() {
         best_offsets[j] = best_off;
         best_off += (size_t)J.n * J.n;
         opl = std::max(opl, anneal_opl(J.n));
+        general = general || J.general != 0;
     }
     // one launch runs every replica with the widest class's kernel and layout
     for (int j = 0; j < njobs; ++j) slot_bytes = std::max(slot_bytes, anneal_slot_bytes(jobs[j].n, jobs[j].m, opl));
@@ -489,7 +509,7 @@ void Batch::load(const std::string& path, const xw_params* over) {
 }
 
 void Batch::configure_shape(int wpb) {
-    const void* fn = anneal_kernel_fn(opl);
+    const void* fn = anneal_kernel_fn(opl, general);
     int optin = 0;
     check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, params.device),
           "cudaDeviceGetAttribute max opt-in shared memory");
@@ -566,7 +586,7 @@ void Batch::enqueue_rounds(uint64_t iters, bool timed) {
         a.pad = 0;
         left -= a.iters;
         if (timed) check(cudaEventRecord(events[2 * k], stream), "cudaEventRecord");
-        check(launch_anneal(a, opl, warps_per_block, blocks, stream), "launch anneal_kernel");
+        check(launch_anneal(a, opl, general, warps_per_block, blocks, stream), "launch anneal_kernel");
         if (timed) check(cudaEventRecord(events[2 * k + 1], stream), "cudaEventRecord");
         if (tempering)
             check(launch_exchange(static_cast<XwJob*>(d_jobs), (int)jobs.size(), static_cast<uint8_t*>(d_arena),
@@ -1223,7 +1243,7 @@ int32_t xw_run(int32_t n, int32_t w, const xw_params* pin, const int8_t* start, 
             // one resident wave: warp slots per SM times SMs
             const int wpb = p.warps_per_block > 0 ? p.warps_per_block : 4;
             int per_sm = 0;
-            const void* fn = anneal_kernel_fn(anneal_opl(n));
+            const void* fn = anneal_kernel_fn(anneal_opl(n), needs_general_kernel(p));
             cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(wpb * slot));
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * wpb, (size_t)wpb * slot);
             replicas = std::max(1, per_sm * wpb * out->device.multiprocessors);

@@ -13,6 +13,9 @@
 namespace xw {
 
 std::string validate(int n, int w, const xw_params& p);
+// the parameters need the general anneal kernel: the squared or parity
+// objective on some replica, or the within-row swap move set
+bool needs_general_kernel(const xw_params& p);
 void set_last_error(const std::string& msg);
 std::string strfmt(const char* f, ...);
 // throws std::runtime_error naming `what` when e is an error
@@ -57,6 +60,7 @@ struct Batch {
     bool tempering = false;
 
     int opl = 1;
+    bool general = false;      // some job needs the general kernel
     uint32_t slot_bytes = 0;
     int warps_per_block = 4;
     int blocks_per_sm = 1;

@@ -29,8 +29,11 @@ struct AnnealArgs {
 uint32_t anneal_slot_bytes(int n, int m, int opl);
 // lanes' rows per lane: 1 for n <= 32, 2 for n <= 64, 4 for n <= 128, 8 for n <= 256
 int anneal_opl(int n);
-const void* anneal_kernel_fn(int opl);
-cudaError_t launch_anneal(const AnnealArgs& args, int opl, int warps_per_block, int blocks,
+// `general`: some replica of the launch uses the squared or parity objective
+// or the within-row swap move set; otherwise the lean kernel (L1 score,
+// the reference's moves) runs, which drops that work from the hot loop
+const void* anneal_kernel_fn(int opl, bool general);
+cudaError_t launch_anneal(const AnnealArgs& args, int opl, bool general, int warps_per_block, int blocks,
                           cudaStream_t stream);
 cudaError_t launch_exchange(XwJob* jobs, int njobs, uint8_t* arena, const uint64_t* rec_off,
                             const double* ladder, int stop_on_solve, cudaStream_t stream);

@@ -25,6 +25,7 @@
 #define XW_STATUS_SOLVED 2u    // best score reached 0
 #define XW_ERR_SCORE 1u        // rebuilt score differs from the tracked one
 #define XW_ERR_MINORITY 2u     // W row weights disagree with the minority lists
+#define XW_ERR_KERNEL 4u       // a lean launch met a replica that needs the general kernel
 
 struct XwJob {
     int32_t n, w, m, sparse;        // m = min(w, n-w); sparse = (w <= n-w)
@@ -38,7 +39,7 @@ struct XwJob {
     uint32_t rep_begin;             // first replica id of the job
     uint32_t record_bytes;
     uint32_t off_w, off_best, off_mino;
-    uint32_t pad0;
+    int32_t general;                // needs the general kernel (objectives, move set 1)
     uint64_t thr_greedy, thr_target, thr_double, thr_sign, thr_swsign;
     double t_min, cooling, reheat;
     uint64_t budget_iters;          // per-replica iteration cap, 0 = none

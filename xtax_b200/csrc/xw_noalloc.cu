@@ -182,10 +182,11 @@ extern "C" int32_t xw_anneal_noalloc(int32_t n, int32_t w, const xw_params* p, i
     if (e != cudaSuccess) return nfail(XW_ERR_CUDA, std::string("cudaGetDevice failed: ") + cudaGetErrorString(e));
     if (dev < 0 || dev >= kMaxDevices) return nfail(XW_ERR_INVALID, "xw_anneal_noalloc: device ordinal too large");
 
+    const bool job_general = needs_general_kernel(*p);
     const int opl = anneal_opl(n);
     const uint32_t slot = anneal_slot_bytes(n, m, opl);
     const int wpb = p->warps_per_block > 0 ? p->warps_per_block : 4;
-    const void* fn = anneal_kernel_fn(opl);
+    const void* fn = anneal_kernel_fn(opl, job_general);
     unsigned char* scratch = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_setup_mu);
@@ -223,6 +224,7 @@ extern "C" int32_t xw_anneal_noalloc(int32_t n, int32_t w, const xw_params* p, i
     job.moves_per_cool = p->moves_per_cool;
     job.stuck_threshold = p->stuck_threshold;
     job.objective = p->objective;
+    job.general = needs_general_kernel(*p) ? 1 : 0;
     job.replicas = replicas;
     const uint32_t base = (uint32_t)p->seed;
     const uint64_t key = ((uint64_t)base << 32) ^ p->seed ^ 0xd1b54a32d192ed03ull;
@@ -269,7 +271,7 @@ extern "C" int32_t xw_anneal_noalloc(int32_t n, int32_t w, const xw_params* p, i
         a.stop_on_solve = p->stop_on_solve;
         a.pad = 0;
         left -= a.iters;
-        e = launch_anneal(a, opl, wpb, blocks, stream);
+        e = launch_anneal(a, opl, job_general, wpb, blocks, stream);
         if (e != cudaSuccess) return nfail(XW_ERR_CUDA, std::string("anneal launch failed: ") + cudaGetErrorString(e));
         if (job.tempering) {
             e = launch_exchange(a.jobs, 1, scratch, a.rec_off, reinterpret_cast<const double*>(scratch + L.off_ladder),

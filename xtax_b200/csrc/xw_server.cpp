@@ -171,6 +171,7 @@ struct Server {
     bool items_dirty = true;
     std::vector<uint32_t> items_host[kClasses];
     uint32_t class_slot[kClasses] = {};
+    bool class_general[kClasses] = {};
     std::map<std::pair<int, uint32_t>, int> per_sm_cache;
     int last_njobs = 0;
 
@@ -186,7 +187,7 @@ struct Server {
     void place(const ReqPtr& q);
     void select_round();
     void rebuild_items();
-    int blocks_for(int cls, uint32_t slot_bytes, int wpb, size_t items);
+    int blocks_for(int cls, bool general, uint32_t slot_bytes, int wpb, size_t items);
     void round(bool& any_tempering);
     void retire(const ReqPtr& q, const JobOut& o, double t_host, uint64_t stamp, int state);
     void finish_locked(const ReqPtr& q, int state);
@@ -383,12 +384,14 @@ void Server::rebuild_items() {
     for (int c = 0; c < kClasses; ++c) {
         items_host[c].clear();
         class_slot[c] = 0;
+        class_general[c] = false;
     }
     for (int s : order) {
         const ReqPtr& q = slot_req[s];
         const int c = class_of(q->spec.n);
         for (int r = 0; r < q->spec.replicas; ++r) items_host[c].push_back((uint32_t)(q->rep_begin + r));
         class_slot[c] = std::max(class_slot[c], anneal_slot_bytes(q->spec.n, q->job.m, opl_of_class(c)));
+        class_general[c] = class_general[c] || q->job.general != 0;
     }
     for (int c = 0; c < kClasses; ++c)
         if (!items_host[c].empty())
@@ -398,12 +401,12 @@ void Server::rebuild_items() {
     items_dirty = false;
 }
 
-int Server::blocks_for(int cls, uint32_t slot_bytes, int wpb, size_t items) {
-    const auto key = std::make_pair(cls * 64 + wpb, slot_bytes);
+int Server::blocks_for(int cls, bool general, uint32_t slot_bytes, int wpb, size_t items) {
+    const auto key = std::make_pair((cls * 64 + wpb) * 2 + (general ? 1 : 0), slot_bytes);
     auto it = per_sm_cache.find(key);
     int per_sm = 0;
     if (it == per_sm_cache.end()) {
-        check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, anneal_kernel_fn(opl_of_class(cls)),
+        check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, anneal_kernel_fn(opl_of_class(cls), general),
                                                                  32 * wpb, (size_t)wpb * slot_bytes),
                    "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
         per_sm_cache[key] = per_sm;
@@ -448,7 +451,8 @@ void Server::round(bool& any_tempering) {
         a.iters = (uint64_t)cfg.quantum_iters;
         a.stop_on_solve = 2;
         a.pad = 0;
-        check_cuda(launch_anneal(a, opl_of_class(c), wpb, blocks_for(c, class_slot[c], wpb, items_host[c].size()),
+        check_cuda(launch_anneal(a, opl_of_class(c), class_general[c], wpb,
+                                 blocks_for(c, class_general[c], class_slot[c], wpb, items_host[c].size()),
                                  st),
                    "launch anneal_kernel");
         if (nclass > 1) {
@@ -614,16 +618,17 @@ void Server::start() {
     check_cuda(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, cfg.device),
                "cudaDeviceGetAttribute max opt-in shared memory");
     for (int c = 0; c < kClasses; ++c)
-        check_cuda(cudaFuncSetAttribute(anneal_kernel_fn(opl_of_class(c)),
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, optin),
-                   "cudaFuncSetAttribute max dynamic shared memory");
+        for (bool general : {false, true})
+            check_cuda(cudaFuncSetAttribute(anneal_kernel_fn(opl_of_class(c), general),
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, optin),
+                       "cudaFuncSetAttribute max dynamic shared memory");
     if (cfg.max_active_replicas <= 0) {
         // four waves of the resident warps at the order-32 slot: enough work
         // per round to keep every SM busy through the round's tail
         int per_sm = 0;
         const int wpb = cfg.warps_per_block > 0 ? cfg.warps_per_block : 4;
         const uint32_t slot = anneal_slot_bytes(32, 16, 1);
-        check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, anneal_kernel_fn(1), 32 * wpb,
+        check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, anneal_kernel_fn(1, false), 32 * wpb,
                                                                  (size_t)wpb * slot),
                    "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
         cfg.max_active_replicas = std::max(256, 4 * per_sm * wpb * sms);
