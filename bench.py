@@ -70,12 +70,12 @@ def run_reference_cpu(seconds, threads, seed=1):
     return int(m.group(1)), float(m.group(2))
 
 
-def run_reference_cuda(seconds, seed=1):
+def run_reference_cuda(seconds, seed=1, n=N_ORDER, w=W_WEIGHT, replicas=INSTANCES * RUNGS):
     """The reference xweigh_cuda (the plain kernel, one instance per launch)
-    on the same shape: 4096 replicas of W(26,25)."""
+    on the same shape: by default 4096 replicas of W(26,25)."""
     with tempfile.TemporaryDirectory() as td:
         out = subprocess.run(
-            [REF_XWEIGH_CUDA, str(N_ORDER), str(W_WEIGHT), "--replicas", str(INSTANCES * RUNGS),
+            [REF_XWEIGH_CUDA, str(n), str(w), "--replicas", str(replicas),
              "--t-init", str(T_MAX), "--t-min", str(T_MIN), "--seed", str(seed), "--max-seconds", str(seconds),
              "--restart-interval", "0", "-o", os.path.join(td, "w.csv")],
             capture_output=True, text=True, timeout=seconds * 4 + 120)
@@ -353,6 +353,8 @@ def ours(args):
         line["single_replica"] = c1_bench(X, args.c1_ref_seconds)
     if args.uneven_iters > 0:
         line["uneven"] = uneven_bench(X, args.uneven_iters)
+    if args.large_iters > 0:
+        line["large_order"] = large_bench(X, args.large_iters, args.large_ref_seconds)
     if args.serve_requests > 0:
         line["serving"] = serving_bench(X, args.serve_requests, args.serve_plain, args.serve_quantum,
                                         args.serve_reference, args.serve_reference_cap)
@@ -488,6 +490,43 @@ def c1_bench(X, ref_seconds):
             seed += 1
         out["reference_cpu_1thread"] = {"moves_per_sec": mv / secs if secs else None, "runs": runs, "solved": ok,
                                         "max_seconds_per_run": 2}
+    return out
+
+
+# ---------------------------------------------------------------- orders beyond shared memory
+LARGE_N, LARGE_W, LARGE_R = 276, 275, 2368
+
+
+def large_bench(X, iters, ref_seconds):
+    """W(276,275) with 2368 replicas (16 warps on each of 148 SMs) and the
+    reference's defaults otherwise (t_init 6, t_min 0.1, cooling and reheat,
+    no restarts).  276 is about the largest order whose state the reference's
+    kernel holds in one CTA's shared memory; here it runs on the HBM-resident
+    kernel.  Beside it the reference's xweigh_cuda on the same order and
+    replica count."""
+    p = X.Params(stop_on_solve=0, t_init=6.0, t_min=0.1, moves_per_launch=1000,
+                 squared_objective_fraction=0.0, parity_objective_fraction=0.0)
+    b = X.Batch([{"n": LARGE_N, "w": LARGE_W, "seed": 1, "replicas": LARGE_R}], p)
+    b.run(1000)          # the first launch builds each replica's Gram arena
+    b.synchronize()
+    m0 = b.results()[0][0].moves
+    b.run_timed(iters)
+    b.synchronize()
+    ms = sum(b.launch_times())
+    r = b.results()[0][0]
+    b.close()
+    moves = r.moves - m0
+    out = {"workload": f"W({LARGE_N},{LARGE_W}) x {LARGE_R} replicas, cooling from T 6 (t_min 0.1), L1 objective, "
+                       f"the reference's moves, {iters} iterations per replica",
+           "device": {"moves": moves, "ms": ms, "moves_per_sec": moves / (ms / 1e3), "error": r.error,
+                      "kernel": "anneal_large_kernel (replica state in HBM)"}}
+    if ref_seconds > 0 and os.path.exists(REF_XWEIGH_CUDA):
+        try:
+            mv, secs = run_reference_cuda(ref_seconds, n=LARGE_N, w=LARGE_W, replicas=LARGE_R)
+            out["reference_xweigh_cuda"] = {"moves_per_sec": mv / secs, "sample_seconds": ref_seconds,
+                                            "impl": "reference xweigh_cuda (sm_100a build), shared-memory state"}
+        except Exception as e:  # noqa: BLE001 - report, do not fail the bench
+            out["reference_xweigh_cuda"] = {"unavailable": str(e)[:200]}
     return out
 
 
@@ -704,6 +743,10 @@ def main():
                     help="wall seconds of single-thread reference runs beside them")
     ap.add_argument("--uneven-iters", type=int, default=20000,
                     help="iterations per replica of the uneven-orders batch (0: none)")
+    ap.add_argument("--large-iters", type=int, default=4000,
+                    help="iterations per replica of the W(276,275) large-order section (0: none)")
+    ap.add_argument("--large-ref-seconds", type=float, default=10.0,
+                    help="seconds of the reference's xweigh_cuda on that order")
     ap.add_argument("--serve-requests", type=int, default=400, help="requests of the serving stream (0: none)")
     ap.add_argument("--serve-plain", type=int, default=60,
                     help="prefix of the stream also run one request at a time")

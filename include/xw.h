@@ -32,7 +32,12 @@ extern "C" {
 #define XW_ERR_TIMEOUT 6   /* a wait ended before the request finished */
 #define XW_ERR_IO 7        /* file read or write failed */
 
-#define XW_MAX_ORDER_CUDA 256       /* largest n the device path anneals */
+#define XW_MAX_ORDER_CUDA 1024      /* largest n the device path anneals */
+#define XW_MAX_ORDER_SHARED 256     /* largest n whose replica state sits in shared memory; larger
+                                       orders keep it in HBM (no counterpart in the reference,
+                                       whose kernel stops where shared memory ends, about n = 276).
+                                       Also the limit of the server, the rescoring kernel and
+                                       xw_anneal_noalloc. */
 #define XW_MAX_CANDIDATE_SAMPLES 32 /* xweigh_cuda.hpp:11 */
 #define XW_MAX_TARGET_SAMPLES 64    /* xweigh_cuda.hpp:12 */
 
@@ -222,7 +227,8 @@ typedef struct xw_replica_state {
 } xw_replica_state;
 
 /* Read replica `replica` of job `job`: state, current W, best W (n*n each,
- * nullable) and the minority lists (n*min(w,n-w) bytes, nullable). */
+ * nullable) and the minority lists (n*min(w,n-w) entries, nullable: one
+ * byte each for n <= XW_MAX_ORDER_SHARED, a native-endian uint16 each above). */
 int32_t xw_batch_read_replica(xw_batch* b, int32_t job, int32_t replica, xw_replica_state* st,
                               int8_t* W, int8_t* best_W, uint8_t* minority);
 

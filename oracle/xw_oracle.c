@@ -1055,12 +1055,12 @@ int64_t xwo_rep_run(xwo_replica* r, int64_t iters, int stop_on_solve) {
 }
 
 void xwo_rep_get(const xwo_replica* r, xwo_replica_scalars* s, int8_t* W, int8_t* best_W,
-                 uint8_t* minority, int32_t* G, int32_t* residual) {
+                 uint16_t* minority, int32_t* G, int32_t* residual) {
     const int n = r->n;
     if (s) *s = r->s;
     if (W) memcpy(W, r->W, (size_t)n * n);
     if (best_W) memcpy(best_W, r->bestW, (size_t)n * n);
-    if (minority) for (int i = 0; i < n * r->m; ++i) minority[i] = (uint8_t)r->mino[i];
+    if (minority) memcpy(minority, r->mino, sizeof(uint16_t) * n * r->m);
     if (G) memcpy(G, r->G, sizeof(int32_t) * n * n);
     if (residual) for (int i = 0; i < n; ++i) residual[i] = (int32_t)r->res[i];
 }

@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define XWO_MAX_N 256
+#define XWO_MAX_N 1024
 
 /* ---- random streams ---------------------------------------------------- */
 void xwo_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
@@ -109,7 +109,7 @@ void xwo_rep_destroy(xwo_replica* r);
  * stop_on_solve; returns iterations run */
 int64_t xwo_rep_run(xwo_replica* r, int64_t iters, int stop_on_solve);
 void xwo_rep_get(const xwo_replica* r, xwo_replica_scalars* s, int8_t* W,
-                 int8_t* best_W, uint8_t* minority, int32_t* G, int32_t* residual);
+                 int8_t* best_W, uint16_t* minority, int32_t* G, int32_t* residual);
 void xwo_rep_set_temperature(xwo_replica* r, double t, int32_t rung);
 /* incremental state vs full recompute: 0 when consistent */
 int xwo_rep_check(const xwo_replica* r);

@@ -82,7 +82,7 @@ def lib():
         L.xwo_rep_run.argtypes = [C.c_void_p, C.c_int64, C.c_int]
         L.xwo_rep_run.restype = C.c_int64
         L.xwo_rep_get.argtypes = [C.c_void_p, P(RepScalars), P(C.c_int8), P(C.c_int8),
-                                  P(C.c_uint8), P(C.c_int32), P(C.c_int32)]
+                                  P(C.c_uint16), P(C.c_int32), P(C.c_int32)]
         L.xwo_rep_set_temperature.argtypes = [C.c_void_p, C.c_double, C.c_int32]
         L.xwo_rep_check.argtypes = [C.c_void_p]
         L.xwo_rep_check.restype = C.c_int
@@ -214,11 +214,11 @@ class Replica:
         s = RepScalars()
         W = np.zeros(n * n, dtype=np.int8)
         B = np.zeros(n * n, dtype=np.int8)
-        M = np.zeros(max(n * m, 1), dtype=np.uint8)
+        M = np.zeros(max(n * m, 1), dtype=np.uint16)
         G = np.zeros(n * n, dtype=np.int32)
         R = np.zeros(n, dtype=np.int32)
         lib().xwo_rep_get(self.h, C.byref(s), ptr(W, C.c_int8), ptr(B, C.c_int8),
-                          ptr(M, C.c_uint8), ptr(G, C.c_int32), ptr(R, C.c_int32))
+                          ptr(M, C.c_uint16), ptr(G, C.c_int32), ptr(R, C.c_int32))
         return s, W, B, M[: n * m], G.reshape(n, n), R
 
 

@@ -1,0 +1,165 @@
+"""The HBM-resident kernel for orders above the shared-memory classes.
+
+Its replicas follow the same draw layout and move rules as the shared-memory
+kernel, so the CPU oracle replays them bit for bit: W, best W, minority
+lists, counters, scores, temperature.  XW_LARGE_MIN_ORDER lowers the order
+from which a batch uses it, which lets the small parity cases run through
+it too, and the two kernels must then agree on every replica.
+"""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+import xtax_b200 as X
+from test_gpu_parity import compare, oracle_job, start_of
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture
+def large_from(monkeypatch):
+    def set_order(n):
+        monkeypatch.setenv("XW_LARGE_MIN_ORDER", str(n))
+    return set_order
+
+
+def run_and_replay(n, w, R, iters, kw, seed):
+    p = X.Params(stop_on_solve=0, **kw)
+    batch = X.Batch([{"n": n, "w": w, "seed": seed, "replicas": R}], p)
+    temps = [batch.replica(0, r)[0].reheat_temperature for r in range(R)]
+    batch.run(iters)
+    batch.synchronize()
+    job = oracle_job(n, w, seed, p)
+    for r in range(R):
+        rep = O.Replica(job, r, start_of(n, w, seed, r, p), temps[r], r)
+        rep.run(iters, stop_on_solve=False)
+        assert rep.check() == 0
+        compare(batch, 0, r, rep)
+    return batch
+
+
+SMALL_CASES = [
+    (12, 11, 4, 2000, dict(t_init=4.0, moves_per_launch=700, stuck_threshold=500, moves_per_cool=50)),
+    (16, 4, 4, 1500, dict(t_init=3.0, moves_per_launch=500, double_sign_fraction=0.4)),
+    (13, 9, 3, 1200, dict(t_init=4.0, moves_per_launch=600, target_samples=12, candidate_samples=7)),
+    (20, 10, 3, 1000, dict(t_init=5.0, moves_per_launch=1000, move_set=1, start_kind=1, objective=1)),
+    (30, 29, 3, 800, dict(t_init=6.0, moves_per_launch=400, objective=2)),
+    (8, 8, 3, 800, dict(t_init=3.0, moves_per_launch=400)),
+    (9, 1, 3, 600, dict(t_init=1.0, moves_per_launch=300)),
+    (70, 30, 2, 200, dict(t_init=8.0, moves_per_launch=100)),
+    (200, 20, 1, 60, dict(t_init=6.0, moves_per_launch=30)),
+]
+
+
+@pytest.mark.parametrize("n,w,R,iters,kw", SMALL_CASES, ids=lambda v: str(v) if not isinstance(v, dict) else "")
+def test_small_orders_through_the_large_kernel_match_oracle(large_from, n, w, R, iters, kw):
+    large_from(1)
+    run_and_replay(n, w, R, iters, kw, 3000 + n * 7 + w).close()
+
+
+LARGE_CASES = [
+    # just above the shared-memory classes; the reference's own limit is about 276
+    (260, 259, 2, 40, dict(t_init=8.0, moves_per_launch=20)),
+    (276, 275, 1, 30, dict(t_init=8.0, moves_per_launch=30)),
+    (300, 20, 2, 40, dict(t_init=6.0, moves_per_launch=40, double_sign_fraction=0.3)),
+    (320, 4, 2, 40, dict(t_init=2.0, moves_per_launch=20, move_set=1, start_kind=1, objective=1)),
+    (333, 150, 1, 30, dict(t_init=10.0, moves_per_launch=30, objective=2)),
+    (384, 384, 1, 30, dict(t_init=8.0, moves_per_launch=30)),
+    (1024, 1000, 1, 12, dict(t_init=10.0, moves_per_launch=12)),
+]
+
+
+@pytest.mark.parametrize("n,w,R,iters,kw", LARGE_CASES, ids=lambda v: str(v) if not isinstance(v, dict) else "")
+def test_large_orders_match_oracle(n, w, R, iters, kw):
+    run_and_replay(n, w, R, iters, kw, 5000 + n * 7 + w).close()
+
+
+def test_both_kernels_agree_on_a_mixed_batch(large_from):
+    """A batch of several orders gives the same results whichever kernel
+    runs which jobs (here: the shared-memory kernel for all, then the large
+    kernel for orders from 20 while the rest stay in shared memory)."""
+    jobs = [{"n": n, "w": w, "seed": 11 + n, "replicas": 6} for n, w in ((12, 11), (18, 9), (26, 25), (40, 8))]
+    p = X.Params(stop_on_solve=0, t_init=5.0, moves_per_launch=500)
+    out = []
+    for threshold in (257, 20):
+        large_from(threshold)
+        b = X.Batch(jobs, p)
+        b.run(1500)
+        b.synchronize()
+        out.append([(r.score, r.conflicts, r.best_replica, r.moves, r.candidate_evaluations, W.tobytes())
+                    for r, W in b.results()])
+        out.append([tuple(np.concatenate([a.ravel().astype(np.int64) for a in b.replica(j, k)[1:]]).tolist())
+                    for j in range(len(jobs)) for k in range(6)])
+        b.close()
+    assert out[0] == out[2]
+    assert out[1] == out[3]
+
+
+def test_large_tempering_matches_oracle():
+    n, w, R, interval, rounds = 264, 263, 4, 15, 3
+    p = X.Params(stop_on_solve=0, tempering=1, exchange_interval=interval, t_min=0.1, t_init=6.0,
+                 squared_objective_fraction=0.0, parity_objective_fraction=0.0)
+    seed = 91
+    batch = X.Batch([{"n": n, "w": w, "seed": seed, "replicas": R}], p)
+    batch.run(interval * rounds)
+    batch.synchronize()
+    # the host builds the ladder by repeated multiplication
+    ratio = (6.0 / 0.1) ** (1.0 / (R - 1))
+    ladder, t = [], 0.1
+    for _ in range(R):
+        ladder.append(t)
+        t *= ratio
+    job = oracle_job(n, w, seed, p)
+    reps = [O.Replica(job, r, start_of(n, w, seed, r, p), ladder[r], r) for r in range(R)]
+    for k in range(rounds):
+        for rep in reps:
+            rep.run(interval, stop_on_solve=False)
+        O.exchange(job, reps, ladder, k)
+    for r in range(R):
+        compare(batch, 0, r, reps[r])
+    batch.close()
+
+
+def test_large_snapshot_resume_equals_uninterrupted(tmp_path):
+    """A snapshot holds no Gram arena: the kernel rebuilds it on resume and
+    the trajectory continues unchanged."""
+    jobs = [{"n": 270, "w": 269, "seed": 7, "replicas": 3}]
+    p = X.Params(stop_on_solve=0, t_init=8.0, moves_per_launch=25)
+    a = X.Batch(jobs, p)
+    a.run(100)
+    a.synchronize()
+    b = X.Batch(jobs, p)
+    b.run(50)
+    b.synchronize()
+    path = str(tmp_path / "large.xwpop")
+    b.save(path)
+    b.close()
+    c = X.Batch.load(path, jobs)
+    c.run(50)
+    c.synchronize()
+    for r in range(3):
+        sa, Wa, Ba, Ma = a.replica(0, r)
+        sc, Wc, Bc, Mc = c.replica(0, r)
+        assert sc.error == 0
+        assert (sa.iterations, sa.moves, sa.score, sa.best_score) == (sc.iterations, sc.moves, sc.score, sc.best_score)
+        assert (Wa == Wc).all() and (Ba == Bc).all() and (Ma == Mc).all()
+    a.close()
+    c.close()
+
+
+def test_large_order_solves_and_verifies():
+    """W(300, 1) from row-only starts needs column changes: the within-row
+    swap finds a signed permutation matrix, which the host verifies (the
+    oracle's replay of these replicas solves within 60000 iterations)."""
+    p = X.Params(stop_on_solve=1, t_init=0.15, t_min=0.05, moves_per_launch=20000, move_set=1, start_kind=1,
+                 squared_objective_fraction=0.0, parity_objective_fraction=0.0)
+    res, best = X.batch_solve([{"n": 300, "w": 1, "seed": 3, "replicas": 8}], p, iters=400000)
+    assert res[0].error == 0
+    assert res[0].solved == 1 and res[0].verified == 1
+    W = best[: 300 * 300].reshape(300, 300).T.astype(np.int64)
+    assert (W @ W.T == np.eye(300, dtype=np.int64)).all()
+
+
+def test_order_above_the_maximum_is_refused():
+    with pytest.raises(X.XwError):
+        X.Batch([{"n": X.MAX_ORDER_CUDA + 1, "w": 4, "seed": 1, "replicas": 1}], X.Params())

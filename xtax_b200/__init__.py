@@ -24,7 +24,8 @@ HEADER = os.path.join(os.path.dirname(_HERE), "include", "xw.h")
 
 XW_OK, XW_ERR_INVALID, XW_ERR_CUDA, XW_ERR_CAPACITY, XW_ERR_INTERNAL = 0, 1, 2, 3, 4
 XW_ERR_NOT_FOUND, XW_ERR_TIMEOUT, XW_ERR_IO = 5, 6, 7
-MAX_ORDER_CUDA = 256
+MAX_ORDER_CUDA = 1024      # largest order the device path anneals
+MAX_ORDER_SHARED = 256     # largest order whose replica state sits in shared memory (and served orders)
 MAX_CANDIDATE_SAMPLES = 32
 MAX_TARGET_SAMPLES = 64
 
@@ -519,7 +520,8 @@ class Batch:
         st = ReplicaState()
         W = np.zeros(n * n, dtype=np.int8)
         B = np.zeros(n * n, dtype=np.int8)
-        M = np.zeros(max(n * m, 1), dtype=np.uint8)
+        # minority lists are u8 up to the shared-memory orders, u16 above
+        M = np.zeros(max(n * m, 1), dtype=np.uint8 if n <= MAX_ORDER_SHARED else np.uint16)
         _check(lib().xw_batch_read_replica(self.h, job, r, C.byref(st), _i8(W), _i8(B),
                                            M.ctypes.data_as(C.POINTER(C.c_uint8))))
         return st, W, B, M[: n * m]
@@ -583,14 +585,14 @@ class Server:
 
     def poll(self, rid):
         res = RequestResult()
-        n = self._orders.get(rid, MAX_ORDER_CUDA)
+        n = self._orders.get(rid, MAX_ORDER_SHARED)
         W = np.zeros(n * n, dtype=np.int8)
         _check(lib().xw_poll(self.h, rid, C.byref(res), _i8(W)))
         return self._out(rid, res, W)
 
     def wait(self, rid, timeout=-1.0):
         res = RequestResult()
-        n = self._orders.get(rid, MAX_ORDER_CUDA)
+        n = self._orders.get(rid, MAX_ORDER_SHARED)
         W = np.zeros(n * n, dtype=np.int8)
         _check(lib().xw_wait(self.h, rid, float(timeout), C.byref(res), _i8(W)))
         return self._out(rid, res, W)

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -111,6 +112,15 @@ std::string strfmt(const char* f, ...) {
 
 void check_cuda(cudaError_t e, const char* what) { check(e, what); }
 
+static_assert(XW_MAX_ORDER_CUDA == XW_MAX_ORDER_LARGE, "public and device order limits agree");
+static_assert(XW_MAX_ORDER_SHARED == XW_MAX_N, "public and shared-memory order limits agree");
+
+int large_min_order() {
+    const char* e = std::getenv("XW_LARGE_MIN_ORDER");
+    if (!e || !*e) return XW_MAX_N + 1;
+    return std::clamp(std::atoi(e), 1, XW_MAX_N + 1);
+}
+
 std::string validate(int n, int w, const xw_params& p) {
     if (n < 1 || n > 32767) return "CUDA xweigh order is out of range";
     if (w < 1 || w > n) return "CUDA xweigh weight must be in [1, n]";
@@ -161,14 +171,15 @@ Batch::~Batch() {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     for (auto e : events) cudaEventDestroy(e);
     for (void* ptr : {d_jobs, d_jobs0, d_arena, d_arena0, d_rec_off, d_items, d_counters, d_ladder,
-                      d_out, d_best_off, d_best, d_t0})
+                      d_out, d_best_off, d_best, d_t0, d_gram, d_gram_off})
         if (ptr) cudaFree(ptr);
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
-static size_t record_bytes(int n, int m) {
+// header, W, best W, minority lists (u16 on the HBM-resident kernel)
+static size_t record_bytes(int n, int m, bool large) {
     const uint32_t nn = xw_pad16((uint32_t)(n * n));
-    const size_t b = 128 + 2 * (size_t)nn + xw_pad16((uint32_t)(n * m));
+    const size_t b = 128 + 2 * (size_t)nn + xw_pad16((uint32_t)(n * m) * (large ? 2u : 1u));
     return (b + 127) & ~size_t(127);
 }
 
@@ -195,6 +206,7 @@ void prepare_job(const xw_job_spec& s, const xw_params& p, const int8_t* starts,
     J.stuck_threshold = p.stuck_threshold;
     J.objective = p.objective;
     J.general = needs_general_kernel(p) ? 1 : 0;
+    J.large = s.n >= large_min_order() ? 1 : 0;
     J.replicas = s.replicas;
     // the Philox key follows the reference's curand seed derivation
     // (xweigh_cuda.cu:1724-1727)
@@ -206,7 +218,7 @@ void prepare_job(const xw_job_spec& s, const xw_params& p, const int8_t* starts,
     J.off_w = 128;
     J.off_best = 128 + nn;
     J.off_mino = 128 + 2 * nn;
-    J.record_bytes = (uint32_t)record_bytes(s.n, J.m);
+    J.record_bytes = (uint32_t)record_bytes(s.n, J.m, J.large != 0);
     J.thr_greedy = coin_threshold(p.greedy_fraction);
     J.thr_target = coin_threshold(p.target_fraction);
     J.thr_double = p.move_set == 0 ? coin_threshold(p.double_sign_fraction) : 0;
@@ -225,10 +237,18 @@ void prepare_job(const xw_job_spec& s, const xw_params& p, const int8_t* starts,
         if (p.start_kind == 1) return row_start(n, w, J.key0, J.key1, (uint32_t)r);
         return CpuState::random_start(n, w, base + (uint32_t)r * 0x9e3779b9u).entries();
     };
+    // start states and their scores (so that results read before the first
+    // launch are meaningful; the kernel rebuilds and checks them)
+    std::vector<std::array<int64_t, 4>> start_stats(R);
+    auto make_start = [&](int r) {
+        W[r] = start_of(r);
+        if (W[r].size() != (size_t)n * n) throw std::invalid_argument("start state size mismatch");
+        xw_score(n, w, W[r].data(), start_stats[r].data());
+    };
     if (parallel) {
-        parallel_for(R, [&](int r) { W[r] = start_of(r); });
+        parallel_for(R, make_start);
     } else {
-        for (int r = 0; r < R; ++r) W[r] = start_of(r);
+        for (int r = 0; r < R; ++r) make_start(r);
     }
     // calibrate_temperature on replica 0 (xweigh_cuda.cu:1563-1567)
     t_init = p.t_init;
@@ -261,14 +281,8 @@ void prepare_job(const xw_job_spec& s, const xw_params& p, const int8_t* starts,
         H->temperature = temps[r];
         H->reheat_temperature = temps[r];
         H->rung = r;
-        // start scores, so that results read before the first launch are
-        // meaningful; the kernel rebuilds and checks them
-        {
-            int64_t st[4];
-            xw_score(n, w, W[r].data(), st);
-            H->score = H->best_score = (int32_t)st[0];
-            H->conflicts = H->best_conflicts = (int32_t)st[1];
-        }
+        H->score = H->best_score = (int32_t)start_stats[r][0];
+        H->conflicts = H->best_conflicts = (int32_t)start_stats[r][1];
         if (p.objective >= 0) {
             H->obj_kind = p.objective;
         } else {
@@ -277,7 +291,6 @@ void prepare_job(const xw_job_spec& s, const xw_params& p, const int8_t* starts,
             H->obj_kind = choice < p.squared_objective_fraction ? 1
                 : choice < p.squared_objective_fraction + p.parity_objective_fraction ? 2 : 0;
         }
-        if (W[r].size() != (size_t)n * n) throw std::invalid_argument("start state size mismatch");
         std::memcpy(rec + J.off_w, W[r].data(), (size_t)n * n);
         std::memcpy(rec + J.off_best, W[r].data(), (size_t)n * n);
     }
@@ -340,26 +353,49 @@ void Batch::derive_layout() {
     opl = 1;
     general = false;
     slot_bytes = 0;
+    n_large = 0;
+    general_large = false;
+    large_slot_bytes = 0;
     for (int j = 0; j < njobs; ++j) {
         const XwJob& J = jobs[j];
         total_replicas += (uint32_t)J.replicas;
         best_offsets[j] = best_off;
         best_off += (size_t)J.n * J.n;
-        opl = std::max(opl, anneal_opl(J.n));
-        general = general || J.general != 0;
+        if (J.large) {
+            n_large += (uint32_t)J.replicas;
+            general_large = general_large || J.general != 0;
+            large_slot_bytes = std::max(large_slot_bytes, anneal_large_slot_bytes(J.n));
+        } else {
+            opl = std::max(opl, anneal_opl(J.n));
+            general = general || J.general != 0;
+        }
     }
-    // one launch runs every replica with the widest class's kernel and layout
-    for (int j = 0; j < njobs; ++j) slot_bytes = std::max(slot_bytes, anneal_slot_bytes(jobs[j].n, jobs[j].m, opl));
+    // one launch runs every shared-memory replica with the widest class's
+    // kernel and layout, another every HBM-resident one
+    for (int j = 0; j < njobs; ++j)
+        if (!jobs[j].large) slot_bytes = std::max(slot_bytes, anneal_slot_bytes(jobs[j].n, jobs[j].m, opl));
     best_bytes = best_off;
-    // work items: longest replicas first (cost grows with n)
+    // work items: the HBM-resident replicas, then the others; longest
+    // replicas first within each (cost grows with n)
     items.resize(total_replicas);
     std::vector<int> job_of(total_replicas);
     for (int j = 0; j < njobs; ++j)
         for (int r = 0; r < jobs[j].replicas; ++r) job_of[jobs[j].rep_begin + r] = j;
     for (uint32_t i = 0; i < total_replicas; ++i) items[i] = i;
     std::stable_sort(items.begin(), items.end(), [&](uint32_t a, uint32_t b) {
-        return jobs[job_of[a]].n > jobs[job_of[b]].n;
+        const XwJob &A = jobs[job_of[a]], &B = jobs[job_of[b]];
+        if (A.large != B.large) return A.large > B.large;
+        return A.n > B.n;
     });
+    // Gram arena offsets of the HBM-resident replicas
+    gram_off.assign(total_replicas, 0);
+    gram_bytes = 0;
+    for (uint32_t i = 0; i < total_replicas; ++i) {
+        const XwJob& J = jobs[job_of[i]];
+        if (!J.large) continue;
+        gram_off[i] = gram_bytes;
+        gram_bytes += anneal_large_gram_bytes(J.n);
+    }
 }
 
 // Device buffers for the batch; the records in `host` become the state that
@@ -373,7 +409,7 @@ void Batch::upload(const std::vector<uint8_t>& host) {
     };
     size_t free_b = 0, total_b = 0;
     check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
-    const size_t need = 2 * arena + 2 * sizeof(XwJob) * njobs + 8 * total_replicas + best_bytes;
+    const size_t need = 2 * arena + 2 * sizeof(XwJob) * njobs + 16 * total_replicas + best_bytes + gram_bytes;
     if (need > free_b)
         throw std::length_error(fmt("CUDA replica state requires %g MiB, but only %g MiB is free",
                                     need / 1048576.0, free_b / 1048576.0));
@@ -392,6 +428,13 @@ void Batch::upload(const std::vector<uint8_t>& host) {
     dmalloc(&d_best_off, sizeof(uint64_t) * njobs, "cudaMalloc result offsets");
     dmalloc(&d_best, best_bytes, "cudaMalloc best states");
     dmalloc(&d_t0, sizeof(uint64_t), "cudaMalloc clock");
+    if (n_large) {
+        dmalloc(&d_gram, gram_bytes, "cudaMalloc Gram arena");
+        dmalloc(&d_gram_off, sizeof(uint64_t) * total_replicas, "cudaMalloc Gram offsets");
+        check(cudaMemcpyAsync(d_gram_off, gram_off.data(), sizeof(uint64_t) * total_replicas, cudaMemcpyHostToDevice,
+                              stream),
+              "upload Gram offsets");
+    }
     check(cudaMemcpyAsync(d_jobs0, jobs.data(), sizeof(XwJob) * njobs, cudaMemcpyHostToDevice, stream), "upload jobs");
     check(cudaMemcpyAsync(d_arena0, host.data(), arena, cudaMemcpyHostToDevice, stream), "upload records");
     check(cudaMemcpyAsync(d_rec_off, rec_off.data(), sizeof(uint64_t) * total_replicas, cudaMemcpyHostToDevice, stream),
@@ -492,6 +535,10 @@ void Batch::load(const std::string& path, const xw_params* over) {
         total += (uint64_t)J.replicas;
     }
     if (total != counts[0]) throw std::invalid_argument("corrupt population snapshot: " + path);
+    // a snapshot holds no Gram arena: the large-order kernel rebuilds it
+    for (size_t j = 0; j < jobs.size(); ++j)
+        for (int r = 0; r < jobs[j].replicas; ++r)
+            reinterpret_cast<RepHeader*>(host.data() + rec_off[jobs[j].rep_begin + r])->status &= ~XW_STATUS_GRAM;
     if (over) {
         // run-time settings may change on resume; the search itself may not
         params.device = over->device;
@@ -509,6 +556,24 @@ void Batch::load(const std::string& path, const xw_params* over) {
 }
 
 void Batch::configure_shape(int wpb) {
+    if (graph_exec) {
+        cudaGraphExecDestroy(graph_exec);
+        graph_exec = nullptr;
+    }
+    if (n_large) {
+        // four warps per CTA, as many CTAs as the SMs hold
+        const void* lfn = anneal_large_kernel_fn(general_large);
+        const size_t lsmem = (size_t)large_wpb * large_slot_bytes;
+        check(cudaFuncSetAttribute(lfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem),
+              "cudaFuncSetAttribute max dynamic shared memory");
+        int per_sm = 0;
+        check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lfn, 32 * large_wpb, lsmem),
+              "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+        if (per_sm < 1) throw std::length_error("CUDA large-order anneal kernel has zero occupancy");
+        const int want = (int)((n_large + large_wpb - 1) / large_wpb);
+        large_blocks = std::max(1, std::min(want, per_sm * props.multiProcessorCount));
+    }
+    if (n_large == total_replicas) return;
     const void* fn = anneal_kernel_fn(opl, general);
     int optin = 0;
     check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, params.device),
@@ -528,12 +593,8 @@ void Batch::configure_shape(int wpb) {
     if (per_sm < 1) throw std::length_error("CUDA anneal kernel has zero occupancy on the selected device");
     warps_per_block = wpb;
     blocks_per_sm = per_sm;
-    const int want = (int)((total_replicas + wpb - 1) / wpb);
+    const int want = (int)((total_replicas - n_large + wpb - 1) / wpb);
     blocks = std::max(1, std::min(want, per_sm * props.multiProcessorCount));
-    if (graph_exec) {
-        cudaGraphExecDestroy(graph_exec);
-        graph_exec = nullptr;
-    }
 }
 
 void Batch::reset() {
@@ -559,7 +620,8 @@ void Batch::reserve_rounds(int rounds) {
         check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
         if (d_counters) cudaFree(d_counters);
         d_counters = nullptr;
-        check(cudaMalloc(&d_counters, sizeof(uint32_t) * rounds), "cudaMalloc counters");
+        // one counter per round for each of the two kernels
+        check(cudaMalloc(&d_counters, sizeof(uint32_t) * 2 * rounds), "cudaMalloc counters");
         counters_cap = rounds;
     }
 }
@@ -570,23 +632,36 @@ void Batch::enqueue_rounds(uint64_t iters, bool timed) {
     if ((int)events.size() < 2 * rounds || counters_cap < rounds)
         throw std::logic_error("round resources not reserved");
     check(launch_mark_t0(static_cast<uint64_t*>(d_t0), stream), "launch mark_t0");
-    check(cudaMemsetAsync(d_counters, 0, sizeof(uint32_t) * rounds, stream), "cudaMemsetAsync counters");
+    check(cudaMemsetAsync(d_counters, 0, sizeof(uint32_t) * 2 * rounds, stream), "cudaMemsetAsync counters");
     uint64_t left = iters;
     for (int k = 0; k < rounds; ++k) {
         AnnealArgs a;
         a.jobs = static_cast<XwJob*>(d_jobs);
         a.arena = static_cast<uint8_t*>(d_arena);
         a.rec_off = static_cast<const uint64_t*>(d_rec_off);
-        a.items = static_cast<const uint32_t*>(d_items);
-        a.n_items = total_replicas;
-        a.slot_bytes = slot_bytes;
-        a.counter = static_cast<uint32_t*>(d_counters) + k;
         a.iters = std::min(left, per);
         a.stop_on_solve = params.stop_on_solve;
         a.pad = 0;
         left -= a.iters;
         if (timed) check(cudaEventRecord(events[2 * k], stream), "cudaEventRecord");
-        check(launch_anneal(a, opl, general, warps_per_block, blocks, stream), "launch anneal_kernel");
+        if (n_large) {
+            AnnealArgs l = a;
+            l.items = static_cast<const uint32_t*>(d_items);
+            l.n_items = n_large;
+            l.slot_bytes = large_slot_bytes;
+            l.counter = static_cast<uint32_t*>(d_counters) + 2 * k + 1;
+            l.gram = static_cast<uint8_t*>(d_gram);
+            l.gram_off = static_cast<const uint64_t*>(d_gram_off);
+            check(launch_anneal_large(l, general_large, large_wpb, large_blocks, stream),
+                  "launch anneal_large_kernel");
+        }
+        if (n_large < total_replicas) {
+            a.items = static_cast<const uint32_t*>(d_items) + n_large;
+            a.n_items = total_replicas - n_large;
+            a.slot_bytes = slot_bytes;
+            a.counter = static_cast<uint32_t*>(d_counters) + 2 * k;
+            check(launch_anneal(a, opl, general, warps_per_block, blocks, stream), "launch anneal_kernel");
+        }
         if (timed) check(cudaEventRecord(events[2 * k + 1], stream), "cudaEventRecord");
         if (tempering)
             check(launch_exchange(static_cast<XwJob*>(d_jobs), (int)jobs.size(), static_cast<uint8_t*>(d_arena),
@@ -725,7 +800,12 @@ int restart_population(Batch& b, int j, const std::vector<int8_t>& elite_best, i
         uint8_t* rec = host.data() + (size_t)r * rb;
         RepHeader* H = reinterpret_cast<RepHeader*>(rec);
         std::memcpy(rec + J.off_w, k.entries().data(), (size_t)n * n);
-        for (int i = 0; i < n * m; ++i) rec[J.off_mino + i] = (uint8_t)k.minority()[(size_t)i];
+        if (J.large) {
+            std::memcpy(rec + J.off_mino, k.minority().data(), sizeof(uint16_t) * n * m);
+            H->status &= ~XW_STATUS_GRAM;   // the kernel rebuilds G from the new W
+        } else {
+            for (int i = 0; i < n * m; ++i) rec[J.off_mino + i] = (uint8_t)k.minority()[(size_t)i];
+        }
         const bool kick_better = k.score() < gbest || (k.score() == gbest && k.conflicts() < gconf);
         std::memcpy(rec + J.off_best, kick_better ? k.entries().data() : elite_best.data(), (size_t)n * n);
         H->score = (int32_t)k.score();
@@ -859,6 +939,37 @@ int32_t xw_score(int32_t n, int32_t w, const int8_t* W, int64_t stats[4]) {
     if (n < 1 || !W || !stats) return fail(XW_ERR_INVALID, "invalid arguments");
     (void)w;
     int64_t s = 0, c = 0, q = 0, par = 0;
+    const size_t nn = (size_t)n * n;
+    bool ternary = true;
+    for (size_t i = 0; i < nn && ternary; ++i) ternary = W[i] >= -1 && W[i] <= 1;
+    if (ternary) {
+        // W_a . W_b = |S_a & S_b| - 2 |S_a & S_b & (N_a ^ N_b)| over the
+        // support (S) and negative-sign (N) bit rows: O(n^3 / 64)
+        const int nw = (n + 63) / 64;
+        std::vector<uint64_t> S((size_t)n * nw, 0), N((size_t)n * nw, 0);
+        for (int k = 0; k < n; ++k)
+            for (int a = 0; a < n; ++a) {
+                const int8_t v = W[(size_t)k * n + a];
+                if (v) S[(size_t)a * nw + k / 64] |= 1ull << (k % 64);
+                if (v < 0) N[(size_t)a * nw + k / 64] |= 1ull << (k % 64);
+            }
+        for (int a = 0; a < n; ++a)
+            for (int b = a + 1; b < n; ++b) {
+                int64_t d = 0;
+                for (int k = 0; k < nw; ++k) {
+                    const uint64_t both = S[(size_t)a * nw + k] & S[(size_t)b * nw + k];
+                    d += __builtin_popcountll(both) -
+                         2 * __builtin_popcountll(both & (N[(size_t)a * nw + k] ^ N[(size_t)b * nw + k]));
+                }
+                const int64_t ad = d < 0 ? -d : d;
+                s += ad;
+                c += d != 0;
+                q += d * d;
+                par += ad & 1;
+            }
+        stats[0] = s; stats[1] = c; stats[2] = q; stats[3] = par;
+        return XW_OK;
+    }
     for (int a = 0; a < n; ++a)
         for (int b = a + 1; b < n; ++b) {
             int64_t d = 0;
@@ -1057,6 +1168,8 @@ int32_t xw_autotune(const xw_job_spec* jobs, int32_t njobs, const xw_params* pin
         }
         Batch b;
         b.build(jobs, njobs, *pin, nullptr);
+        if (b.n_large == b.total_replicas)
+            return fail(XW_ERR_INVALID, "autotune covers the shared-memory kernel; every job here is of larger order");
         int optin = 0;
         check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, pin->device),
               "cudaDeviceGetAttribute max opt-in shared memory");
@@ -1143,7 +1256,17 @@ int32_t xw_batch_read_replica(xw_batch* h, int32_t job, int32_t replica, xw_repl
         const size_t nn = (size_t)J.n * J.n;
         if (W) std::memcpy(W, rec.data() + J.off_w, nn);
         if (best_W) std::memcpy(best_W, rec.data() + J.off_best, nn);
-        if (minority) std::memcpy(minority, rec.data() + J.off_mino, (size_t)J.n * J.m);
+        // one byte per entry up to XW_MAX_ORDER_SHARED, two above, whichever
+        // kernel holds the replica
+        const size_t nm = (size_t)J.n * J.m;
+        if (minority && !J.large) {
+            std::memcpy(minority, rec.data() + J.off_mino, nm);
+        } else if (minority && J.n > XW_MAX_ORDER_SHARED) {
+            std::memcpy(minority, rec.data() + J.off_mino, 2 * nm);
+        } else if (minority) {
+            const uint16_t* src = reinterpret_cast<const uint16_t*>(rec.data() + J.off_mino);
+            for (size_t i = 0; i < nm; ++i) minority[i] = (uint8_t)src[i];
+        }
         return XW_OK;
     })
 }
@@ -1220,13 +1343,9 @@ int32_t xw_run(int32_t n, int32_t w, const xw_params* pin, const int8_t* start, 
     }
     int32_t rc = xw_query_device(p.device, &out->device);
     if (rc != XW_OK) return rc;
-    if (n > XW_MAX_ORDER_CUDA) {
-        const double need = anneal_slot_bytes(std::min(n, 4096), std::min(w, n - w), 8) / 1024.0;
-        return fail(XW_ERR_CAPACITY,
-                    fmt("CUDA replica requires %.2f KiB of shared memory, but device %d permits %.2f KiB per "
-                        "opt-in block",
-                        need, p.device, out->device.max_shared_memory_per_block / 1024.0));
-    }
+    if (n > XW_MAX_ORDER_CUDA)
+        return fail(XW_ERR_CAPACITY, fmt("CUDA replica of order %d is above the device path's maximum order %d", n,
+                                         XW_MAX_ORDER_CUDA));
     XW_GUARD({
         check(cudaSetDevice(p.device), "cudaSetDevice");
         const auto t_init0 = std::chrono::steady_clock::now();
@@ -1238,12 +1357,14 @@ int32_t xw_run(int32_t n, int32_t w, const xw_params* pin, const int8_t* start, 
         spec.seed = p.seed;
         int replicas = p.replicas;
         const int m = std::min(w, n - w);
-        const uint32_t slot = anneal_slot_bytes(n, m, anneal_opl(n));
+        const bool large = n >= large_min_order();
+        const uint32_t slot = large ? anneal_large_slot_bytes(n) : anneal_slot_bytes(n, m, anneal_opl(n));
         if (replicas == 0) {
             // one resident wave: warp slots per SM times SMs
-            const int wpb = p.warps_per_block > 0 ? p.warps_per_block : 4;
+            const int wpb = large ? 4 : p.warps_per_block > 0 ? p.warps_per_block : 4;
             int per_sm = 0;
-            const void* fn = anneal_kernel_fn(anneal_opl(n), needs_general_kernel(p));
+            const void* fn = large ? anneal_large_kernel_fn(needs_general_kernel(p))
+                                   : anneal_kernel_fn(anneal_opl(n), needs_general_kernel(p));
             cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(wpb * slot));
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * wpb, (size_t)wpb * slot);
             replicas = std::max(1, per_sm * wpb * out->device.multiprocessors);

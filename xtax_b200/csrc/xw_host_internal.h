@@ -17,6 +17,10 @@ std::string validate(int n, int w, const xw_params& p);
 // objective on some replica, or the within-row swap move set
 bool needs_general_kernel(const xw_params& p);
 void set_last_error(const std::string& msg);
+// The least order that runs on the HBM-resident kernel: XW_MAX_N + 1, or
+// the value of XW_LARGE_MIN_ORDER in [1, XW_MAX_N + 1] (tests run small
+// orders through that kernel to compare it with the shared-memory one).
+int large_min_order();
 std::string strfmt(const char* f, ...);
 // throws std::runtime_error naming `what` when e is an error
 void check_cuda(cudaError_t e, const char* what);
@@ -66,6 +70,16 @@ struct Batch {
     int blocks_per_sm = 1;
     int blocks = 1;
 
+    // jobs with J.large run on the HBM-resident kernel: items[0, n_large)
+    // are their replicas; the rest run on the shared-memory kernel
+    uint32_t n_large = 0;
+    bool general_large = false;
+    uint32_t large_slot_bytes = 0;
+    int large_wpb = 4;
+    int large_blocks = 1;
+    std::vector<uint64_t> gram_off;   // per replica, into d_gram
+    size_t gram_bytes = 0;
+
     void* d_jobs = nullptr;
     void* d_jobs0 = nullptr;
     void* d_arena = nullptr;
@@ -79,6 +93,8 @@ struct Batch {
     void* d_best_off = nullptr;
     void* d_best = nullptr;
     void* d_t0 = nullptr;
+    void* d_gram = nullptr;
+    void* d_gram_off = nullptr;
     uint64_t t0_host = 0;
 
     std::vector<cudaEvent_t> events;

@@ -21,9 +21,10 @@ struct AnnealArgs {
     uint64_t iters;            // iterations per replica this launch
     int32_t stop_on_solve;
     int32_t pad;
+    uint8_t* gram = nullptr;            // large-order kernel: Gram and mask arena
+    const uint64_t* gram_off = nullptr; // byte offset of each replica's Gram there
 };
 
-// shared-memory bytes one warp needs for a replica of order n, minority m
 // shared-memory bytes one warp needs for a replica of order n, minority m,
 // in a launch of the `opl` rows-per-lane kernel
 uint32_t anneal_slot_bytes(int n, int m, int opl);
@@ -35,6 +36,14 @@ int anneal_opl(int n);
 const void* anneal_kernel_fn(int opl, bool general);
 cudaError_t launch_anneal(const AnnealArgs& args, int opl, bool general, int warps_per_block, int blocks,
                           cudaStream_t stream);
+// Orders above XW_MAX_N: the kernel whose replica state lives in HBM
+// (xw_anneal_large.cu).  Shared memory per warp, Gram-arena bytes per
+// replica (a multiple of 256), the kernel, and its launch.
+uint32_t anneal_large_slot_bytes(int n);
+uint64_t anneal_large_gram_bytes(int n);
+const void* anneal_large_kernel_fn(bool general);
+cudaError_t launch_anneal_large(const AnnealArgs& args, bool general, int warps_per_block, int blocks,
+                                cudaStream_t stream);
 cudaError_t launch_exchange(XwJob* jobs, int njobs, uint8_t* arena, const uint64_t* rec_off,
                             const double* ladder, int stop_on_solve, cudaStream_t stream);
 

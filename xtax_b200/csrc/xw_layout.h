@@ -12,17 +12,23 @@
 // memory from W when it loads a replica (O(n^3/32) per lane, negligible next
 // to the thousands of moves per launch) and checks the rebuilt score against
 // the tracked one.
+//
+// Orders above XW_MAX_N keep 16-bit minority lists (n*m u16) and a Gram
+// arena beside the records (int16 G, support and sign masks per replica)
+// that persists between launches; see xw_anneal_large.cu.
 #pragma once
 
 #include <stdint.h>
 
-#define XW_MAX_N 256
+#define XW_MAX_N 256           // largest order of the shared-memory kernel
+#define XW_MAX_ORDER_LARGE 1024 // largest order of the HBM-resident kernel
 #define XW_MAX_CANDIDATES 32
 #define XW_MAX_TARGET_SAMPLES 64
 #define XW_NOALLOC_SCRATCH_BYTES (4 * 1024 * 1024)
 
 #define XW_STATUS_INIT 1u      // record holds incremental state (score etc.)
 #define XW_STATUS_SOLVED 2u    // best score reached 0
+#define XW_STATUS_GRAM 4u      // large orders: the Gram arena holds this W's Gram and masks
 #define XW_ERR_SCORE 1u        // rebuilt score differs from the tracked one
 #define XW_ERR_MINORITY 2u     // W row weights disagree with the minority lists
 #define XW_ERR_KERNEL 4u       // a lean launch met a replica that needs the general kernel
@@ -50,7 +56,7 @@ struct XwJob {
     uint64_t solved_it;
     uint64_t solve_ns;              // %globaltimer at the solve
     int32_t done;                   // host: job retired, skip its replicas
-    int32_t pad1;
+    int32_t large;                  // runs on the HBM-resident kernel (u16 minority lists)
     uint64_t exchange_iters;        // tempering: exchange only when the job's
                                     // iteration count is a multiple of this
                                     // (0 = after every anneal launch)

@@ -154,8 +154,8 @@ extern "C" int32_t xw_anneal_noalloc(int32_t n, int32_t w, const xw_params* p, i
         const std::string e = validate(n, w, *p);
         if (!e.empty()) return nfail(XW_ERR_INVALID, e);
     }
-    if (n > XW_MAX_ORDER_CUDA)
-        return nfail(XW_ERR_CAPACITY, "xw_anneal_noalloc: order above the device path's maximum of 256");
+    if (n > XW_MAX_ORDER_SHARED)
+        return nfail(XW_ERR_CAPACITY, "xw_anneal_noalloc: order above the shared-memory kernel's maximum of 256");
     if (replicas < 1) return nfail(XW_ERR_INVALID, "xw_anneal_noalloc: replica count must be positive");
     if (iters < 1) return nfail(XW_ERR_INVALID, "xw_anneal_noalloc: iterations must be positive");
     if (!(p->t_init > 0.0))

@@ -399,7 +399,7 @@ int* error_flag_ptr() {
 int32_t rescore_device(const int8_t* W, int64_t count, int n, int w, int32_t* stats, int32_t* gram,
                        cudaStream_t stream, int* err_flag, bool force_simt) {
     if (count < 0 || count > INT32_MAX / 4) return rfail(XW_ERR_INVALID, "rescore: count out of range");
-    if (n < 1 || n > XW_MAX_ORDER_CUDA) return rfail(XW_ERR_INVALID, "rescore: order must be in [1, 256]");
+    if (n < 1 || n > XW_MAX_ORDER_SHARED) return rfail(XW_ERR_INVALID, "rescore: order must be in [1, 256]");
     if (count == 0) return XW_OK;
     cudaError_t e;
     // tensor cores for n in {32, 64, 96, 128}: a tile row is one 128-byte TMA row
@@ -474,7 +474,7 @@ extern "C" int32_t xw_rescore_status(void) {
 }
 
 extern "C" int32_t xw_rescore(const int8_t* W, int64_t count, int32_t n, int32_t w, int32_t* stats, int32_t* gram) {
-    if (!W || !stats || count < 0 || n < 1 || n > XW_MAX_ORDER_CUDA) return rfail(XW_ERR_INVALID, "rescore: bad arguments");
+    if (!W || !stats || count < 0 || n < 1 || n > XW_MAX_ORDER_SHARED) return rfail(XW_ERR_INVALID, "rescore: bad arguments");
     if (count == 0) return XW_OK;
     const size_t in_bytes = (size_t)count * n * n, st_bytes = (size_t)count * 16,
                  g_bytes = gram ? (size_t)count * n * n * 4 : 0;

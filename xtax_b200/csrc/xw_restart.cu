@@ -70,8 +70,8 @@ __global__ void __launch_bounds__(kScanThreads) escape_scan_kernel(const int8_t*
     const int n = sh.n;
     const int r1 = blockIdx.y, r2 = blockIdx.x;
     if (r2 <= r1) return;
-    __shared__ int32_t g1[XW_MAX_N], g2[XW_MAX_N];
-    __shared__ uint8_t c1s[XW_MAX_N], c2s[XW_MAX_N];
+    __shared__ int32_t g1[XW_MAX_ORDER_LARGE], g2[XW_MAX_ORDER_LARGE];
+    __shared__ uint16_t c1s[XW_MAX_ORDER_LARGE], c2s[XW_MAX_ORDER_LARGE];
     __shared__ int k1, k2;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int o = tid; o < n; o += kScanThreads) {
@@ -87,8 +87,8 @@ __global__ void __launch_bounds__(kScanThreads) escape_scan_kernel(const int8_t*
             const unsigned m1 = __ballot_sync(0xffffffffu, v1 != 0 && v2 == 0);
             const unsigned m2 = __ballot_sync(0xffffffffu, v2 != 0 && v1 == 0);
             const unsigned lower = (1u << lane) - 1u;
-            if (v1 != 0 && v2 == 0) c1s[a + __popc(m1 & lower)] = (uint8_t)c;
-            if (v2 != 0 && v1 == 0) c2s[b + __popc(m2 & lower)] = (uint8_t)c;
+            if (v1 != 0 && v2 == 0) c1s[a + __popc(m1 & lower)] = (uint16_t)c;
+            if (v2 != 0 && v1 == 0) c2s[b + __popc(m2 & lower)] = (uint16_t)c;
             a += __popc(m1);
             b += __popc(m2);
         }

@@ -810,9 +810,9 @@ int32_t xw_submit(xw_server* h, const xw_request* r, uint64_t* id) {
     if (!err.empty()) return fail_with(XW_ERR_INVALID, err);
     const char* why = xw_impossibility_reason(r->n, r->w);
     if (why && *why) return fail_with(XW_ERR_INVALID, why);
-    if (r->n > XW_MAX_ORDER_CUDA)
-        return fail_with(XW_ERR_CAPACITY, xw::strfmt("order %d is beyond the device path's %d", r->n,
-                                                     XW_MAX_ORDER_CUDA));
+    if (r->n > XW_MAX_ORDER_SHARED)
+        return fail_with(XW_ERR_CAPACITY, xw::strfmt("order %d is beyond the served orders' maximum of %d", r->n,
+                                                     XW_MAX_ORDER_SHARED));
     if (r->replicas < 1) return fail_with(XW_ERR_INVALID, "CUDA replica count must be positive");
     if (r->replicas > s.cfg.max_replica_ids || r->replicas > s.cfg.max_resident_replicas)
         return fail_with(XW_ERR_CAPACITY, "request has more replicas than the server can hold");
