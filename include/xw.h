@@ -422,6 +422,33 @@ int32_t xw_poll(xw_server* s, uint64_t id, xw_request_result* res, int8_t* best_
  * XW_ERR_TIMEOUT when it is still unfinished. */
 int32_t xw_wait(xw_server* s, uint64_t id, double timeout_seconds, xw_request_result* res,
                 int8_t* best_colmajor);
+/* Checkpoint of a request: the reference writes its best W to best_W.csv
+ * every save_interval during a run (xweigh_cuda.cu:2350-2362).  For a
+ * running request this waits (timeout_seconds < 0: no limit) until the end
+ * of the next engine round that it is resident for and returns its progress
+ * then (moves, iterations, the score and conflicts of its best W) with
+ * best (nullable, n*n column-major) receiving that W: the first solver's,
+ * else the least (score, conflicts, replica).  A finished request: as
+ * xw_poll.  XW_ERR_TIMEOUT when no round ended in time (a queued request
+ * waits for its admission). */
+int32_t xw_checkpoint(xw_server* s, uint64_t id, double timeout_seconds, xw_request_result* res,
+                      int8_t* best_colmajor);
+/* Exact snapshot of a running request's population -- its job entry, every
+ * replica record, its ladder and initial temperature -- as the next engine
+ * round leaves them, written atomically to `path` in the format of
+ * xw_batch_save (one job).  Resume it in a server with xw_submit_snapshot
+ * or as a batch with xw_batch_load: the search continues move for move.
+ * Fails with XW_ERR_INVALID for a finished request, XW_ERR_IO when the file
+ * cannot be written, XW_ERR_TIMEOUT when no round ended in time (the
+ * snapshot is then still written, its result dropped).  The engine thread
+ * writes the file, which delays the next round by that long.  No
+ * counterpart in the reference, which can only restart from a CSV. */
+int32_t xw_request_save(xw_server* s, uint64_t id, const char* path, double timeout_seconds);
+/* Queue a request that continues the population of a one-job snapshot
+ * (xw_request_save, or xw_batch_save of a batch of one job of an order the
+ * server takes).  Its parameters are the snapshot's; device, replicas and
+ * stop rule are the server's, as for xw_submit. */
+int32_t xw_submit_snapshot(xw_server* s, const char* path, uint64_t* id);
 /* Cancel: a queued request ends at once, a resident one at the end of the
  * current round with its best W so far.  No effect on finished requests. */
 int32_t xw_cancel(xw_server* s, uint64_t id);

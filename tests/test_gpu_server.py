@@ -195,3 +195,64 @@ def test_least_attained_schedule_runs_one_request_per_round_at_capacity():
     out, st = serve(reqs, max_active_replicas=256)
     assert all(r.state == X.REQ_DONE and r.iterations == 2000 for r, _ in out)
     assert st.rounds == 12 and st.schedule == X.SCHED_LEAST_ATTAINED
+
+
+def test_checkpoint_of_a_running_request_reports_its_best_so_far():
+    """xw_checkpoint: the best W of a running request at the end of its next
+    round, with that W's own score; later checkpoints never get worse."""
+    n, w = 30, 29
+    with X.Server(quantum_iters=500) as s:
+        rid = s.submit(**req(n, w, 77, 64, 10 ** 6))
+        r1, W1 = s.checkpoint(rid, timeout=120)
+        assert r1.state == X.REQ_RUNNING and r1.iterations >= 500
+        st = X.score(n, w, W1)
+        assert (st[0], st[1]) == (r1.score, r1.conflicts)
+        r2, W2 = s.checkpoint(rid, timeout=120)
+        assert r2.iterations > r1.iterations
+        assert (r2.score, r2.conflicts) <= (r1.score, r1.conflicts)
+        st = X.score(n, w, W2)
+        assert (st[0], st[1]) == (r2.score, r2.conflicts)
+        s.cancel(rid)
+        res, _ = s.wait(rid, timeout=120)
+        assert res.state == X.REQ_CANCELLED
+
+
+@pytest.mark.parametrize("tempering", [0, 1])
+def test_request_snapshot_resumes_move_for_move(tmp_path, tempering):
+    """xw_request_save + xw_submit_snapshot: a request saved after a few
+    rounds, cancelled, and resumed in another server ends exactly as the
+    same request run without interruption (rounds of the same length from
+    the same iteration counts)."""
+    kw = dict(tempering=1, exchange_interval=1000, t_min=0.1, t_init=6.0) if tempering else {}
+    r = req(30, 29, 91, 32, 12000, **kw)
+    (ref, Wref), = serve([r], quantum_iters=500)[0]
+    path = tmp_path / "request.xwpop"
+    with X.Server(quantum_iters=500) as s:
+        rid = s.submit(**r)
+        for _ in range(3):
+            s.checkpoint(rid, timeout=120)
+        s.save(rid, path, timeout=120)
+        s.cancel(rid)
+        s.wait(rid, timeout=120)
+    with X.Server(quantum_iters=500) as s:
+        rid = s.submit_snapshot(path)
+        res, W = s.wait(rid, timeout=300)
+    assert res.state == X.REQ_DONE and res.status == X.XW_OK
+    assert (res.best_replica, res.score, res.conflicts, res.moves, res.candidate_evaluations, res.iterations) == \
+        (ref.best_replica, ref.score, ref.conflicts, ref.moves, ref.candidate_evaluations, ref.iterations)
+    assert (W == Wref).all()
+    # the same snapshot also resumes as a batch
+    b = X.Batch.load(path, [{"n": 30, "w": 29, "replicas": 32}])
+    b.run(500)
+    b.synchronize()
+    (jr, _), = b.results()
+    assert jr.error == 0
+    b.close()
+
+
+def test_saving_a_finished_request_is_refused(tmp_path):
+    with X.Server(quantum_iters=500) as s:
+        rid = s.submit(**req(12, 11, 5, 8, 200000))
+        s.wait(rid, timeout=120)
+        with pytest.raises(X.XwError):
+            s.save(rid, tmp_path / "late.xwpop", timeout=10)

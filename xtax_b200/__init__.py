@@ -207,6 +207,9 @@ def lib():
             "xw_poll": (i32, [C.c_void_p, u64, P(RequestResult), P(i8)]),
             "xw_wait": (i32, [C.c_void_p, u64, C.c_double, P(RequestResult), P(i8)]),
             "xw_cancel": (i32, [C.c_void_p, u64]),
+            "xw_checkpoint": (i32, [C.c_void_p, u64, C.c_double, P(RequestResult), P(i8)]),
+            "xw_request_save": (i32, [C.c_void_p, u64, C.c_char_p, C.c_double]),
+            "xw_submit_snapshot": (i32, [C.c_void_p, C.c_char_p, P(u64)]),
             "xw_release": (i32, [C.c_void_p, u64]),
             "xw_server_get_stats": (i32, [C.c_void_p, P(ServerStats)]),
             "xw_server_destroy": (None, [C.c_void_p]),
@@ -596,6 +599,28 @@ class Server:
         W = np.zeros(n * n, dtype=np.int8)
         _check(lib().xw_wait(self.h, rid, float(timeout), C.byref(res), _i8(W)))
         return self._out(rid, res, W)
+
+    def checkpoint(self, rid, timeout=-1.0):
+        """xw_checkpoint: (result, best W so far) at the end of the request's
+        next round; a finished request's final result and W."""
+        res = RequestResult()
+        n = self._orders.get(rid, MAX_ORDER_SHARED)
+        W = np.zeros(n * n, dtype=np.int8)
+        _check(lib().xw_checkpoint(self.h, rid, float(timeout), C.byref(res), _i8(W)))
+        return res, W
+
+    def save(self, rid, path, timeout=-1.0):
+        """xw_request_save: exact snapshot of a running request's population."""
+        _check(lib().xw_request_save(self.h, rid, os.fspath(path).encode(), float(timeout)))
+
+    def submit_snapshot(self, path):
+        """xw_submit_snapshot: continue a one-job snapshot as a new request."""
+        rid = C.c_uint64()
+        _check(lib().xw_submit_snapshot(self.h, os.fspath(path).encode(), C.byref(rid)))
+        res = RequestResult()
+        _check(lib().xw_poll(self.h, rid.value, C.byref(res), None))
+        self._orders[rid.value] = res.n
+        return rid.value
 
     def cancel(self, rid):
         _check(lib().xw_cancel(self.h, rid))

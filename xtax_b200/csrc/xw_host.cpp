@@ -450,39 +450,28 @@ void Batch::upload(const std::vector<uint8_t>& host) {
     configure_shape(params.warps_per_block);
 }
 
-// Population snapshot: the job table and every replica record as they are on
-// the device now, with the batch's parameters, ladder and initial
-// temperatures.  Layout (native byte order, this build's struct sizes):
-//   "XWPOP001" | u32 sizeof(XwJob), sizeof(RepHeader), sizeof(xw_params), njobs
-//   | u64 replicas, arena bytes, ladder entries | xw_params | XwJob[njobs]
-//   | u64 record offsets[replicas] | f64 ladder[] | f64 t_init[njobs] | arena
-// written to a temporary file and renamed into place.
+// Population snapshots (the format is described with Snapshot): a batch
+// saves its job table and records as they are on the device now.
 static const char kSnapMagic[8] = {'X', 'W', 'P', 'O', 'P', '0', '0', '1'};
 
-void Batch::save(const std::string& path) {
-    std::vector<XwJob> dj(jobs.size());
-    std::vector<uint8_t> arena(arena_bytes);
-    check(cudaMemcpyAsync(dj.data(), d_jobs, sizeof(XwJob) * dj.size(), cudaMemcpyDeviceToHost, stream),
-          "read job table");
-    check(cudaMemcpyAsync(arena.data(), d_arena, arena_bytes, cudaMemcpyDeviceToHost, stream), "read records");
-    check(cudaStreamSynchronize(stream), "cudaStreamSynchronize snapshot");
+void write_snapshot(const std::string& path, const Snapshot& sn) {
     const std::string tmp = path + ".tmp";
     FILE* f = std::fopen(tmp.c_str(), "wb");
     if (!f) throw std::runtime_error("cannot write snapshot " + tmp);
     bool ok = true;
     auto put = [&](const void* p, size_t n) { ok = ok && std::fwrite(p, 1, n, f) == n; };
     const uint32_t sizes[4] = {(uint32_t)sizeof(XwJob), (uint32_t)sizeof(RepHeader), (uint32_t)sizeof(xw_params),
-                               (uint32_t)jobs.size()};
-    const uint64_t counts[3] = {total_replicas, arena_bytes, ladder.size()};
+                               (uint32_t)sn.jobs.size()};
+    const uint64_t counts[3] = {sn.rec_off.size(), sn.arena.size(), sn.ladder.size()};
     put(kSnapMagic, 8);
     put(sizes, sizeof sizes);
     put(counts, sizeof counts);
-    put(&params, sizeof params);
-    put(dj.data(), sizeof(XwJob) * dj.size());
-    put(rec_off.data(), sizeof(uint64_t) * rec_off.size());
-    put(ladder.data(), sizeof(double) * ladder.size());
-    put(t_init_used.data(), sizeof(double) * t_init_used.size());
-    put(arena.data(), arena.size());
+    put(&sn.params, sizeof sn.params);
+    put(sn.jobs.data(), sizeof(XwJob) * sn.jobs.size());
+    put(sn.rec_off.data(), sizeof(uint64_t) * sn.rec_off.size());
+    put(sn.ladder.data(), sizeof(double) * sn.ladder.size());
+    put(sn.t_init.data(), sizeof(double) * sn.t_init.size());
+    put(sn.arena.data(), sn.arena.size());
     ok = (std::fclose(f) == 0) && ok;
     if (!ok || std::rename(tmp.c_str(), path.c_str()) != 0) {
         std::remove(tmp.c_str());
@@ -490,7 +479,7 @@ void Batch::save(const std::string& path) {
     }
 }
 
-void Batch::load(const std::string& path, const xw_params* over) {
+Snapshot read_snapshot(const std::string& path) {
     FILE* f = std::fopen(path.c_str(), "rb");
     if (!f) throw std::invalid_argument("cannot open snapshot " + path);
     bool ok = true;
@@ -507,38 +496,67 @@ void Batch::load(const std::string& path, const xw_params* over) {
         std::fclose(f);
         throw std::invalid_argument("not a population snapshot of this build: " + path);
     }
-    get(&params, sizeof params);
-    jobs.resize(sizes[3]);
-    get(jobs.data(), sizeof(XwJob) * jobs.size());
-    rec_off.resize(counts[0]);
-    get(rec_off.data(), sizeof(uint64_t) * rec_off.size());
-    ladder.resize(counts[2]);
-    get(ladder.data(), sizeof(double) * ladder.size());
-    t_init_used.resize(jobs.size());
-    get(t_init_used.data(), sizeof(double) * t_init_used.size());
-    std::vector<uint8_t> host(counts[1]);
-    get(host.data(), host.size());
+    Snapshot sn;
+    get(&sn.params, sizeof sn.params);
+    sn.jobs.resize(sizes[3]);
+    get(sn.jobs.data(), sizeof(XwJob) * sn.jobs.size());
+    sn.rec_off.resize(counts[0]);
+    get(sn.rec_off.data(), sizeof(uint64_t) * sn.rec_off.size());
+    sn.ladder.resize(counts[2]);
+    get(sn.ladder.data(), sizeof(double) * sn.ladder.size());
+    sn.t_init.resize(sn.jobs.size());
+    get(sn.t_init.data(), sizeof(double) * sn.t_init.size());
+    sn.arena.resize(counts[1]);
+    get(sn.arena.data(), sn.arena.size());
     std::fclose(f);
     if (!ok) throw std::invalid_argument("truncated population snapshot: " + path);
     // the saved records must lie inside the arena and name their own job
     uint64_t total = 0;
-    for (size_t j = 0; j < jobs.size(); ++j) {
-        const XwJob& J = jobs[j];
-        if (J.n < 1 || J.n > XW_MAX_ORDER_CUDA || J.replicas < 1 || (uint64_t)J.rep_begin + J.replicas > counts[0])
+    for (size_t j = 0; j < sn.jobs.size(); ++j) {
+        const XwJob& J = sn.jobs[j];
+        if (J.n < 1 || J.n > XW_MAX_ORDER_CUDA || J.replicas < 1 ||
+            (uint64_t)J.rep_begin + J.replicas > counts[0])
             throw std::invalid_argument("corrupt population snapshot: " + path);
         for (int r = 0; r < J.replicas; ++r) {
-            const uint64_t off = rec_off[J.rep_begin + r];
-            if (off + J.record_bytes > host.size() ||
-                reinterpret_cast<const RepHeader*>(host.data() + off)->job != (uint32_t)j)
+            const uint64_t off = sn.rec_off[J.rep_begin + r];
+            if (off + J.record_bytes > sn.arena.size() ||
+                reinterpret_cast<const RepHeader*>(sn.arena.data() + off)->job != (uint32_t)j)
                 throw std::invalid_argument("corrupt population snapshot: " + path);
         }
         total += (uint64_t)J.replicas;
     }
     if (total != counts[0]) throw std::invalid_argument("corrupt population snapshot: " + path);
     // a snapshot holds no Gram arena: the large-order kernel rebuilds it
-    for (size_t j = 0; j < jobs.size(); ++j)
-        for (int r = 0; r < jobs[j].replicas; ++r)
-            reinterpret_cast<RepHeader*>(host.data() + rec_off[jobs[j].rep_begin + r])->status &= ~XW_STATUS_GRAM;
+    for (size_t j = 0; j < sn.jobs.size(); ++j)
+        for (int r = 0; r < sn.jobs[j].replicas; ++r)
+            reinterpret_cast<RepHeader*>(sn.arena.data() + sn.rec_off[sn.jobs[j].rep_begin + r])->status &=
+                ~XW_STATUS_GRAM;
+    return sn;
+}
+
+void Batch::save(const std::string& path) {
+    Snapshot sn;
+    sn.params = params;
+    sn.jobs.resize(jobs.size());
+    sn.arena.resize(arena_bytes);
+    check(cudaMemcpyAsync(sn.jobs.data(), d_jobs, sizeof(XwJob) * sn.jobs.size(), cudaMemcpyDeviceToHost, stream),
+          "read job table");
+    check(cudaMemcpyAsync(sn.arena.data(), d_arena, arena_bytes, cudaMemcpyDeviceToHost, stream), "read records");
+    check(cudaStreamSynchronize(stream), "cudaStreamSynchronize snapshot");
+    sn.rec_off = rec_off;
+    sn.ladder = ladder;
+    sn.t_init = t_init_used;
+    write_snapshot(path, sn);
+}
+
+void Batch::load(const std::string& path, const xw_params* over) {
+    Snapshot sn = read_snapshot(path);
+    params = sn.params;
+    jobs = std::move(sn.jobs);
+    rec_off = std::move(sn.rec_off);
+    ladder = std::move(sn.ladder);
+    t_init_used = std::move(sn.t_init);
+    std::vector<uint8_t> host = std::move(sn.arena);
     if (over) {
         // run-time settings may change on resume; the search itself may not
         params.device = over->device;

@@ -124,6 +124,27 @@ struct Batch {
     void fill_results(const std::vector<JobOut>& out, const int8_t* best_host, xw_job_result* res) const;
 };
 
+// Population snapshot: the job table and every replica record, with the
+// parameters, ladder and initial temperatures.  File layout (native byte
+// order, this build's struct sizes):
+//   "XWPOP001" | u32 sizeof(XwJob), sizeof(RepHeader), sizeof(xw_params), njobs
+//   | u64 replicas, arena bytes, ladder entries | xw_params | XwJob[njobs]
+//   | u64 record offsets[replicas] | f64 ladder[] | f64 t_init[njobs] | arena
+// written to a temporary file and renamed into place.  Batches and served
+// requests write and read the same format.
+struct Snapshot {
+    xw_params params{};
+    std::vector<XwJob> jobs;
+    std::vector<uint64_t> rec_off;
+    std::vector<double> ladder;
+    std::vector<double> t_init;
+    std::vector<uint8_t> arena;
+};
+void write_snapshot(const std::string& path, const Snapshot& sn);
+// checks that every record lies in the arena and names its job; clears the
+// records' Gram-arena bits
+Snapshot read_snapshot(const std::string& path);
+
 // The escape-move scan of an elite restart on the device (xw_restart.cu): the
 // `limit` best support switches out of the column-major W (G its Gram,
 // row-major) by (score delta, conflict delta, scan order).

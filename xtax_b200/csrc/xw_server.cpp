@@ -122,6 +122,14 @@ struct Request {
     // result
     xw_request_result res{};
     std::vector<int8_t> best;
+    // checkpoints and snapshots, taken by the engine at the end of a round
+    bool ckpt_want = false;
+    uint64_t ckpt_seq = 0;                      // checkpoints taken so far
+    xw_request_result ckpt_res{};
+    std::vector<int8_t> ckpt_best;
+    std::deque<std::pair<uint64_t, std::string>> saves;   // (ticket, path) pending
+    uint64_t save_tickets = 0, saves_done = 0;
+    std::map<uint64_t, std::pair<int32_t, std::string>> save_results;
 };
 
 using ReqPtr = std::shared_ptr<Request>;
@@ -190,6 +198,7 @@ struct Server {
     int blocks_for(int cls, bool general, uint32_t slot_bytes, int wpb, size_t items);
     void round(bool& any_tempering);
     void retire(const ReqPtr& q, const JobOut& o, double t_host, uint64_t stamp, int state);
+    void checkpoint(const ReqPtr& q, const JobOut& o, bool want_best, size_t nsaves);
     void finish_locked(const ReqPtr& q, int state);
     void fail_all(const std::string& msg);
 };
@@ -212,6 +221,10 @@ void fill_result_header(Request& q) {
 }  // namespace
 
 void Server::finish_locked(const ReqPtr& q, int state) {
+    for (const auto& sv : q->saves)
+        q->save_results[sv.first] = {XW_ERR_INVALID, "request finished before its snapshot was taken"};
+    q->saves.clear();
+    q->saves_done = q->save_tickets;
     q->state = state;
     q->t_finish = now();
     q->records.clear();
@@ -539,6 +552,87 @@ void Server::retire(const ReqPtr& q, const JobOut& o, double t_host, uint64_t st
     finish_locked(q, state);
 }
 
+// Engine thread, after a round: the request's best W so far and its
+// progress (want_best), and its first `nsaves` pending snapshots: the job
+// entry and every replica record as this round left them, as a one-job
+// population snapshot.
+void Server::checkpoint(const ReqPtr& q, const JobOut& o, bool want_best, size_t nsaves) {
+    const int n = q->spec.n, w = q->spec.w, R = q->spec.replicas;
+    if (want_best) {
+        std::vector<int8_t> W((size_t)n * n);
+        check_cuda(cudaMemcpy(W.data(), d_best + (size_t)q->slot * kBestStride, W.size(), cudaMemcpyDeviceToHost),
+                   "read request best state");
+        int64_t st[4] = {0, 0, 0, 0};
+        xw_score(n, w, W.data(), st);
+        std::lock_guard<std::mutex> lk(mu);
+        xw_request_result r = q->res;
+        r.solved = o.first_solver >= 0;
+        r.best_replica = o.best_replica;
+        r.score = st[0];
+        r.conflicts = st[1];
+        r.moves = o.moves;
+        r.candidate_evaluations = o.cand_evals;
+        r.iterations = o.iters;
+        r.solved_iteration = o.first_solver >= 0 ? o.solved_it : 0;
+        r.t_init = q->t_init;
+        q->ckpt_res = r;
+        q->ckpt_best = std::move(W);
+        q->ckpt_want = false;
+        ++q->ckpt_seq;
+        cv_done.notify_all();
+    }
+    if (nsaves == 0) return;
+    xw::Snapshot sn;
+    std::string err;
+    try {
+        sn.jobs.resize(1);
+        sn.arena.resize((size_t)R * q->job.record_bytes);
+        check_cuda(cudaMemcpy(sn.jobs.data(), d_jobs + q->slot, sizeof(XwJob), cudaMemcpyDeviceToHost),
+                   "read request job");
+        check_cuda(cudaMemcpy(sn.arena.data(), d_arena + q->arena_off, sn.arena.size(), cudaMemcpyDeviceToHost),
+                   "read request records");
+        XwJob& J = sn.jobs[0];
+        J.rep_begin = 0;
+        J.ladder_off = 0;
+        sn.rec_off.resize(R);
+        for (int r = 0; r < R; ++r) {
+            sn.rec_off[r] = (uint64_t)r * J.record_bytes;
+            reinterpret_cast<RepHeader*>(sn.arena.data() + sn.rec_off[r])->job = 0;
+        }
+        sn.ladder = q->has_ladder ? q->temps : std::vector<double>(1, 0.0);
+        sn.t_init.assign(1, q->t_init);
+        sn.params = q->params;
+    } catch (const std::exception& e) {
+        err = e.what();
+    }
+    for (size_t k = 0; k < nsaves; ++k) {
+        std::pair<uint64_t, std::string> sv;
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            if (q->saves.empty()) break;
+            sv = q->saves.front();
+            q->saves.pop_front();
+        }
+        int32_t code = XW_OK;
+        std::string msg = err;
+        if (!err.empty()) {
+            code = XW_ERR_CUDA;
+        } else {
+            try {
+                xw::write_snapshot(sv.second, sn);
+            } catch (const std::exception& e) {
+                code = XW_ERR_IO;
+                msg = e.what();
+            }
+        }
+        std::lock_guard<std::mutex> lk(mu);
+        q->save_results[sv.first] = {code, msg};
+        q->saves_done = std::max(q->saves_done, sv.first);
+        cv_done.notify_all();
+    }
+    if (!err.empty()) throw std::runtime_error(err);
+}
+
 void Server::fail_all(const std::string& msg) {
     std::lock_guard<std::mutex> lk(mu);
     fatal = msg;
@@ -577,12 +671,21 @@ void Server::engine_loop() {
             const double t_host = now();
             const uint64_t stamp = *h_stamp;
             for (int s : selected) slot_req[s]->attained = h_out[s].iters;
+            std::vector<std::pair<ReqPtr, std::pair<bool, size_t>>> wanted;
             {
                 std::lock_guard<std::mutex> lk(mu);
                 stats.busy_seconds += t_host - t_round0;
                 cancel_flag.resize(slot_req.size(), 0);
-                for (int s : active) cancel_flag[s] = slot_req[s]->cancel;
+                for (int s : active) {
+                    const ReqPtr& q = slot_req[s];
+                    cancel_flag[s] = q->cancel;
+                    if (q->ckpt_want || !q->saves.empty())
+                        wanted.push_back({q, {q->ckpt_want, q->saves.size()}});
+                }
             }
+            // checkpoints and snapshots asked for since the last round, of
+            // the state this round left (before any request retires)
+            for (const auto& wv : wanted) checkpoint(wv.first, h_out[wv.first->slot], wv.second.first, wv.second.second);
             std::vector<int> keep;
             keep.reserve(active.size());
             const std::vector<int> current(active);
@@ -878,6 +981,151 @@ int32_t xw_wait(xw_server* h, uint64_t id, double timeout_seconds, xw_request_re
         return fail_with(XW_ERR_TIMEOUT, "request is still running");
     }
     copy_out(*q, res, best);
+    return XW_OK;
+}
+
+int32_t xw_checkpoint(xw_server* h, uint64_t id, double timeout_seconds, xw_request_result* res, int8_t* best) {
+    if (!h) return fail_with(XW_ERR_INVALID, "server is null");
+    Server& s = h->s;
+    std::unique_lock<std::mutex> lk(s.mu);
+    auto it = s.table.find(id);
+    if (it == s.table.end()) return fail_with(XW_ERR_NOT_FOUND, xw::strfmt("unknown request %llu",
+                                                                           (unsigned long long)id));
+    ReqPtr q = it->second;
+    if (q->state >= XW_REQ_DONE) {
+        copy_out(*q, res, best);
+        return XW_OK;
+    }
+    const uint64_t seq0 = q->ckpt_seq;
+    q->ckpt_want = true;
+    s.cv_engine.notify_one();
+    auto ready = [&] { return q->ckpt_seq > seq0 || q->state >= XW_REQ_DONE; };
+    if (timeout_seconds < 0.0) {
+        s.cv_done.wait(lk, ready);
+    } else if (!s.cv_done.wait_for(lk, std::chrono::duration<double>(timeout_seconds), ready)) {
+        copy_out(*q, res, nullptr);
+        return fail_with(XW_ERR_TIMEOUT, "no engine round has ended for the request yet");
+    }
+    if (q->state >= XW_REQ_DONE) {
+        copy_out(*q, res, best);
+        return XW_OK;
+    }
+    if (res) {
+        copy_out(*q, res, nullptr);
+        const int32_t state = res->state, status = res->status;
+        const double ts = res->submit_seconds, ta = res->admit_seconds, tf = res->finish_seconds;
+        char error[sizeof res->error];
+        std::memcpy(error, res->error, sizeof error);
+        *res = q->ckpt_res;
+        res->state = state;
+        res->status = status;
+        res->n = q->spec.n;
+        res->w = q->spec.w;
+        res->replicas = q->spec.replicas;
+        res->submit_seconds = ts;
+        res->admit_seconds = ta;
+        res->finish_seconds = tf;
+        std::memcpy(res->error, error, sizeof error);
+    }
+    if (best && !q->ckpt_best.empty()) std::memcpy(best, q->ckpt_best.data(), q->ckpt_best.size());
+    return XW_OK;
+}
+
+int32_t xw_request_save(xw_server* h, uint64_t id, const char* path, double timeout_seconds) {
+    if (!h || !path || !*path) return fail_with(XW_ERR_INVALID, "server and path must be non-null");
+    Server& s = h->s;
+    std::unique_lock<std::mutex> lk(s.mu);
+    auto it = s.table.find(id);
+    if (it == s.table.end()) return fail_with(XW_ERR_NOT_FOUND, xw::strfmt("unknown request %llu",
+                                                                           (unsigned long long)id));
+    ReqPtr q = it->second;
+    if (q->state >= XW_REQ_DONE)
+        return fail_with(XW_ERR_INVALID, "request has finished: its population is no longer resident");
+    const uint64_t ticket = ++q->save_tickets;
+    q->saves.emplace_back(ticket, std::string(path));
+    s.cv_engine.notify_one();
+    auto done = [&] { return q->saves_done >= ticket; };
+    if (timeout_seconds < 0.0) {
+        s.cv_done.wait(lk, done);
+    } else if (!s.cv_done.wait_for(lk, std::chrono::duration<double>(timeout_seconds), done)) {
+        // the snapshot may still be written later; its result is dropped
+        return fail_with(XW_ERR_TIMEOUT, "no engine round has ended for the request yet");
+    }
+    auto r = q->save_results.find(ticket);
+    if (r == q->save_results.end()) return fail_with(XW_ERR_INTERNAL, "snapshot result missing");
+    const std::pair<int32_t, std::string> out = r->second;
+    q->save_results.erase(r);
+    if (out.first != XW_OK) return fail_with(out.first, out.second);
+    return XW_OK;
+}
+
+int32_t xw_submit_snapshot(xw_server* h, const char* path, uint64_t* id) {
+    if (!h || !path || !id) return fail_with(XW_ERR_INVALID, "server, path and id must be non-null");
+    Server& s = h->s;
+    xw::Snapshot sn;
+    try {
+        sn = xw::read_snapshot(path);
+    } catch (const std::exception& e) {
+        return fail_with(XW_ERR_INVALID, e.what());
+    }
+    if (sn.jobs.size() != 1) return fail_with(XW_ERR_INVALID, "a request snapshot holds exactly one job");
+    XwJob J = sn.jobs[0];
+    const int R = J.replicas;
+    if (J.n > XW_MAX_ORDER_SHARED || J.large)
+        return fail_with(XW_ERR_CAPACITY, xw::strfmt("order %d is beyond the served orders' maximum of %d", J.n,
+                                                     XW_MAX_ORDER_SHARED));
+    if (R > s.cfg.max_replica_ids || R > s.cfg.max_resident_replicas)
+        return fail_with(XW_ERR_CAPACITY, "request has more replicas than the server can hold");
+    if ((uint64_t)R * J.record_bytes > s.cfg.arena_bytes)
+        return fail_with(XW_ERR_CAPACITY, "request records exceed the server arena");
+    xw_params p = sn.params;
+    p.device = s.cfg.device;
+    p.stop_on_solve = 2;
+    p.replicas = R;
+    if (p.tempering) {
+        if (R > XW_MAX_RUNGS)
+            return fail_with(XW_ERR_INVALID, xw::strfmt("a tempering ladder has at most %d rungs", XW_MAX_RUNGS));
+        if (p.exchange_interval % s.cfg.quantum_iters != 0)
+            return fail_with(XW_ERR_INVALID, xw::strfmt("exchange interval %d is not a multiple of the server "
+                                                        "quantum %d", p.exchange_interval, s.cfg.quantum_iters));
+        if ((uint64_t)J.ladder_off + R > sn.ladder.size())
+            return fail_with(XW_ERR_INVALID, "corrupt population snapshot: ladder");
+    }
+    auto q = std::make_shared<xw::Request>();
+    q->spec.n = J.n;
+    q->spec.w = J.w;
+    q->spec.seed = 0;
+    q->spec.replicas = R;
+    q->spec.max_moves = 0;
+    q->params = p;
+    // a batch snapshot exchanges after every launch of exchange_interval
+    // iterations; the server at the same iteration counts
+    J.exchange_iters = p.tempering ? (uint64_t)p.exchange_interval : 0;
+    J.done = 0;
+    q->records.resize((size_t)R * J.record_bytes);
+    for (int r = 0; r < R; ++r) {
+        const uint8_t* src = sn.arena.data() + sn.rec_off[J.rep_begin + r];
+        std::memcpy(q->records.data() + (size_t)r * J.record_bytes, src, J.record_bytes);
+        q->attained = std::max(q->attained, reinterpret_cast<const RepHeader*>(src)->it);
+    }
+    if (p.tempering) q->temps.assign(sn.ladder.begin() + J.ladder_off, sn.ladder.begin() + J.ladder_off + R);
+    q->t_init = sn.t_init[0];
+    J.rep_begin = 0;
+    J.ladder_off = 0;
+    q->job = J;
+    std::lock_guard<std::mutex> lk(s.mu);
+    if (!s.fatal.empty()) return fail_with(XW_ERR_CUDA, s.fatal);
+    if (s.stopping) return fail_with(XW_ERR_INVALID, "server is stopping");
+    q->id = s.next_id++;
+    q->t_submit = s.now();
+    q->res.admit_seconds = -1.0;
+    q->res.finish_seconds = -1.0;
+    q->res.time_to_solution_seconds = -1.0;
+    s.table[q->id] = q;
+    s.ready[q->id] = q;   // built already: straight to admission
+    ++s.stats.submitted;
+    s.cv_engine.notify_one();
+    *id = q->id;
     return XW_OK;
 }
 
