@@ -12,7 +12,8 @@
 // rows of that array (4 matrices of n=32, 2 of n=64, 1 of n=96 or 128),
 // loaded by TMA with 128-byte swizzle into shared memory, the K (column)
 // extent zero-filled to 128.  One MMA chain computes D = A A^T (M = 128,
-// N = rows of the tile, K = 128 in four K=32 steps) into a TMEM
+// N = rows of the tile, K in ceil(n/32) steps of 32: the zero-filled
+// columns past n are not multiplied) into a TMEM
 // accumulator; the diagonal n x n blocks of D are the tile's Gram matrices.
 // The epilogue warps read their TMEM lane quarter (one row per thread) and
 // reduce the row statistics per matrix.  The kernel is persistent over
@@ -181,6 +182,9 @@ __global__ void __launch_bounds__(128, 4) rescore_tc_kernel(const __grid_constan
         }
     }
     const uint32_t idesc = instr_desc(p.rows_per_tile);
+    // K steps of 32 columns that hold matrix entries; the box's columns past
+    // n are zero-filled by the TMA load and add nothing to the product
+    const int ksteps = (p.n + 31) / 32;
     int iter = 0;
     for (int t = blockIdx.x; t < p.ntiles; t += grid, ++iter) {
         const int s = iter % kStages;
@@ -192,8 +196,9 @@ __global__ void __launch_bounds__(128, 4) rescore_tc_kernel(const __grid_constan
             } else {
                 asm volatile("tcgen05.fence::after_thread_sync;");
                 const uint64_t d = smem_desc(tiles + s * kTileBytes);
-#pragma unroll
-                for (int k = 0; k < 4; ++k) mma_i8(tmem, d + (uint64_t)(2 * k), d + (uint64_t)(2 * k), idesc, k > 0);
+#pragma unroll 1
+                for (int k = 0; k < ksteps; ++k)
+                    mma_i8(tmem, d + (uint64_t)(2 * k), d + (uint64_t)(2 * k), idesc, k > 0);
                 mma_commit(&mma_bar);
             }
         }
