@@ -1,0 +1,69 @@
+"""Chunked launches: more replicas than resident warps.
+
+A batch whose replicas outnumber the device's resident warps splits each
+replica's iterations per launch into consecutive chunks, scheduled
+chunk-major (a chunk waits for its replica's previous one), so that the last
+wave of a launch is not part-filled.  Each replica still runs its iterations
+in order, so every replica state is identical whatever the chunk count
+(XW_CHUNKS forces one), and the oracle replays them.
+"""
+import pytest
+
+import oracle_lib as O
+import xtax_b200 as X
+from test_gpu_parity import compare, oracle_job, start_of
+
+pytestmark = pytest.mark.gpu
+
+
+def run_states(monkeypatch, chunks, jobs, p, iters):
+    if chunks is None:
+        monkeypatch.delenv("XW_CHUNKS", raising=False)
+    else:
+        monkeypatch.setenv("XW_CHUNKS", str(chunks))
+    b = X.Batch(jobs, p)
+    b.run(iters)
+    b.synchronize()
+    states = []
+    for j, jb in enumerate(jobs):
+        for r in range(jb["replicas"]):
+            st, W, B, M = b.replica(j, r)
+            assert st.error == 0
+            states.append((st.iterations, st.moves, st.candidate_evaluations, st.score, st.conflicts,
+                           st.best_score, st.best_conflicts, st.objective_total, st.temperature, st.rung,
+                           W.tobytes(), B.tobytes(), M.tobytes()))
+    results = [(r.score, r.conflicts, r.best_replica, r.moves) for r, _ in b.results()]
+    b.close()
+    return states, results
+
+
+@pytest.mark.parametrize("tempering", [0, 1])
+def test_chunked_launches_leave_every_replica_unchanged(monkeypatch, tempering):
+    # 3600 replicas: more than the 2368 resident warps of a B200 for these orders
+    jobs = [{"n": 12, "w": 11, "seed": 40 + k, "replicas": 16} for k in range(150)] + \
+           [{"n": 14, "w": 7, "seed": 900 + k, "replicas": 16} for k in range(75)]
+    if tempering:
+        p = X.Params(stop_on_solve=0, tempering=1, exchange_interval=400, t_min=0.1, t_init=6.0,
+                     squared_objective_fraction=0.0, parity_objective_fraction=0.0)
+    else:
+        p = X.Params(stop_on_solve=0, t_init=4.0, moves_per_launch=400, stuck_threshold=300, moves_per_cool=40)
+    base = run_states(monkeypatch, 1, jobs, p, 1200)
+    assert run_states(monkeypatch, None, jobs, p, 1200) == base     # the batch's own choice
+    assert run_states(monkeypatch, 5, jobs, p, 1200) == base
+
+
+def test_chunked_launch_matches_oracle(monkeypatch):
+    monkeypatch.setenv("XW_CHUNKS", "4")
+    n, w, R, iters = 13, 9, 3000, 900
+    p = X.Params(stop_on_solve=0, t_init=4.0, moves_per_launch=300)
+    seed = 4321
+    b = X.Batch([{"n": n, "w": w, "seed": seed, "replicas": R}], p)
+    temps = {r: b.replica(0, r)[0].reheat_temperature for r in (0, 1, 1777, R - 1)}
+    b.run(iters)
+    b.synchronize()
+    job = oracle_job(n, w, seed, p)
+    for r, t in temps.items():
+        rep = O.Replica(job, r, start_of(n, w, seed, r, p), t, r)
+        rep.run(iters, stop_on_solve=False)
+        compare(b, 0, r, rep)
+    b.close()

@@ -530,7 +530,7 @@ __device__ __forceinline__ uint64_t globaltimer() {
 }
 
 template <int OPL, bool GEN>
-__device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int lane) {
+__device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int lane, uint64_t chunk_iters) {
     uint8_t* rec = a.arena + a.rec_off[rid];
     RepHeader* H = reinterpret_cast<RepHeader*>(rec);
     const uint32_t jid = H->job;
@@ -555,7 +555,7 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
     uint64_t* sThr = reinterpret_cast<uint64_t*>(slot + L.off_thr);
 
     uint64_t it = H->it;
-    uint64_t iters = a.iters;
+    uint64_t iters = chunk_iters;
     if (J->budget_iters) {
         if (it >= J->budget_iters) return;
         if (iters > J->budget_iters - it) iters = J->budget_iters - it;
@@ -854,6 +854,31 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
     __syncwarp();
 }
 
+// Chunked launches: chunk c of a replica starts once chunk c-1 has released
+// the replica's record.  Items are taken in chunk-major order by resident
+// warps, so the chunk waited for is running or done; the wait is bounded
+// all the same (about a second) and flags the replica when it gives up.
+constexpr uint32_t kChunkSpinLimit = 1u << 22;
+
+__device__ __noinline__ bool wait_chunk(const uint32_t* flag, uint32_t want) {
+    uint32_t v = 0;
+#pragma unroll 1
+    for (uint32_t spin = 0; spin < kChunkSpinLimit; ++spin) {
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
+        if (v >= want) return true;
+        __nanosleep(256);
+    }
+    return false;
+}
+
+// every lane's record writes are made visible device-wide before lane 0
+// publishes the chunk count
+__device__ __forceinline__ void release_chunk(uint32_t* flag, uint32_t value, int lane) {
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(flag), "r"(value) : "memory");
+}
+
 // Register budget per thread; it sets how many replica warps an SM holds.
 #ifndef XW_ANNEAL_MAXNREG
 #define XW_ANNEAL_MAXNREG 128
@@ -864,12 +889,29 @@ __global__ void __maxnreg__(XW_ANNEAL_MAXNREG) anneal_kernel(AnnealArgs a) {
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     uint8_t* slot = smem + (size_t)warp * a.slot_bytes;
+    const uint64_t total = (uint64_t)a.n_items * a.chunks;
     for (;;) {
         uint32_t item = 0;
         if (lane == 0) item = atomicAdd(a.counter, 1u);
         item = __shfl_sync(FULL, item, 0);
-        if (item >= a.n_items) break;
-        run_replica<OPL, GEN>(a, a.items[item], slot, lane);
+        if (item >= total) break;
+        if (a.chunks == 1) {
+            run_replica<OPL, GEN>(a, a.items[item], slot, lane, a.iters);
+            continue;
+        }
+        const uint32_t c = item / a.n_items;
+        const uint32_t rid = a.items[item - c * a.n_items];
+        const uint64_t lo = a.iters * c / a.chunks, hi = a.iters * (c + 1) / a.chunks;
+        bool ok = true;
+        if (c > 0) ok = __all_sync(FULL, wait_chunk(a.chunk_done + rid, c));
+        __syncwarp();
+        if (ok) {
+            run_replica<OPL, GEN>(a, rid, slot, lane, hi - lo);
+        } else if (lane == 0) {
+            RepHeader* H = reinterpret_cast<RepHeader*>(a.arena + a.rec_off[rid]);
+            atomicOr(&H->err, XW_ERR_CHUNK);
+        }
+        release_chunk(a.chunk_done + rid, c + 1, lane);
     }
 }
 

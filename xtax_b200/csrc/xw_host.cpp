@@ -171,7 +171,7 @@ Batch::~Batch() {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     for (auto e : events) cudaEventDestroy(e);
     for (void* ptr : {d_jobs, d_jobs0, d_arena, d_arena0, d_rec_off, d_items, d_counters, d_ladder,
-                      d_out, d_best_off, d_best, d_t0, d_gram, d_gram_off})
+                      d_out, d_best_off, d_best, d_t0, d_gram, d_gram_off, d_chunk_done})
         if (ptr) cudaFree(ptr);
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
@@ -573,6 +573,21 @@ void Batch::load(const std::string& path, const xw_params* over) {
     upload(host);
 }
 
+uint32_t choose_chunks(uint32_t replicas, uint32_t slots) {
+    if (const char* e = std::getenv("XW_CHUNKS"); e && *e) return (uint32_t)std::clamp(std::atoi(e), 1, 64);
+    if (slots == 0 || replicas <= slots) return 1;
+    uint32_t best = 1;
+    double best_waves = 0.0;
+    for (uint32_t k = 1; k <= 8; ++k) {
+        const double waves = (double)((uint64_t)replicas * k / slots + ((uint64_t)replicas * k % slots != 0)) / k;
+        if (k == 1 || waves < best_waves - 1e-9) {
+            best = k;
+            best_waves = waves;
+        }
+    }
+    return best;
+}
+
 void Batch::configure_shape(int wpb) {
     if (graph_exec) {
         cudaGraphExecDestroy(graph_exec);
@@ -611,8 +626,17 @@ void Batch::configure_shape(int wpb) {
     if (per_sm < 1) throw std::length_error("CUDA anneal kernel has zero occupancy on the selected device");
     warps_per_block = wpb;
     blocks_per_sm = per_sm;
-    const int want = (int)((total_replicas - n_large + wpb - 1) / wpb);
+    const uint32_t small = total_replicas - n_large;
+    const int want = (int)((small + wpb - 1) / wpb);
     blocks = std::max(1, std::min(want, per_sm * props.multiProcessorCount));
+    // More replicas than resident warps: a launch of whole replicas ends in a
+    // part-filled wave (4096 replicas on 2368 warps run 2 waves for 1.73
+    // waves of work).  Split each replica's iterations into k chunks, k in
+    // [1, 8] with the fewest waves per unit of work, the least k on ties.
+    chunks = choose_chunks(small, (uint32_t)(blocks * wpb));
+    if (chunks > 1 && !d_chunk_done)
+        check(cudaMalloc(&d_chunk_done, sizeof(uint32_t) * std::max<uint32_t>(total_replicas, 1)),
+              "cudaMalloc chunk counters");
 }
 
 void Batch::reset() {
@@ -678,6 +702,12 @@ void Batch::enqueue_rounds(uint64_t iters, bool timed) {
             a.n_items = total_replicas - n_large;
             a.slot_bytes = slot_bytes;
             a.counter = static_cast<uint32_t*>(d_counters) + 2 * k;
+            a.chunks = a.iters >= chunks ? chunks : 1;
+            if (a.chunks > 1) {
+                a.chunk_done = static_cast<uint32_t*>(d_chunk_done);
+                check(cudaMemsetAsync(d_chunk_done, 0, sizeof(uint32_t) * total_replicas, stream),
+                      "cudaMemsetAsync chunk counters");
+            }
             check(launch_anneal(a, opl, general, warps_per_block, blocks, stream), "launch anneal_kernel");
         }
         if (timed) check(cudaEventRecord(events[2 * k + 1], stream), "cudaEventRecord");

@@ -42,6 +42,9 @@ int32_t rescore_device(const int8_t* W, int64_t count, int n, int w, int32_t* st
 // Warps per block for the anneal kernel of a given lanes-per-row class and
 // shared-memory slot, from the autotuner's cache (xw_tune.cpp).
 int tuned_warps_per_block(int opl, uint32_t slot_bytes, int device);
+// Chunks per replica and launch for `replicas` on `slots` resident warps
+// (XW_CHUNKS overrides: tests compare chunked and whole-replica launches).
+uint32_t choose_chunks(uint32_t replicas, uint32_t slots);
 // Record the fastest warps per block for that class in the tuning cache.
 void record_tuned(int opl, uint32_t slot_bytes, int wpb);
 
@@ -69,6 +72,10 @@ struct Batch {
     int warps_per_block = 4;
     int blocks_per_sm = 1;
     int blocks = 1;
+    // shared-memory kernel: work items per replica and launch (see
+    // AnnealArgs::chunks), chosen so that the resident warps' waves fill
+    uint32_t chunks = 1;
+    void* d_chunk_done = nullptr;
 
     // jobs with J.large run on the HBM-resident kernel: items[0, n_large)
     // are their replicas; the rest run on the shared-memory kernel

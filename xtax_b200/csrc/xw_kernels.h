@@ -23,6 +23,12 @@ struct AnnealArgs {
     int32_t pad;
     uint8_t* gram = nullptr;            // large-order kernel: Gram and mask arena
     const uint64_t* gram_off = nullptr; // byte offset of each replica's Gram there
+    // The shared-memory kernel can split each replica's `iters` into `chunks`
+    // consecutive work items, scheduled chunk-major, so that a launch with
+    // more replicas than resident warps does not end in a part-filled wave.
+    // chunk_done[rid] (zeroed per launch) counts a replica's finished chunks.
+    uint32_t chunks = 1;
+    uint32_t* chunk_done = nullptr;
 };
 
 // shared-memory bytes one warp needs for a replica of order n, minority m,

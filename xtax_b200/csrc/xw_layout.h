@@ -32,6 +32,7 @@
 #define XW_ERR_SCORE 1u        // rebuilt score differs from the tracked one
 #define XW_ERR_MINORITY 2u     // W row weights disagree with the minority lists
 #define XW_ERR_KERNEL 4u       // a lean launch met a replica that needs the general kernel
+#define XW_ERR_CHUNK 8u        // a chunk's wait for its replica's previous chunk timed out
 
 struct XwJob {
     int32_t n, w, m, sparse;        // m = min(w, n-w); sparse = (w <= n-w)
