@@ -163,6 +163,7 @@ struct Server {
     uint64_t* d_rec_off = nullptr;
     uint32_t* d_items = nullptr;               // kClasses x max_replica_ids
     uint32_t* d_counters = nullptr;            // kClasses
+    uint32_t* d_chunk_done = nullptr;          // max_replica_ids: chunks finished per replica
     double* d_ladder = nullptr;
     JobOut* d_out = nullptr;
     uint64_t* d_best_off = nullptr;
@@ -438,6 +439,25 @@ void Server::round(bool& any_tempering) {
     last_njobs = njobs;
     check_cuda(cudaEventRecord(ev0, stream), "cudaEventRecord");
     check_cuda(cudaMemsetAsync(d_counters, 0, sizeof(uint32_t) * kClasses, stream), "reset work counters");
+    // per class: warps per block, CTAs, and chunks per replica (a class with
+    // more replicas than its resident warps runs chunked, as batches do)
+    int cls_wpb[kClasses] = {}, cls_blocks[kClasses] = {};
+    uint32_t cls_chunks[kClasses] = {};
+    bool any_chunked = false;
+    for (int c = 0; c < kClasses; ++c) {
+        if (items_host[c].empty()) continue;
+        int wpb = cfg.warps_per_block > 0 ? cfg.warps_per_block
+                                          : tuned_warps_per_block(opl_of_class(c), class_slot[c], cfg.device);
+        wpb = std::max(1, std::min(16, wpb));
+        cls_wpb[c] = wpb;
+        cls_blocks[c] = blocks_for(c, class_general[c], class_slot[c], wpb, items_host[c].size());
+        cls_chunks[c] = choose_chunks((uint32_t)items_host[c].size(), (uint32_t)(cls_blocks[c] * wpb));
+        if (cls_chunks[c] > (uint32_t)cfg.quantum_iters) cls_chunks[c] = 1;
+        any_chunked = any_chunked || cls_chunks[c] > 1;
+    }
+    if (any_chunked)
+        check_cuda(cudaMemsetAsync(d_chunk_done, 0, sizeof(uint32_t) * cfg.max_replica_ids, stream),
+                   "reset chunk counters");
     // the classes' persistent launches run side by side on their own
     // streams, so that one launch's tail overlaps the other's work
     int nclass = 0;
@@ -450,9 +470,7 @@ void Server::round(bool& any_tempering) {
             st = side[c];
             check_cuda(cudaStreamWaitEvent(st, fork, 0), "cudaStreamWaitEvent");
         }
-        int wpb = cfg.warps_per_block > 0 ? cfg.warps_per_block
-                                          : tuned_warps_per_block(opl_of_class(c), class_slot[c], cfg.device);
-        wpb = std::max(1, std::min(16, wpb));
+        const int wpb = cls_wpb[c];
         AnnealArgs a;
         a.jobs = d_jobs;
         a.arena = d_arena;
@@ -464,10 +482,9 @@ void Server::round(bool& any_tempering) {
         a.iters = (uint64_t)cfg.quantum_iters;
         a.stop_on_solve = 2;
         a.pad = 0;
-        check_cuda(launch_anneal(a, opl_of_class(c), class_general[c], wpb,
-                                 blocks_for(c, class_general[c], class_slot[c], wpb, items_host[c].size()),
-                                 st),
-                   "launch anneal_kernel");
+        a.chunks = cls_chunks[c];
+        if (a.chunks > 1) a.chunk_done = d_chunk_done;
+        check_cuda(launch_anneal(a, opl_of_class(c), class_general[c], wpb, cls_blocks[c], st), "launch anneal_kernel");
         if (nclass > 1) {
             check_cuda(cudaEventRecord(join[c], st), "cudaEventRecord");
             check_cuda(cudaStreamWaitEvent(stream, join[c], 0), "cudaStreamWaitEvent");
@@ -755,6 +772,7 @@ void Server::start() {
     dmalloc((void**)&d_rec_off, sizeof(uint64_t) * RI, "cudaMalloc record offsets");
     dmalloc((void**)&d_items, sizeof(uint32_t) * RI * kClasses, "cudaMalloc work items");
     dmalloc((void**)&d_counters, sizeof(uint32_t) * kClasses, "cudaMalloc work counters");
+    dmalloc((void**)&d_chunk_done, sizeof(uint32_t) * cfg.max_replica_ids, "cudaMalloc chunk counters");
     dmalloc((void**)&d_ladder, sizeof(double) * RI, "cudaMalloc ladders");
     dmalloc((void**)&d_out, sizeof(JobOut) * J, "cudaMalloc results");
     dmalloc((void**)&d_best_off, sizeof(uint64_t) * J, "cudaMalloc result offsets");
@@ -802,7 +820,7 @@ void Server::stop() {
         }
     }
     if (stream) cudaStreamSynchronize(stream);
-    for (void* p : {(void*)d_jobs, (void*)d_arena, (void*)d_rec_off, (void*)d_items, (void*)d_counters,
+    for (void* p : {(void*)d_jobs, (void*)d_arena, (void*)d_rec_off, (void*)d_items, (void*)d_counters, (void*)d_chunk_done,
                     (void*)d_ladder, (void*)d_out, (void*)d_best_off, (void*)d_best, (void*)d_stamp})
         if (p) cudaFree(p);
     if (h_out) cudaFreeHost(h_out);
