@@ -67,3 +67,12 @@ def test_chunked_launch_matches_oracle(monkeypatch):
         rep.run(iters, stop_on_solve=False)
         compare(b, 0, r, rep)
     b.close()
+
+
+def test_chunked_large_order_launches_leave_every_replica_unchanged(monkeypatch):
+    # the HBM-resident kernel (orders above 256): its Gram arena and lazy best
+    # copies carry over between a replica's chunks
+    jobs = [{"n": 260, "w": 259, "seed": 71, "replicas": 24}, {"n": 300, "w": 20, "seed": 72, "replicas": 16}]
+    p = X.Params(stop_on_solve=0, t_init=8.0, moves_per_launch=30)
+    base = run_states(monkeypatch, 1, jobs, p, 90)
+    assert run_states(monkeypatch, 3, jobs, p, 90) == base

@@ -854,31 +854,6 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
     __syncwarp();
 }
 
-// Chunked launches: chunk c of a replica starts once chunk c-1 has released
-// the replica's record.  Items are taken in chunk-major order by resident
-// warps, so the chunk waited for is running or done; the wait is bounded
-// all the same (about a second) and flags the replica when it gives up.
-constexpr uint32_t kChunkSpinLimit = 1u << 22;
-
-__device__ __noinline__ bool wait_chunk(const uint32_t* flag, uint32_t want) {
-    uint32_t v = 0;
-#pragma unroll 1
-    for (uint32_t spin = 0; spin < kChunkSpinLimit; ++spin) {
-        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
-        if (v >= want) return true;
-        __nanosleep(256);
-    }
-    return false;
-}
-
-// every lane's record writes are made visible device-wide before lane 0
-// publishes the chunk count
-__device__ __forceinline__ void release_chunk(uint32_t* flag, uint32_t value, int lane) {
-    __threadfence();
-    __syncwarp();
-    if (lane == 0) asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(flag), "r"(value) : "memory");
-}
-
 // Register budget per thread; it sets how many replica warps an SM holds.
 #ifndef XW_ANNEAL_MAXNREG
 #define XW_ANNEAL_MAXNREG 128

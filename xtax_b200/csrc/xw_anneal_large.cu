@@ -543,7 +543,7 @@ __device__ bool build_gram(const int8_t* W, int16_t* G, uint64_t* mask, uint64_t
 }
 
 template <bool GEN>
-__device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int lane) {
+__device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int lane, uint64_t chunk_iters) {
     uint8_t* rec = a.arena + a.rec_off[rid];
     RepHeader* H = reinterpret_cast<RepHeader*>(rec);
     const uint32_t jid = H->job;
@@ -568,7 +568,7 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
     uint64_t* sThr = reinterpret_cast<uint64_t*>(slot + L.off_thr);
 
     uint64_t it = H->it;
-    uint64_t iters = a.iters;
+    uint64_t iters = chunk_iters;
     if (J->budget_iters) {
         if (it >= J->budget_iters) return;
         if (iters > J->budget_iters - it) iters = J->budget_iters - it;
@@ -851,12 +851,31 @@ __global__ void __launch_bounds__(128, XW_LARGE_MIN_BLOCKS) anneal_large_kernel(
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     uint8_t* slot = smem + (size_t)warp * a.slot_bytes;
+    // work items as in anneal_kernel (xw_anneal.cu): whole replicas, or
+    // chunks of their iterations in chunk-major order
+    const uint64_t total = (uint64_t)a.n_items * a.chunks;
     for (;;) {
         uint32_t item = 0;
         if (lane == 0) item = atomicAdd(a.counter, 1u);
         item = __shfl_sync(FULL, item, 0);
-        if (item >= a.n_items) break;
-        run_large<GEN>(a, a.items[item], slot, lane);
+        if (item >= total) break;
+        if (a.chunks == 1) {
+            run_large<GEN>(a, a.items[item], slot, lane, a.iters);
+            continue;
+        }
+        const uint32_t c = item / a.n_items;
+        const uint32_t rid = a.items[item - c * a.n_items];
+        const uint64_t lo = a.iters * c / a.chunks, hi = a.iters * (c + 1) / a.chunks;
+        bool ok = true;
+        if (c > 0) ok = __all_sync(FULL, wait_chunk(a.chunk_done + rid, c));
+        __syncwarp();
+        if (ok) {
+            run_large<GEN>(a, rid, slot, lane, hi - lo);
+        } else if (lane == 0) {
+            RepHeader* H = reinterpret_cast<RepHeader*>(a.arena + a.rec_off[rid]);
+            atomicOr(&H->err, XW_ERR_CHUNK);
+        }
+        release_chunk(a.chunk_done + rid, c + 1, lane);
     }
 }
 

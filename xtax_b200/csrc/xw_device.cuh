@@ -113,6 +113,31 @@ __device__ __forceinline__ double acceptance_exp(double x) {
     return __dmul_rn(p, scale);
 }
 
+// Chunked launches: chunk c of a replica starts once chunk c-1 has released
+// the replica's record.  Items are taken in chunk-major order by resident
+// warps, so the chunk waited for is running or done; the wait is bounded
+// all the same (about a second) and flags the replica when it gives up.
+constexpr uint32_t kChunkSpinLimit = 1u << 22;
+
+static __device__ __noinline__ bool wait_chunk(const uint32_t* flag, uint32_t want) {
+    uint32_t v = 0;
+#pragma unroll 1
+    for (uint32_t spin = 0; spin < kChunkSpinLimit; ++spin) {
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
+        if (v >= want) return true;
+        __nanosleep(256);
+    }
+    return false;
+}
+
+// every lane's record writes are made visible device-wide before lane 0
+// publishes the chunk count
+__device__ __forceinline__ void release_chunk(uint32_t* flag, uint32_t value, int lane) {
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(flag), "r"(value) : "memory");
+}
+
 // Metropolis test u*2^-32 < exp(-delta/T), delta > 0.
 __device__ __forceinline__ bool metropolis_accept(int64_t delta, double temperature, uint32_t u) {
     const double t = temperature > 1.0e-12 ? temperature : 1.0e-12;

@@ -605,6 +605,10 @@ void Batch::configure_shape(int wpb) {
         if (per_sm < 1) throw std::length_error("CUDA large-order anneal kernel has zero occupancy");
         const int want = (int)((n_large + large_wpb - 1) / large_wpb);
         large_blocks = std::max(1, std::min(want, per_sm * props.multiProcessorCount));
+        large_chunks = choose_chunks(n_large, (uint32_t)(large_blocks * large_wpb));
+        if (large_chunks > 1 && !d_chunk_done)
+            check(cudaMalloc(&d_chunk_done, sizeof(uint32_t) * std::max<uint32_t>(total_replicas, 1)),
+                  "cudaMalloc chunk counters");
     }
     if (n_large == total_replicas) return;
     const void* fn = anneal_kernel_fn(opl, general);
@@ -634,7 +638,7 @@ void Batch::configure_shape(int wpb) {
     // waves of work).  Split each replica's iterations into k chunks, k in
     // [1, 8] with the fewest waves per unit of work, the least k on ties.
     chunks = choose_chunks(small, (uint32_t)(blocks * wpb));
-    if (chunks > 1 && !d_chunk_done)
+    if ((chunks > 1 || large_chunks > 1) && !d_chunk_done)
         check(cudaMalloc(&d_chunk_done, sizeof(uint32_t) * std::max<uint32_t>(total_replicas, 1)),
               "cudaMalloc chunk counters");
 }
@@ -694,6 +698,12 @@ void Batch::enqueue_rounds(uint64_t iters, bool timed) {
             l.counter = static_cast<uint32_t*>(d_counters) + 2 * k + 1;
             l.gram = static_cast<uint8_t*>(d_gram);
             l.gram_off = static_cast<const uint64_t*>(d_gram_off);
+            l.chunks = l.iters >= large_chunks ? large_chunks : 1;
+            if (l.chunks > 1) {
+                l.chunk_done = static_cast<uint32_t*>(d_chunk_done);
+                check(cudaMemsetAsync(d_chunk_done, 0, sizeof(uint32_t) * total_replicas, stream),
+                      "cudaMemsetAsync chunk counters");
+            }
             check(launch_anneal_large(l, general_large, large_wpb, large_blocks, stream),
                   "launch anneal_large_kernel");
         }

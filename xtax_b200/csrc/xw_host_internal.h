@@ -84,6 +84,7 @@ struct Batch {
     uint32_t large_slot_bytes = 0;
     int large_wpb = 4;
     int large_blocks = 1;
+    uint32_t large_chunks = 1;
     std::vector<uint64_t> gram_off;   // per replica, into d_gram
     size_t gram_bytes = 0;
 
