@@ -281,6 +281,11 @@ def ours(args):
     starts = None
     e2e_value = None
     h2d, d2h = batch.transfer_bytes()
+    launch_shape = list(batch.shape())
+    # the device-resident batch is done: its device memory returns to the
+    # library's pool, where the end-to-end call's batch finds it
+    torch.cuda.synchronize()
+    batch.close()
     if args.e2e_steps > 0:
         import numpy as np
         starts = np.concatenate([X.random_start(N_ORDER, W_WEIGHT, (j["seed"] + r * 0x9e3779b9) & 0xffffffff)
@@ -321,7 +326,7 @@ def ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "replicas_per_gpu": INSTANCES * RUNGS,
                    "iterations_per_replica": iters, "l2": "flushed between steps (256 MiB write)",
-                   "launch_shape": list(batch.shape()), "parallelism": f"instances x{world} GPUs"},
+                   "launch_shape": launch_shape, "parallelism": f"instances x{world} GPUs"},
         "gpu_launches": args.steps * (2 * (-(-iters // EXCHANGE)) + 1),
         "roofline": {"bound": "smem", "achieved": achieved, "peak": smem_peak, "unit": "GB/s",
                      "frac": achieved / smem_peak, "traffic": int(prof) if prof else None,

@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <random>
 #include <stdexcept>
 #include <string>
@@ -167,12 +168,42 @@ std::string validate(int n, int w, const xw_params& p) {
 // ------------------------------------------------------------------------
 // Batch: device arena of replica records for a set of jobs.
 
+// Device memory of batches comes from one pool per device, in stream order,
+// and goes back to that pool when a batch is destroyed: handing it back to
+// the driver (cudaFree) stalled the next call for up to 0.8 s on B200.  The
+// pool keeps what it has been given (release threshold: never), so memory a
+// batch frees is the next batch's without a driver call.
+cudaMemPool_t batch_pool(int device) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    if (device < 0 || device >= 64) throw std::invalid_argument("device ordinal out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!pools[device]) {
+        cudaMemPoolProps props;
+        std::memset(&props, 0, sizeof props);
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        check(cudaMemPoolCreate(&pools[device], &props), "cudaMemPoolCreate");
+        uint64_t keep = UINT64_MAX;
+        check(cudaMemPoolSetAttribute(pools[device], cudaMemPoolAttrReleaseThreshold, &keep),
+              "cudaMemPoolSetAttribute");
+    }
+    return pools[device];
+}
+
+void Batch::dalloc(void** ptr, size_t bytes, const char* what) {
+    check(cudaMallocFromPoolAsync(ptr, std::max<size_t>(bytes, 16), batch_pool(params.device), stream), what);
+}
+
 Batch::~Batch() {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     for (auto e : events) cudaEventDestroy(e);
+    if (stream) cudaStreamSynchronize(stream);
     for (void* ptr : {d_jobs, d_jobs0, d_arena, d_arena0, d_rec_off, d_items, d_counters, d_ladder,
                       d_out, d_best_off, d_best, d_t0, d_gram, d_gram_off, d_chunk_done})
-        if (ptr) cudaFree(ptr);
+        if (ptr) cudaFreeAsync(ptr, stream);
+    if (stream) cudaStreamSynchronize(stream);
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
@@ -404,11 +435,17 @@ void Batch::upload(const std::vector<uint8_t>& host) {
     const int njobs = (int)jobs.size();
     const size_t arena = host.size();
     arena_bytes = arena;
-    auto dmalloc = [&](void** ptr, size_t bytes, const char* what) {
-        check(cudaMalloc(ptr, std::max<size_t>(bytes, 16)), what);
-    };
+    auto dmalloc = [&](void** ptr, size_t bytes, const char* what) { dalloc(ptr, bytes, what); };
     size_t free_b = 0, total_b = 0;
     check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    {
+        // memory the batch pool holds but no batch uses is free to this batch
+        uint64_t reserved = 0, used = 0;
+        cudaMemPool_t pool = batch_pool(params.device);
+        check(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved), "cudaMemPoolGetAttribute");
+        check(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used), "cudaMemPoolGetAttribute");
+        if (reserved > used) free_b += (size_t)(reserved - used);
+    }
     const size_t need = 2 * arena + 2 * sizeof(XwJob) * njobs + 16 * total_replicas + best_bytes + gram_bytes;
     if (need > free_b)
         throw std::length_error(fmt("CUDA replica state requires %g MiB, but only %g MiB is free",
@@ -607,8 +644,7 @@ void Batch::configure_shape(int wpb) {
         large_blocks = std::max(1, std::min(want, per_sm * props.multiProcessorCount));
         large_chunks = choose_chunks(n_large, (uint32_t)(large_blocks * large_wpb));
         if (large_chunks > 1 && !d_chunk_done)
-            check(cudaMalloc(&d_chunk_done, sizeof(uint32_t) * std::max<uint32_t>(total_replicas, 1)),
-                  "cudaMalloc chunk counters");
+            dalloc(&d_chunk_done, sizeof(uint32_t) * std::max<uint32_t>(total_replicas, 1), "cudaMalloc chunk counters");
     }
     if (n_large == total_replicas) return;
     const void* fn = anneal_kernel_fn(opl, general);
@@ -639,8 +675,7 @@ void Batch::configure_shape(int wpb) {
     // [1, 8] with the fewest waves per unit of work, the least k on ties.
     chunks = choose_chunks(small, (uint32_t)(blocks * wpb));
     if ((chunks > 1 || large_chunks > 1) && !d_chunk_done)
-        check(cudaMalloc(&d_chunk_done, sizeof(uint32_t) * std::max<uint32_t>(total_replicas, 1)),
-              "cudaMalloc chunk counters");
+        dalloc(&d_chunk_done, sizeof(uint32_t) * std::max<uint32_t>(total_replicas, 1), "cudaMalloc chunk counters");
 }
 
 void Batch::reset() {
@@ -663,11 +698,11 @@ void Batch::reserve_rounds(int rounds) {
         events.push_back(e);
     }
     if (counters_cap < rounds) {
-        check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
-        if (d_counters) cudaFree(d_counters);
+        if (d_counters) check(cudaFreeAsync(d_counters, stream), "cudaFreeAsync counters");
         d_counters = nullptr;
         // one counter per round for each of the two kernels
-        check(cudaMalloc(&d_counters, sizeof(uint32_t) * 2 * rounds), "cudaMalloc counters");
+        dalloc(&d_counters, sizeof(uint32_t) * 2 * rounds, "cudaMalloc counters");
+        check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
         counters_cap = rounds;
     }
 }

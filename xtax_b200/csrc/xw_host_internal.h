@@ -115,6 +115,8 @@ struct Batch {
     Batch& operator=(const Batch&) = delete;
     ~Batch();
 
+    // device memory from the engine's per-device pool, in the batch's stream
+    void dalloc(void** ptr, size_t bytes, const char* what);
     void build(const xw_job_spec* specs, int njobs, const xw_params& p, const int8_t* starts);
     void derive_layout();
     void upload(const std::vector<uint8_t>& host);
