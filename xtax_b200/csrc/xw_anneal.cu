@@ -855,11 +855,23 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
 }
 
 // Register budget per thread; it sets how many replica warps an SM holds.
+// An SM's registers are split between its four schedulers (16384 each), so
+// 128 registers per thread give 4 warps per scheduler and 96 give 5.  The
+// lean one-row-per-lane kernel gains from the fifth warp (W(26,25) with
+// 4096 replicas: 0.82 -> 0.87 G moves/s); the general and the wider kernels
+// lose more to the spills of a 96-register budget than they gain (measured
+// 6-18% slower), and keep 128.
 #ifndef XW_ANNEAL_MAXNREG
 #define XW_ANNEAL_MAXNREG 128
 #endif
+#ifndef XW_ANNEAL_MAXNREG_LEAN1
+#define XW_ANNEAL_MAXNREG_LEAN1 96
+#endif
+constexpr int anneal_maxnreg(int opl, bool general) {
+    return opl == 1 && !general ? XW_ANNEAL_MAXNREG_LEAN1 : XW_ANNEAL_MAXNREG;
+}
 template <int OPL, bool GEN>
-__global__ void __maxnreg__(XW_ANNEAL_MAXNREG) anneal_kernel(AnnealArgs a) {
+__global__ void __maxnreg__(anneal_maxnreg(OPL, GEN)) anneal_kernel(AnnealArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
