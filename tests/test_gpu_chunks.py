@@ -76,3 +76,14 @@ def test_chunked_large_order_launches_leave_every_replica_unchanged(monkeypatch)
     p = X.Params(stop_on_solve=0, t_init=8.0, moves_per_launch=30)
     base = run_states(monkeypatch, 1, jobs, p, 90)
     assert run_states(monkeypatch, 3, jobs, p, 90) == base
+
+
+def test_a_chunk_waits_out_a_long_predecessor(monkeypatch):
+    """One replica in two chunks: a second warp takes the second chunk at
+    once and waits for the whole first chunk (over a second here, at the
+    largest order).  The wait is bounded by device time, not by a short spin
+    count, so the replica ends unflagged and as the unchunked run."""
+    jobs = [{"n": 1024, "w": 1023, "seed": 5, "replicas": 1}]
+    p = X.Params(stop_on_solve=0, t_init=8.0, moves_per_launch=60000)
+    base = run_states(monkeypatch, 1, jobs, p, 60000)
+    assert run_states(monkeypatch, 2, jobs, p, 60000) == base

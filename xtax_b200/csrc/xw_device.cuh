@@ -115,17 +115,26 @@ __device__ __forceinline__ double acceptance_exp(double x) {
 
 // Chunked launches: chunk c of a replica starts once chunk c-1 has released
 // the replica's record.  Items are taken in chunk-major order by resident
-// warps, so the chunk waited for is running or done; the wait is bounded
-// all the same (about a second) and flags the replica when it gives up.
-constexpr uint32_t kChunkSpinLimit = 1u << 22;
+// warps, so the chunk waited for is always running or done and the wait
+// ends; how long it lasts is at most that chunk's own run time, which can be
+// long when the queue runs ahead of a slow replica (a mixed batch, or
+// replicas that finished early).  So the wait is bounded by elapsed device
+// time, kChunkWaitNs (%globaltimer), with an iteration cap behind it, and the
+// replica is flagged (XW_ERR_CHUNK) if it gives up.
+constexpr uint64_t kChunkWaitNs = 30ull * 1000000000ull;
+constexpr uint32_t kChunkSpinLimit = 1u << 28;
 
 static __device__ __noinline__ bool wait_chunk(const uint32_t* flag, uint32_t want) {
     uint32_t v = 0;
+    uint64_t t0, t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
 #pragma unroll 1
     for (uint32_t spin = 0; spin < kChunkSpinLimit; ++spin) {
         asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
         if (v >= want) return true;
         __nanosleep(256);
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        if (t - t0 > kChunkWaitNs) return false;
     }
     return false;
 }
