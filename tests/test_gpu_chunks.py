@@ -87,3 +87,16 @@ def test_a_chunk_waits_out_a_long_predecessor(monkeypatch):
     p = X.Params(stop_on_solve=0, t_init=8.0, moves_per_launch=60000)
     base = run_states(monkeypatch, 1, jobs, p, 60000)
     assert run_states(monkeypatch, 2, jobs, p, 60000) == base
+
+
+def test_served_requests_end_the_same_in_chunked_rounds(monkeypatch):
+    """The serving loop's class launches run chunked when a class has more
+    replicas than resident warps; forcing chunks on small requests shows that
+    a served request's outcome does not depend on them."""
+    from test_gpu_server import outcome, req, serve
+    reqs = [req(12, 11, 4242, 8, 200000), req(16, 4, 77, 16, 5000), req(26, 25, 9, 32, 4000)]
+    monkeypatch.setenv("XW_CHUNKS", "1")
+    base, _ = serve(reqs)
+    monkeypatch.setenv("XW_CHUNKS", "3")
+    chunked, _ = serve(reqs)
+    assert [outcome(r, W) for r, W in chunked] == [outcome(r, W) for r, W in base]
