@@ -197,3 +197,20 @@ def test_cli_runs_a_large_order(tmp_path):
     W = np.array(rows, dtype=np.int8).T.reshape(-1)
     st = X.score(300, 299, W)
     assert final == f"Final best score: {st[0]} conflicts={st[1]}"
+
+
+def test_restarts_at_a_large_order_with_weight_near_half_stay_quick():
+    """The escape scan of W(512,256) would take about 4e12 operations, many
+    seconds per restart: past the scan budget a restart kicks without an
+    escape move, so a short run still restarts several times."""
+    p = X.Params(seed=4, replicas=32, moves_per_launch=100, max_seconds=6.0, restart_interval=0.05,
+                 restart_fraction=0.5, t_init=1000.0, t_min=1000.0)
+    r = X.run_annealer(512, 256, p)
+    restarts = [line for line in r.log if line.startswith("[restart] seconds=")]
+    assert len(restarts) >= 2
+    assert all("min_escape_delta=0" in line for line in restarts)
+    # once the search stagnates, restarts follow one another within the
+    # interval plus a launch, not seconds of scanning apart
+    t = [float(line.split("seconds=")[1].split()[0]) for line in restarts]
+    assert max(b - a for a, b in zip(t, t[1:])) < 2.0
+    assert X.score(512, 256, r.best.entries)[0] == r.best.score

@@ -848,6 +848,29 @@ void Batch::fill_results(const std::vector<JobOut>& out, const int8_t* best_host
 // better of it and the global best as its best, and the reheat temperature.
 // The job's records make one round trip through host memory.  Returns the
 // number of replicas restarted; `line` receives the reference's log line.
+// Operations of the escape scan of W: about 4 n per candidate switch, and a
+// row pair (r1, r2) has k1 * k2 of them, k1 (k2) the columns that are
+// nonzero in r1 (r2) and zero in the other row.
+double escape_scan_work(int n, const std::vector<int8_t>& W) {
+    const int nw = (n + 63) / 64;
+    std::vector<uint64_t> S((size_t)n * nw, 0);
+    for (int c = 0; c < n; ++c)
+        for (int r = 0; r < n; ++r)
+            if (W[(size_t)c * n + r]) S[(size_t)r * nw + c / 64] |= 1ull << (c % 64);
+    double pairs = 0.0;
+    for (int a = 0; a < n; ++a)
+        for (int b2 = a + 1; b2 < n; ++b2) {
+            int k1 = 0, k2 = 0;
+            for (int q = 0; q < nw; ++q) {
+                const uint64_t x = S[(size_t)a * nw + q], y = S[(size_t)b2 * nw + q];
+                k1 += __builtin_popcountll(x & ~y);
+                k2 += __builtin_popcountll(y & ~x);
+            }
+            pairs += (double)k1 * k2;
+        }
+    return pairs * 4.0 * n;
+}
+
 int restart_population(Batch& b, int j, const std::vector<int8_t>& elite_best, int64_t gbest, int64_t gconf,
                        RestartState& rs, double elapsed, std::string& line) {
     const xw_params& p = b.params;
@@ -861,7 +884,13 @@ int restart_population(Batch& b, int j, const std::vector<int8_t>& elite_best, i
     std::vector<int32_t> eg((size_t)n * n);
     for (int a = 0; a < n; ++a)
         for (int c = 0; c < n; ++c) eg[(size_t)a * n + c] = elite.gram_at(a, c);
-    const std::vector<EscapeMove> escapes = escape_moves_from(elite, escape_scan(n, elite_best.data(), eg.data(), limit));
+    // Within the reference's orders the scan is at most ~1.4e11 operations
+    // (W(256,128), 0.3 s); above them, with weights near n/2, it grows as
+    // n^5 (W(300,150) ~3e11, W(1024,512) ~5e14).  Past kEscapeScanBudget
+    // the restart kicks without an escape move rather than stall the run.
+    std::vector<EscapeMove> escapes;
+    if (escape_scan_work(n, elite_best) <= kEscapeScanBudget)
+        escapes = escape_moves_from(elite, escape_scan(n, elite_best.data(), eg.data(), limit));
     std::vector<int> selected;
     size_t scanned = 0;
     while ((int)selected.size() < count && scanned < (size_t)R * 2) {

@@ -169,6 +169,11 @@ struct RestartState {
     int elite = 0;
 };
 
+// Escape-scan cost (operations) for an elite W, and the most a restart
+// spends on it: above, restarts kick without an escape move.
+double escape_scan_work(int n, const std::vector<int8_t>& W);
+constexpr double kEscapeScanBudget = 1.0e12;
+
 // Elite restart of job j's replicas (xweigh_cuda.cu:1817-2289); returns how
 // many replicas were restarted and the reference's log line.
 int restart_population(Batch& b, int j, const std::vector<int8_t>& elite_best, int64_t gbest, int64_t gconf,
