@@ -18,6 +18,7 @@ tempering setup.  N > 1: one process per GPU, each running its own 128
 instances (weak scaling, no collective on the data path).
 """
 import argparse
+import dataclasses
 import json
 import os
 import re
@@ -107,8 +108,12 @@ def reference_arm(args):
         "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
         "impl": "reference",
-        "config": {"workload": WORKLOAD, "engine": "reference xweigh CPU, parallel tempering over threads",
-                   "threads": threads, "sample_seconds_per_step": sample},
+        "config": {"workload": f"W({N_ORDER},{W_WEIGHT}): one reference xweigh search, parallel tempering "
+                               f"with one rung per host thread ({threads} rungs, T {T_MIN}..{T_MAX}, exchange "
+                               f"every {EXCHANGE} moves per thread), {sample:g} s of search per step",
+                   "engine": "reference xweigh CPU, parallel tempering over threads",
+                   "threads": threads, "sample_seconds_per_step": sample,
+                   "compared_with": WORKLOAD},
         "cpu_baseline": {"value": value, "unit": "moves/s", "cores": threads, "kind": "reference",
                          "sample": f"xweigh {N_ORDER} {W_WEIGHT} -t {threads} --max-seconds {sample} per step"},
         "e2e": {"value": value, "unit": "moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -282,6 +287,7 @@ def ours(args):
     e2e_value = None
     h2d, d2h = batch.transfer_bytes()
     launch_shape = list(batch.shape())
+    launch_classes = batch.classes()
     # the device-resident batch is done: its device memory returns to the
     # library's pool, where the end-to-end call's batch finds it
     torch.cuda.synchronize()
@@ -326,7 +332,8 @@ def ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "replicas_per_gpu": INSTANCES * RUNGS,
                    "iterations_per_replica": iters, "l2": "flushed between steps (256 MiB write)",
-                   "launch_shape": launch_shape, "parallelism": f"instances x{world} GPUs"},
+                   "launch_shape": launch_shape, "launch_classes": launch_classes,
+                   "parallelism": f"instances x{world} GPUs"},
         "gpu_launches": args.steps * (2 * (-(-iters // EXCHANGE)) + 1),
         "roofline": {"bound": "smem", "achieved": achieved, "peak": smem_peak, "unit": "GB/s",
                      "frac": achieved / smem_peak, "traffic": int(prof) if prof else None,
@@ -337,7 +344,7 @@ def ours(args):
     }
     if e2e_value is not None:
         line["e2e"] = {"value": e2e_value, "unit": "moves/s", "h2d_bytes_per_step": h2d,
-                       "d2h_bytes_per_step": d2h}
+                       "d2h_bytes_per_step": d2h, "steps": args.e2e_steps}
     if args.cpu_seconds > 0 and os.path.exists(REF_XWEIGH):
         threads = os.cpu_count() or 1
         mv, s = run_reference_cpu(args.cpu_seconds, threads)
@@ -362,7 +369,8 @@ def ours(args):
         line["large_order"] = large_bench(X, args.large_iters, args.large_ref_seconds)
     if args.serve_requests > 0:
         line["serving"] = serving_bench(X, args.serve_requests, args.serve_plain, args.serve_quantum,
-                                        args.serve_reference, args.serve_reference_cap)
+                                        args.serve_reference, args.serve_reference_cap, args.serve_light,
+                                        args.serve_light_rate)
     print(json.dumps(line), flush=True)
 
 
@@ -461,20 +469,31 @@ def c1_bench(X, ref_seconds):
                  objective=1, move_set=1, start_kind=1, stop_on_solve=2, moves_per_launch=100_000,
                  max_moves=C1_MOVES)
     jobs = [{"n": 12, "w": 11, "seed": k, "replicas": 1} for k in range(1, C1_SEEDS + 1)]
-    b = X.Batch(jobs, p)
-    b.run_timed(C1_MOVES)
-    b.synchronize()
-    ms = sum(b.launch_times())
-    res = b.results()
-    b.close()
-    moves = sum(r.moves for r, _ in res)
-    solved = [r for r, _ in res if r.solved]
+
+    def searches(params):
+        b = X.Batch(jobs, params)
+        classes = b.classes()
+        b.run_timed(C1_MOVES)
+        b.synchronize()
+        ms = sum(b.launch_times())
+        res = b.results()
+        b.close()
+        moves = sum(r.moves for r, _ in res)
+        solved = [r for r, _ in res if r.solved]
+        return {"moves": moves, "ms": ms, "moves_per_sec": moves / (ms / 1e3),
+                "moves_per_sec_per_search": moves / (ms / 1e3) / C1_SEEDS,
+                "solved": len(solved), "searches": C1_SEEDS,
+                "median_solve_iteration": float(np.median([r.solved_iteration for r in solved])) if solved else None,
+                "launch_classes": classes}
+
     out = {"workload": f"W(12,11) x {C1_SEEDS} seeds, 1 replica each, squared objective, flips + within-row "
                        f"swaps, cooling 4 -> 0.05 over {C1_MOVES:.0e} moves",
-           "device": {"moves": moves, "ms": ms, "moves_per_sec": moves / (ms / 1e3),
-                      "solved": len(solved), "searches": C1_SEEDS,
-                      "median_solve_iteration": float(np.median([r.solved_iteration for r in solved]))
-                      if solved else None}}
+           "device": searches(p)}
+    # the same searches one warp per replica (no latency mode)
+    out["device_one_warp"] = searches(dataclasses.replace(p, warps_per_replica=1))
+    # the same schedule with the reference's moves, L1 objective and regular
+    # starts: the solve rate of the move set, on the device
+    out["device_reference_moves"] = searches(dataclasses.replace(p, objective=0, move_set=0, start_kind=0))
     if ref_seconds > 0 and os.path.exists(REF_XWEIGH):
         mv = secs = 0.0
         ok = runs = 0
@@ -554,6 +573,7 @@ def uneven_bench(X, iters):
 
     def timed(js, steps=3):
         b = X.Batch(js, p)
+        timed.classes = b.classes()
         b.reset()
         b.run(iters)           # warm-up (builds the CUDA graph)
         b.synchronize()
@@ -572,6 +592,7 @@ def uneven_bench(X, iters):
     out = {"workload": f"{len(UNEVEN)} orders x {UNEVEN_INSTANCES} instances x {UNEVEN_RUNGS}-rung ladder "
                        f"T {T_MIN}..{T_MAX}, exchange every {EXCHANGE}, {iters} iterations per replica",
            "autotuned_warps_per_block": wpb, "autotune_trial_ms": tune_ms, "launch_shape": list(shape),
+           "launch_classes": timed.classes,
            "batched": {"moves": moves, "ms": ms, "moves_per_sec": moves / (ms / 1e3)}}
     pm = pms = 0.0
     for (n, w) in UNEVEN:
@@ -589,15 +610,16 @@ SERVE_REPLICAS = 256
 SERVE_BUDGET = 10 ** 8
 
 
-def serving_stream(count, seed=5):
-    """The mixed request stream: Poisson arrivals at 200 requests/s (seeded
-    exponential gaps); 70% W(n, n-1) with n uniform in SERVE_ORDERS, 30%
-    W(n, 4) with n uniform in 16..64; request k has seed 1000 + k."""
+def serving_stream(count, seed=5, rate=SERVE_RATE):
+    """The mixed request stream: Poisson arrivals at `rate` requests/s
+    (seeded exponential gaps; 200/s is the workload's); 70% W(n, n-1) with
+    n uniform in SERVE_ORDERS, 30% W(n, 4) with n uniform in 16..64; request
+    k has seed 1000 + k."""
     import numpy as np
     rng = np.random.default_rng(seed)
     out, t = [], 0.0
     for k in range(count):
-        t += rng.exponential(1.0 / SERVE_RATE)
+        t += rng.exponential(1.0 / rate)
         if rng.random() < 0.7:
             n = int(rng.choice(SERVE_ORDERS))
             w = n - 1
@@ -647,37 +669,45 @@ def serve_stream(X, reqs, **cfg):
 def serve_reference_plain(reqs, cap_seconds):
     """The reference's plain kernel on the stream's first requests, one
     xweigh_cuda process per request (its one-instance-per-launch mode), 256
-    replicas, at most `cap_seconds` of search each (it has no move budget).
-    Queueing is the single-server FIFO of the measured service times:
-    start_k = max(arrival_k, finish_{k-1}); time-to-exact = wait + process
-    start-up + the solve time of its `new best score=0` line.  Requests the
-    reference answers with Sylvester blocks are counted apart."""
+    replicas, at most `cap_seconds` of search each (it has no move budget),
+    replayed live: each request arrives at its own time, waits while the
+    process of an earlier one holds the GPU, and its time-to-exact runs from
+    its arrival to the moment the process prints its `new best score=0`
+    line (read as it is printed).  Requests the reference answers with
+    Sylvester blocks are counted apart."""
     import numpy as np
-    finish, tte, moves, busy, solved, syl = 0.0, [], 0, 0.0, 0, 0
+    tte, moves, busy, solved, syl = [], 0, 0.0, 0, 0
+    t0 = time.perf_counter()
     for (ta, n, w, seed) in reqs:
+        wait = ta - (time.perf_counter() - t0)
+        if wait > 0:
+            time.sleep(wait)
         with tempfile.TemporaryDirectory() as td:
-            t0 = time.perf_counter()
-            out = subprocess.run(
+            ts = time.perf_counter()
+            proc = subprocess.Popen(
                 [REF_XWEIGH_CUDA, str(n), str(w), "--replicas", str(SERVE_REPLICAS), "--seed", str(seed),
                  "--max-seconds", str(cap_seconds), "--restart-interval", "0", "-o", os.path.join(td, "w.csv")],
-                capture_output=True, text=True, timeout=cap_seconds * 4 + 120)
-            wall = time.perf_counter() - t0
-        start = max(ta, finish)
-        finish = start + wall
-        busy += wall
-        m = re.search(r"done moves=(\d+) .*?seconds=([0-9.e+-]+)", out.stdout)
-        search_s = float(m.group(2)) if m else 0.0
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True, bufsize=1)
+            t_solve, lines = None, []
+            for line in proc.stdout:
+                lines.append(line)
+                if t_solve is None and " new best score=0 " in line:
+                    t_solve = time.perf_counter()
+            proc.wait(timeout=cap_seconds * 4 + 120)
+            busy += time.perf_counter() - ts
+        out_text = "".join(lines)
+        m = re.search(r"done moves=(\d+) ", out_text)
         moves += int(m.group(1)) if m else 0
-        sol = re.search(r"\[t=([0-9.e+-]+)s\] new best score=0 ", out.stdout)
-        if sol:
+        if t_solve is not None:
             solved += 1
-            tte.append(start - ta + (wall - search_s) + float(sol.group(1)))
-        elif "[construct] using direct sum of Sylvester blocks" in out.stdout:
+            tte.append(t_solve - t0 - ta)
+        elif "[construct] using direct sum of Sylvester blocks" in out_text:
             syl += 1
     t = np.array(tte) if tte else np.array([-1.0])
     return {"requests": len(reqs), "sylvester": syl, "solved": solved, "cap_seconds_per_request": cap_seconds,
             "time_to_exact_s": {"p50": float(np.percentile(t, 50)), "p99": float(np.percentile(t, 99))},
             "moves": moves, "busy_s": busy, "moves_per_sec": moves / busy if busy > 0 else 0.0,
+            "arrivals": "live (real-time arrivals, one process at a time)",
             "impl": "reference xweigh_cuda (sm_100a build), one process per request"}
 
 
@@ -690,7 +720,7 @@ def tte_summary(per_request):
             "searched": int(sum(1 for syl, _, _ in per_request if not syl))}
 
 
-def serving_bench(X, count, plain_count, quantum, ref_count=0, ref_cap=3.0):
+def serving_bench(X, count, plain_count, quantum, ref_count=0, ref_cap=3.0, light_count=0, light_rate=10.0):
     """The serving workload: the request stream through the continuous-
     batching server, and its first `plain_count` requests both served and
     one request at a time (resident cap of one request: the plain
@@ -707,6 +737,11 @@ def serving_bench(X, count, plain_count, quantum, ref_count=0, ref_cap=3.0):
         per_pre, out["served_prefix"] = serve_stream(X, pre, quantum_iters=quantum)
         out["plain_prefix"] = serve_stream(X, pre, quantum_iters=quantum, schedule=X.SCHED_ALL,
                                            max_resident_replicas=SERVE_REPLICAS)[1]
+    if light_count > 0:
+        # the same mix at a rate the device keeps up with: time-to-exact is
+        # then the engine's, not the queue's
+        light = serving_stream(light_count, seed=9, rate=light_rate)
+        out["unsaturated"] = dict(serve_stream(X, light, quantum_iters=quantum)[1], rate_per_s=light_rate)
     if ref_count > 0 and os.path.exists(REF_XWEIGH_CUDA):
         try:
             out["plain_reference"] = serve_reference_plain(reqs[:ref_count], ref_cap)
@@ -731,15 +766,32 @@ def load_profile_figure(name):
         return None
 
 
+def free_port():
+    import socket
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
+def spawn_ranks(gpus):
+    """`--gpus N` without a launcher: start N ranks of this script under
+    torch.distributed.run on this node (one process per GPU) and return its
+    exit status.  Under torchrun (WORLD_SIZE set) nothing is spawned."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(free_port()), os.path.abspath(__file__)] + sys.argv[1:]
+    log(f"[bench] starting {gpus} ranks: {' '.join(cmd)}")
+    return subprocess.call(cmd)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--e2e-steps", type=int, default=1)
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--plain-seconds", type=float, default=10.0)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--plain-seconds", type=float, default=8.0)
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--iters", type=int, default=ITERS, help="iterations per replica per step (profiling cases)")
     ap.add_argument("--rescore", type=int, default=1, help="also time the batched tensor-core rescoring")
@@ -750,17 +802,23 @@ def main():
                     help="iterations per replica of the uneven-orders batch (0: none)")
     ap.add_argument("--large-iters", type=int, default=4000,
                     help="iterations per replica of the W(276,275) large-order section (0: none)")
-    ap.add_argument("--large-ref-seconds", type=float, default=10.0,
+    ap.add_argument("--large-ref-seconds", type=float, default=6.0,
                     help="seconds of the reference's xweigh_cuda on that order")
     ap.add_argument("--serve-requests", type=int, default=400, help="requests of the serving stream (0: none)")
     ap.add_argument("--serve-plain", type=int, default=60,
                     help="prefix of the stream also run one request at a time")
     ap.add_argument("--serve-quantum", type=int, default=1000, help="iterations per replica per server round")
-    ap.add_argument("--serve-reference", type=int, default=10,
-                    help="requests of the stream also run by the reference's xweigh_cuda, one process each")
-    ap.add_argument("--serve-reference-cap", type=float, default=3.0,
+    ap.add_argument("--serve-reference", type=int, default=60,
+                    help="requests of the stream also run by the reference's xweigh_cuda, one process each, "
+                         "arriving live")
+    ap.add_argument("--serve-reference-cap", type=float, default=2.0,
                     help="search seconds per request for the reference's xweigh_cuda")
+    ap.add_argument("--serve-light", type=int, default=100,
+                    help="requests of the same mix at an unsaturating rate (0: none)")
+    ap.add_argument("--serve-light-rate", type=float, default=10.0, help="arrivals per second of that stream")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_ranks(args.gpus))
     if args.warmup < 3:
         log("[bench] warmup raised to 3")
         args.warmup = 3

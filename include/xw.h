@@ -32,6 +32,14 @@ extern "C" {
 #define XW_ERR_TIMEOUT 6   /* a wait ended before the request finished */
 #define XW_ERR_IO 7        /* file read or write failed */
 
+/* Device error bits of a replica (xw_replica_state.error, OR-ed over a
+ * job's replicas in xw_job_result.error). */
+#define XW_DEVERR_SCORE 1u     /* the Gram rebuilt from W disagrees with the tracked score */
+#define XW_DEVERR_MINORITY 2u  /* a row's weight is not w, or disagrees with its minority list */
+#define XW_DEVERR_KERNEL 4u    /* a lean launch met a replica that needs the general kernel */
+#define XW_DEVERR_CHUNK 8u     /* a chunk's wait for the replica's previous chunk ran out;
+                                  the replica's later chunks of that launch did not run */
+
 #define XW_MAX_ORDER_CUDA 1024      /* largest n the device path anneals */
 #define XW_MAX_ORDER_SHARED 256     /* largest n whose replica state sits in shared memory; larger
                                        orders keep it in HBM (no counterpart in the reference,
@@ -80,7 +88,18 @@ typedef struct xw_params {
                                      its own solve and the others finish the launch, so that
                                      results do not depend on launch timing */
     int32_t warps_per_block;      /* 0 = autotuned */
-    int32_t reserved;
+    int32_t replicas_per_warp;    /* 0 = autotuned; 2: orders up to 16 run two replicas per warp,
+                                     one per half-warp (needs candidate_samples <= 16) */
+    int32_t warps_per_replica;    /* orders up to 32: 0 = autotuned (the latency mode when a
+                                     launch class has at most one replica per SM), 1 = one warp
+                                     per replica, 2..16 = that many warps per replica, which
+                                     speculate as many iterations at once and keep the first
+                                     accepted one (same trajectory, lower latency per move) */
+    int32_t restart_kicks;        /* elite restarts: 0 = kicks on the host with the reference's
+                                     mt19937 streams (xweigh_cuda.cu:2089-2193), after reading
+                                     the job's records back; 1 = kicks on the device with a
+                                     Philox stream per (job, restart round, replica), records
+                                     rewritten in place (no record crosses to the host) */
 } xw_params;
 
 /* xweigh_cuda::DeviceInfo (xweigh_cuda.hpp:46-54) */
@@ -186,6 +205,9 @@ typedef struct xw_job_result {
     uint64_t iterations;          /* max over replicas */
     uint64_t solved_iteration;    /* iteration of the first solve */
     double time_to_solution_seconds; /* device clock, from the first launch */
+    uint64_t accepted_moves;      /* Metropolis acceptances (sum of 32-bit per-replica counters) */
+    uint64_t accepted_rows;       /* rows of W those accepted moves changed (1 or 2 each) */
+    uint64_t two_row_evaluations; /* candidate evaluations of moves that change two rows */
 } xw_job_result;
 
 typedef struct xw_batch xw_batch;
@@ -224,6 +246,8 @@ typedef struct xw_replica_state {
     double temperature, reheat_temperature;
     int32_t moves_since_improvement, cooling_counter, rung, objective_kind;
     uint32_t status, error;
+    uint32_t accepted_moves, accepted_rows, two_row_evaluations;   /* 32-bit, wrapping */
+    uint32_t reserved;
 } xw_replica_state;
 
 /* Read replica `replica` of job `job`: state, current W, best W (n*n each,
@@ -249,8 +273,38 @@ int32_t xw_batch_load(const char* path, const xw_params* over, xw_batch** out);
  * records, job table, offsets, ladder), d2h per xw_batch_results call. */
 int32_t xw_batch_bytes(xw_batch* b, uint64_t* h2d, uint64_t* d2h);
 
-/* Launch shape of the batch: warps per block, blocks, shared bytes per warp. */
+/* One elite restart of job `job` now, as xw_run makes one after
+ * restart_interval seconds without improvement (xweigh_cuda.cu:1817-2289):
+ * the job's best replica is the elite; restart_fraction of the others,
+ * from a cursor that persists between calls, get kicked copies of its best
+ * W (on the host or the device per params.restart_kicks).  *restarted
+ * receives how many.  Cooling jobs only (a tempering job restarts none). */
+int32_t xw_batch_restart(xw_batch* b, int32_t job, int32_t* restarted);
+
+/* Launch shape of the batch's class with the most replicas: warps per
+ * block, blocks, shared bytes per replica slot. */
 int32_t xw_batch_shape(xw_batch* b, int32_t* warps_per_block, int32_t* blocks, int32_t* slot_bytes);
+
+/* One launch of a batch's round.  Replicas of one rows-per-lane class (or
+ * of the orders up to 16, which may share a warp two by two) run in one
+ * launch with one shape; the launches of a round run side by side.  No
+ * counterpart in the reference, which launches one search at a time. */
+typedef struct xw_launch_class {
+    int32_t min_order, max_order;
+    int32_t large;                 /* 1: the HBM-resident kernel (orders above 256) */
+    int32_t rows_per_lane;         /* 1, 2, 4 or 8 (shared-memory kernel) */
+    int32_t replicas_per_warp;     /* 1, or 2 (half-warp replicas, orders up to 16) */
+    int32_t warps_per_block;
+    int32_t blocks;
+    int32_t slot_bytes;            /* shared memory per replica */
+    int32_t chunks;                /* work items per replica and launch */
+    int32_t replicas;
+    int32_t general;               /* the general kernel (squared/parity objectives, row swaps) */
+    int32_t warps_per_replica;     /* 1, or 2..16 in the latency mode (one replica per CTA) */
+} xw_launch_class;
+/* Up to `cap` launch classes of the batch into out; *count receives how
+ * many there are. */
+int32_t xw_batch_classes(xw_batch* b, xw_launch_class* out, int32_t cap, int32_t* count);
 void xw_batch_destroy(xw_batch* b);
 
 /* Launch-shape autotuner (the tunable is warps per CTA; each replica is one
@@ -351,7 +405,8 @@ typedef struct xw_server_config {
                                       up to max_active_replicas */
     int32_t max_active_replicas;   /* replicas advanced per round under XW_SCHED_LEAST_ATTAINED
                                       (0 = four waves of the device's resident warps) */
-    int32_t reserved[6];
+    int32_t replicas_per_warp;     /* orders up to 16: 1 or 2 replicas per warp, 0 = tuned */
+    int32_t reserved[5];
 } xw_server_config;
 
 #define XW_SCHED_ALL 0
@@ -472,7 +527,10 @@ void xw_server_destroy(xw_server* s);
  * Inputs and outputs are the caller's device buffers:
  *   starts  replicas*n*n int8, column-major start states
  *   best    replicas*n*n int8, each replica's best state
- *   stats   replicas*4 int64: best score, best conflicts, score, moves
+ *   stats   replicas*4 int64: best score, best conflicts, score, moves;
+ *           a replica the kernel refused (a start row whose weight is not
+ *           w, a failed device self-check) reports best score -1, best
+ *           conflicts -(its XW_ERR_* device error bits) and score -1
  * p->t_init must be positive (no host calibration).  Work is enqueued on
  * `stream` (cudaStream_t, NULL = legacy default) and the call returns
  * without waiting.  The first call on a device looks up the array's device

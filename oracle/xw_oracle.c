@@ -1175,3 +1175,112 @@ int xwo_move_eval(int n, int w, int8_t* W, int kind, int r1, int r2, int c1, int
     free(r);
     return bad;
 }
+
+/* ======================================================================= */
+/* Device elite-restart kicks (the batch engine's restart mode 1, which
+ * replaces the reference's host kicks, cu:2089-2193, by a kernel with its
+ * own Philox stream).  Draw k of the kick of replica `replica` in restart
+ * round `round`: word k%4 of Philox({k/4, round_lo, round_hi,
+ * 0x20000000 | replica}, key).  Indices in [0,count) by Lemire's
+ * multiply-shift, a word in the rejection zone replaced by the next word
+ * (at most 64 tries). */
+typedef struct {
+    uint32_t key[2], ctr[4];
+    uint32_t k;
+} kick_rng;
+
+static uint32_t kick_word(kick_rng* g) {
+    uint32_t ctr[4] = {g->k >> 2, g->ctr[1], g->ctr[2], g->ctr[3]}, out[4];
+    xwo_philox4x32_10(ctr, g->key, out);
+    return out[(g->k++) & 3];
+}
+
+static uint32_t kick_index(kick_rng* g, uint32_t count) {
+    uint64_t prod = 0;
+    for (int t = 0; t < 64; ++t) {
+        prod = (uint64_t)kick_word(g) * count;
+        const uint32_t low = (uint32_t)prod;
+        if (low >= count || low >= (0u - count) % count) break;
+    }
+    return (uint32_t)(prod >> 32);
+}
+
+/* the k-th nonzero column of `row`, in column order */
+static int kick_nonzero(const int8_t* K, int n, int row, int k) {
+    for (int c = 0; c < n; ++c)
+        if (K[(size_t)c * n + row] != 0 && k-- == 0) return c;
+    return -1;
+}
+
+void xwo_kick(int n, int w, const int8_t* E, const int32_t* esc, uint32_t key0, uint32_t key1, uint64_t round,
+              uint32_t replica, uint32_t index, int kick, uint64_t thr_sign, int8_t* K) {
+    memcpy(K, E, (size_t)n * n);
+#define KAT(r, c) K[(size_t)(c) * n + (r)]
+    if (esc) {
+        /* the escape switch: the nonzero at (r1,c1) moves to (r1,c2) with
+         * sign new1, the one at (r2,c2) to (r2,c1) with sign new2 */
+        KAT(esc[0], esc[2]) = 0;
+        KAT(esc[1], esc[3]) = 0;
+        KAT(esc[0], esc[3]) = (int8_t)esc[4];
+        KAT(esc[1], esc[2]) = (int8_t)esc[5];
+    }
+    kick_rng g;
+    g.key[0] = key0; g.key[1] = key1;
+    g.ctr[0] = 0; g.ctr[1] = (uint32_t)round; g.ctr[2] = (uint32_t)(round >> 32); g.ctr[3] = 0x20000000u | replica;
+    g.k = 0;
+    const int mode = (int)((index + round) % 3);
+    int steps = kick;
+    uint64_t thr = thr_sign;
+    if (mode == 0) {
+        steps = 0;
+    } else if (mode == 1 && kick > 0 && w >= 3) {
+        /* row kicks: 2..max(2, w/2) distinct nonzeros of 1..4 random rows flip */
+        int rows = 1 + kick / (w > 1 ? w : 1);
+        if (rows > 4) rows = 4;
+        const int maxf = w / 2 > 2 ? w / 2 : 2;
+        int cols[MAXN];
+        for (int rk = 0; rk < rows; ++rk) {
+            const int row = (int)kick_index(&g, (uint32_t)n);
+            int cnt = 0;
+            for (int c = 0; c < n; ++c)
+                if (KAT(row, c) != 0) cols[cnt++] = c;
+            const int flips = 2 + (int)kick_index(&g, (uint32_t)(maxf - 1));
+            for (int f = 0; f < flips && f < cnt; ++f) {
+                const int j = f + (int)kick_index(&g, (uint32_t)(cnt - f));
+                const int t = cols[f]; cols[f] = cols[j]; cols[j] = t;
+                KAT(row, cols[f]) = (int8_t)-KAT(row, cols[f]);
+            }
+        }
+        steps = kick / 4;
+    } else if (mode == 2) {
+        thr = 0;   /* support switches only */
+    }
+    /* random moves: a sign flip (u < thr, or no zeros at all) or a
+     * value-preserving 2x2 support switch; `steps` moves within 8*steps
+     * attempts */
+    int applied = 0;
+    for (int a = 0; a < 8 * steps && applied < steps; ++a) {
+        const uint32_t u = kick_word(&g);
+        if (w == n || (uint64_t)u < thr) {
+            const int row = (int)kick_index(&g, (uint32_t)n);
+            const int col = kick_nonzero(K, n, row, (int)kick_index(&g, (uint32_t)w));
+            KAT(row, col) = (int8_t)-KAT(row, col);
+            ++applied;
+            continue;
+        }
+        if (n < 2) continue;
+        const int r1 = (int)kick_index(&g, (uint32_t)n);
+        int r2 = (int)kick_index(&g, (uint32_t)(n - 1));
+        if (r2 >= r1) ++r2;
+        const int c1 = kick_nonzero(K, n, r1, (int)kick_index(&g, (uint32_t)w));
+        const int c2 = kick_nonzero(K, n, r2, (int)kick_index(&g, (uint32_t)w));
+        if (c1 == c2 || KAT(r1, c2) != 0 || KAT(r2, c1) != 0) continue;
+        const int8_t v1 = KAT(r1, c1), v2 = KAT(r2, c2);
+        KAT(r1, c1) = 0;
+        KAT(r2, c2) = 0;
+        KAT(r1, c2) = v1;
+        KAT(r2, c1) = v2;
+        ++applied;
+    }
+#undef KAT
+}

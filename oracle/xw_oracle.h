@@ -125,6 +125,14 @@ int xwo_exchange(const xwo_job* job, xwo_replica** reps, int R,
 int xwo_move_eval(int n, int w, int8_t* W, int kind, int r1, int r2, int c1, int c2,
                   int v1, int v2, int commit, int64_t out[4]);
 
+/* The device kick of an elite restart (restart mode 1): replica `replica`,
+ * the index-th restarted in restart round `round`, from the elite E
+ * (column-major), with the escape move esc = {row1, row2, col1, col2,
+ * new1, new2} (NULL: none), `kick` steps and the sign-flip threshold
+ * thr_sign on a 32-bit draw.  Writes the kicked W to K. */
+void xwo_kick(int n, int w, const int8_t* E, const int32_t* esc, uint32_t key0, uint32_t key1, uint64_t round,
+              uint32_t replica, uint32_t index, int kick, uint64_t thr_sign, int8_t* K);
+
 #ifdef __cplusplus
 }
 #endif

@@ -88,6 +88,8 @@ def lib():
         L.xwo_rep_check.restype = C.c_int
         L.xwo_exchange.argtypes = [P(Job), P(C.c_void_p), C.c_int, P(C.c_double), C.c_uint64]
         L.xwo_exchange.restype = C.c_int
+        L.xwo_kick.argtypes = [C.c_int, C.c_int, P(C.c_int8), P(C.c_int32), C.c_uint32, C.c_uint32, C.c_uint64,
+                               C.c_uint32, C.c_uint32, C.c_int, C.c_uint64, P(C.c_int8)]
         _lib = L
     return _lib
 
@@ -226,3 +228,15 @@ def exchange(job, reps, ladder, rnd):
     arr = (C.c_void_p * len(reps))(*[r.h for r in reps])
     lad = np.ascontiguousarray(ladder, dtype=np.float64)
     return lib().xwo_exchange(C.byref(job), arr, len(reps), ptr(lad, C.c_double), rnd)
+
+
+def kick(n, w, E, esc, key0, key1, rnd, replica, index, steps, thr_sign):
+    """The device kick of an elite restart (restart mode 1) of replica
+    `replica`, the index-th restarted in round `rnd`, from elite E
+    (column-major); esc = (row1, row2, col1, col2, new1, new2) or None."""
+    E = np.ascontiguousarray(E, dtype=np.int8).reshape(-1)
+    K = np.zeros(n * n, dtype=np.int8)
+    e = None if esc is None else np.ascontiguousarray(esc[:6], dtype=np.int32)
+    lib().xwo_kick(n, w, ptr(E, C.c_int8), None if e is None else ptr(e, C.c_int32), key0, key1, rnd, replica,
+                   index, steps, thr_sign, ptr(K, C.c_int8))
+    return K

@@ -89,6 +89,34 @@ def test_a_chunk_waits_out_a_long_predecessor(monkeypatch):
     assert run_states(monkeypatch, 2, jobs, p, 60000) == base
 
 
+def test_a_chunk_wait_that_runs_out_flags_the_replica_and_skips_its_later_chunks(monkeypatch):
+    """The wait of a chunk for its replica's previous chunk is bounded by
+    device time.  With the bound cut to 2 ms (XW_CHUNK_WAIT_NS) and a first
+    chunk of 10^5 iterations (a few tenths of a second for one warp), the
+    second chunk's wait runs out: it flags the replica, runs nothing, and
+    marks the replica's chunk count so that the third chunk skips as well
+    instead of running beside the first on the same record.  The first
+    chunk runs to its end, so the replica holds exactly its iterations, and
+    the next batch (default bound) runs normally."""
+    jobs = [{"n": 26, "w": 25, "seed": 17, "replicas": 1}]
+    p = X.Params(stop_on_solve=0, t_init=4.0, moves_per_launch=300000,
+                 squared_objective_fraction=0.0, parity_objective_fraction=0.0)
+    monkeypatch.setenv("XW_CHUNKS", "3")
+    monkeypatch.setenv("XW_CHUNK_WAIT_NS", "2000000")
+    b = X.Batch(jobs, p)
+    b.run(300000)
+    b.synchronize()
+    st = b.replica(0, 0)[0]
+    assert st.error == X.XW_DEVERR_CHUNK
+    assert st.iterations == 100000
+    assert b.results()[0][0].error == X.XW_DEVERR_CHUNK
+    b.close()
+    monkeypatch.delenv("XW_CHUNK_WAIT_NS")
+    monkeypatch.setenv("XW_CHUNKS", "1")
+    base, _ = run_states(monkeypatch, 1, jobs, p, 30000)
+    assert run_states(monkeypatch, 3, jobs, p, 30000)[0] == base
+
+
 def test_served_requests_end_the_same_in_chunked_rounds(monkeypatch):
     """The serving loop's class launches run chunked when a class has more
     replicas than resident warps; forcing chunks on small requests shows that

@@ -84,11 +84,18 @@ CASES = [
 ]
 
 
+@pytest.mark.parametrize("wpr", [1, 0], ids=["one_warp", "latency_mode"])
 @pytest.mark.parametrize("n,w,R,iters,kw", CASES, ids=lambda v: str(v) if not isinstance(v, dict) else "")
-def test_cooling_population_matches_oracle(n, w, R, iters, kw):
-    p = X.Params(stop_on_solve=0, **kw)
+def test_cooling_population_matches_oracle(n, w, R, iters, kw, wpr):
+    # wpr 0: a population this small runs in the latency mode (orders up to
+    # 32: a CTA of warps per replica speculating iterations); 1: one warp
+    # per replica
+    if wpr == 0 and n > 32:
+        pytest.skip("the latency mode covers orders up to 32")
+    p = X.Params(stop_on_solve=0, warps_per_replica=wpr, **kw)
     seed = 1000 + n * 7 + w
     batch = X.Batch([{"n": n, "w": w, "seed": seed, "replicas": R}], p)
+    assert all((c["warps_per_replica"] > 1) == (wpr == 0) for c in batch.classes())
     temps = [batch.replica(0, r)[0].reheat_temperature for r in range(R)]
     batch.run(iters)
     batch.synchronize()
@@ -101,10 +108,11 @@ def test_cooling_population_matches_oracle(n, w, R, iters, kw):
     batch.close()
 
 
+@pytest.mark.parametrize("wpr", [1, 0], ids=["one_warp", "latency_mode"])
 @pytest.mark.parametrize("n,w,R,interval,rounds", [(12, 11, 8, 300, 4), (26, 25, 6, 500, 3), (16, 4, 5, 250, 4)])
-def test_tempering_matches_oracle(n, w, R, interval, rounds):
+def test_tempering_matches_oracle(n, w, R, interval, rounds, wpr):
     p = X.Params(stop_on_solve=0, tempering=1, exchange_interval=interval, t_min=0.1, t_init=6.0,
-                 squared_objective_fraction=0.0, parity_objective_fraction=0.0)
+                 squared_objective_fraction=0.0, parity_objective_fraction=0.0, warps_per_replica=wpr)
     seed = 77 + n
     batch = X.Batch([{"n": n, "w": w, "seed": seed, "replicas": R},
                      {"n": n, "w": w, "seed": seed + 1, "replicas": R}], p)
@@ -129,7 +137,7 @@ def test_tempering_matches_oracle(n, w, R, interval, rounds):
 
 
 def test_mixed_orders_in_one_launch_match_oracle():
-    # replicas of different (n, w) share one persistent launch
+    # replicas of different (n, w) share one persistent launch per class
     p = X.Params(stop_on_solve=0, t_init=4.0, moves_per_launch=600)
     jobs = [{"n": 14, "w": 13, "seed": 5, "replicas": 3}, {"n": 24, "w": 23, "seed": 6, "replicas": 2},
             {"n": 18, "w": 9, "seed": 7, "replicas": 2}, {"n": 33, "w": 32, "seed": 8, "replicas": 2}]
@@ -147,9 +155,60 @@ def test_mixed_orders_in_one_launch_match_oracle():
     batch.close()
 
 
-def test_small_orders_in_an_eight_rows_per_lane_launch_match_oracle():
-    # a batch with an order above 128 runs every replica with the wide
-    # kernel (int16 Gram, 256-bit masks), small orders included
+SMALL_CASES = [c for c in CASES if c[0] <= 16]
+
+
+@pytest.mark.parametrize("rpw", [1, 2])
+@pytest.mark.parametrize("n,w,R,iters,kw", SMALL_CASES, ids=lambda v: str(v) if not isinstance(v, dict) else "")
+def test_orders_up_to_16_match_oracle_at_one_and_two_replicas_per_warp(n, w, R, iters, kw, rpw):
+    # two replicas per warp: each half-warp owns a replica; an odd count
+    # leaves one half of the last warp without one
+    R = R + 1
+    p = X.Params(stop_on_solve=0, replicas_per_warp=rpw, warps_per_replica=1, **kw)
+    seed = 3000 + n * 7 + w
+    batch = X.Batch([{"n": n, "w": w, "seed": seed, "replicas": R}], p)
+    assert all(c["replicas_per_warp"] == rpw for c in batch.classes())
+    temps = [batch.replica(0, r)[0].reheat_temperature for r in range(R)]
+    batch.run(iters)
+    batch.synchronize()
+    job = oracle_job(n, w, seed, p)
+    for r in range(R):
+        rep = O.Replica(job, r, start_of(n, w, seed, r, p), temps[r], r)
+        rep.run(iters, stop_on_solve=False)
+        compare(batch, 0, r, rep)
+    batch.close()
+
+
+def test_replicas_per_warp_leaves_every_replica_unchanged():
+    # a mixed batch at one and at two replicas per warp (orders up to 16
+    # share warps two by two), tempering and cooling jobs, 900 replicas
+    jobs = [{"n": 12, "w": 11, "seed": 60 + k, "replicas": 16} for k in range(30)] + \
+           [{"n": 16, "w": 4, "seed": 160 + k, "replicas": 16} for k in range(20)] + \
+           [{"n": 15, "w": 9, "seed": 260 + k, "replicas": 5} for k in range(12)]
+    out = []
+    for rpw in (1, 2):
+        p = X.Params(stop_on_solve=0, tempering=1, exchange_interval=300, t_min=0.1, t_init=6.0,
+                     replicas_per_warp=rpw, squared_objective_fraction=0.0, parity_objective_fraction=0.0)
+        b = X.Batch(jobs, p)
+        b.run(900)
+        b.synchronize()
+        states = []
+        for j, jb in enumerate(jobs):
+            for r in range(jb["replicas"]):
+                st, W, B, M = b.replica(j, r)
+                assert st.error == 0
+                states.append((st.iterations, st.moves, st.score, st.best_score, st.objective_total,
+                               st.temperature, st.rung, W.tobytes(), B.tobytes(), M.tobytes()))
+        b.close()
+        out.append(states)
+    assert out[0] == out[1]
+
+
+def test_orders_of_several_classes_in_one_round_match_oracle():
+    # a batch whose orders span the rows-per-lane classes runs one launch
+    # per class side by side in each round (eight rows per lane with the
+    # int16 Gram and 256-bit masks for the order above 128, one row per
+    # lane for 26, two for 40)
     p = X.Params(stop_on_solve=0, t_init=5.0, moves_per_launch=100)
     jobs = [{"n": 150, "w": 149, "seed": 21, "replicas": 1}, {"n": 26, "w": 25, "seed": 22, "replicas": 2},
             {"n": 40, "w": 4, "seed": 23, "replicas": 2}]
@@ -165,3 +224,33 @@ def test_small_orders_in_an_eight_rows_per_lane_launch_match_oracle():
             rep.run(200, stop_on_solve=False)
             compare(batch, j, r, rep)
     batch.close()
+
+
+@pytest.mark.parametrize("wpr", [2, 4, 8, 16])
+@pytest.mark.parametrize("stop", [0, 2])
+def test_latency_mode_ends_every_replica_as_one_warp(wpr, stop):
+    # every warps-per-replica count and both deterministic stop rules (run
+    # on, or stop at the replica's own solve): replicas end identical to the
+    # one-warp kernel's, counters and best states included; W(12,11) solves
+    # within the budget for some seeds, so stop rule 2 ends replicas early
+    jobs = [{"n": 12, "w": 11, "seed": 900 + k, "replicas": 3} for k in range(6)] + \
+           [{"n": 30, "w": 29, "seed": 950, "replicas": 2}, {"n": 15, "w": 5, "seed": 951, "replicas": 3}]
+    out = []
+    for k in (1, wpr):
+        p = X.Params(stop_on_solve=stop, t_init=3.0, moves_per_launch=2500, warps_per_replica=k,
+                     stuck_threshold=900, moves_per_cool=60, max_moves=3 * 9000)
+        b = X.Batch(jobs, p)
+        b.run(9000)
+        b.synchronize()
+        states = []
+        for j, jb in enumerate(jobs):
+            for r in range(jb["replicas"]):
+                st, W, B, M = b.replica(j, r)
+                assert st.error == 0
+                states.append((st.iterations, st.moves, st.candidate_evaluations, st.score, st.best_score,
+                               st.objective_total, st.temperature, st.moves_since_improvement,
+                               st.cooling_counter, W.tobytes(), B.tobytes(), M.tobytes()))
+        res = [(r.score, r.conflicts, r.best_replica, r.moves, r.solved, r.solved_iteration) for r, _ in b.results()]
+        b.close()
+        out.append((states, res))
+    assert out[0] == out[1]

@@ -256,3 +256,23 @@ def test_saving_a_finished_request_is_refused(tmp_path):
         s.wait(rid, timeout=120)
         with pytest.raises(X.XwError):
             s.save(rid, tmp_path / "late.xwpop", timeout=10)
+
+
+def test_retired_requests_are_verified_on_the_device_as_on_the_host():
+    """Every retiring request's W is rescored on the device (tensor cores
+    for orders padded to 32..128, zero padding past n) in one batch per
+    round; the returned score, conflicts and exact flag must agree with the
+    host's int64 check (xw_score / xw_verify) for solved and unsolved
+    requests alike, across orders of every padded size."""
+    reqs = [req(12, 11, 31, 8, 200000), req(14, 13, 32, 8, 200000), req(20, 19, 33, 8, 3000),
+            req(36, 4, 34, 8, 200000), req(40, 39, 35, 4, 2000), req(70, 4, 36, 4, 200000),
+            req(100, 99, 37, 2, 300), req(26, 25, 38, 16, 4000), req(150, 149, 39, 2, 100)]
+    out, _ = serve(reqs)
+    for (res, W), r in zip(out, reqs):
+        n, w = r["n"], r["w"]
+        assert res.state == X.REQ_DONE and res.status == X.XW_OK, (n, w)
+        host = X.score(n, w, W)
+        assert (res.score, res.conflicts) == (host[0], host[1]), (n, w)
+        assert bool(res.verified) == (bool(res.solved) and X.verify(n, w, W) == 3), (n, w)
+        if res.solved:
+            assert res.verified and res.score == 0, (n, w)

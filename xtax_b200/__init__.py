@@ -24,6 +24,8 @@ HEADER = os.path.join(os.path.dirname(_HERE), "include", "xw.h")
 
 XW_OK, XW_ERR_INVALID, XW_ERR_CUDA, XW_ERR_CAPACITY, XW_ERR_INTERNAL = 0, 1, 2, 3, 4
 XW_ERR_NOT_FOUND, XW_ERR_TIMEOUT, XW_ERR_IO = 5, 6, 7
+# device error bits of a replica (xw_replica_state.error)
+XW_DEVERR_SCORE, XW_DEVERR_MINORITY, XW_DEVERR_KERNEL, XW_DEVERR_CHUNK = 1, 2, 4, 8
 MAX_ORDER_CUDA = 1024      # largest order the device path anneals
 MAX_ORDER_SHARED = 256     # largest order whose replica state sits in shared memory (and served orders)
 MAX_CANDIDATE_SAMPLES = 32
@@ -51,7 +53,8 @@ class _Params(C.Structure):
                 ("max_moves", C.c_uint64), ("tempering", C.c_int32),
                 ("exchange_interval", C.c_int32), ("objective", C.c_int32),
                 ("move_set", C.c_int32), ("start_kind", C.c_int32), ("stop_on_solve", C.c_int32),
-                ("warps_per_block", C.c_int32), ("reserved", C.c_int32)]
+                ("warps_per_block", C.c_int32), ("replicas_per_warp", C.c_int32),
+                ("warps_per_replica", C.c_int32), ("restart_kicks", C.c_int32)]
 
 
 class _DeviceInfo(C.Structure):
@@ -80,7 +83,8 @@ class JobResult(C.Structure):
                 ("solved", C.c_int32), ("verified", C.c_int32), ("error", C.c_int32),
                 ("moves", C.c_uint64), ("candidate_evaluations", C.c_uint64),
                 ("iterations", C.c_uint64), ("solved_iteration", C.c_uint64),
-                ("time_to_solution_seconds", C.c_double)]
+                ("time_to_solution_seconds", C.c_double), ("accepted_moves", C.c_uint64),
+                ("accepted_rows", C.c_uint64), ("two_row_evaluations", C.c_uint64)]
 
 
 class ReplicaState(C.Structure):
@@ -91,7 +95,17 @@ class ReplicaState(C.Structure):
                 ("temperature", C.c_double), ("reheat_temperature", C.c_double),
                 ("moves_since_improvement", C.c_int32), ("cooling_counter", C.c_int32),
                 ("rung", C.c_int32), ("objective_kind", C.c_int32), ("status", C.c_uint32),
-                ("error", C.c_uint32)]
+                ("error", C.c_uint32), ("accepted_moves", C.c_uint32), ("accepted_rows", C.c_uint32),
+                ("two_row_evaluations", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class LaunchClass(C.Structure):
+    """xw_launch_class: one launch of a batch's round and its shape."""
+    _fields_ = [("min_order", C.c_int32), ("max_order", C.c_int32), ("large", C.c_int32),
+                ("rows_per_lane", C.c_int32), ("replicas_per_warp", C.c_int32),
+                ("warps_per_block", C.c_int32), ("blocks", C.c_int32), ("slot_bytes", C.c_int32),
+                ("chunks", C.c_int32), ("replicas", C.c_int32), ("general", C.c_int32),
+                ("warps_per_replica", C.c_int32)]
 
 
 class ServerConfig(C.Structure):
@@ -101,7 +115,7 @@ class ServerConfig(C.Structure):
                 ("warps_per_block", C.c_int32), ("prep_threads", C.c_int32),
                 ("sylvester_shortcut", C.c_int32), ("arena_bytes", C.c_uint64),
                 ("schedule", C.c_int32), ("max_active_replicas", C.c_int32),
-                ("reserved", C.c_int32 * 6)]
+                ("replicas_per_warp", C.c_int32), ("reserved", C.c_int32 * 5)]
 
 
 class _Request(C.Structure):
@@ -188,6 +202,8 @@ def lib():
             "xw_batch_read_replica": (i32, [C.c_void_p, i32, i32, P(ReplicaState), P(i8), P(i8),
                                             P(C.c_uint8)]),
             "xw_batch_shape": (i32, [C.c_void_p, P(i32), P(i32), P(i32)]),
+            "xw_batch_classes": (i32, [C.c_void_p, P(LaunchClass), i32, P(i32)]),
+            "xw_batch_restart": (i32, [C.c_void_p, i32, P(i32)]),
             "xw_batch_bytes": (i32, [C.c_void_p, P(u64), P(u64)]),
             "xw_batch_destroy": (None, [C.c_void_p]),
             "xw_batch_solve": (i32, [P(JobSpec), i32, P(_Params), P(i8), u64, P(JobResult), P(i8)]),
@@ -270,6 +286,9 @@ class Params:
     start_kind: int = 0
     stop_on_solve: int = 1
     warps_per_block: int = 0
+    replicas_per_warp: int = 0
+    warps_per_replica: int = 0
+    restart_kicks: int = 0
 
     def to_c(self):
         p = _Params()
@@ -498,6 +517,20 @@ class Batch:
         a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
         _check(lib().xw_batch_shape(self.h, C.byref(a), C.byref(b), C.byref(c)))
         return a.value, b.value, c.value
+
+    def restart(self, job=0):
+        """xw_batch_restart: one elite restart of `job`; returns the number of
+        replicas restarted."""
+        n = C.c_int32()
+        _check(lib().xw_batch_restart(self.h, job, C.byref(n)))
+        return n.value
+
+    def classes(self):
+        """The launches of a round, one dict per launch class (xw_batch_classes)."""
+        arr = (LaunchClass * 16)()
+        n = C.c_int32()
+        _check(lib().xw_batch_classes(self.h, arr, 16, C.byref(n)))
+        return [{f: getattr(arr[i], f) for f, _ in LaunchClass._fields_} for i in range(min(n.value, 16))]
 
     def transfer_bytes(self):
         """(host-to-device bytes at creation, device-to-host bytes per results())"""

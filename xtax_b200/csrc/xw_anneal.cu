@@ -46,6 +46,18 @@ namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
 
+// Lane groups.  A replica is owned by a group of GW lanes: the whole warp
+// (GW = 32), or one half of it (GW = 16, orders up to 16: two replicas per
+// warp, each half with its own shared-memory slot and its own work items).
+// Warp collectives name only the group's lanes; the two halves' replicas
+// are independent and the hardware runs them side by side wherever their
+// control flow agrees.
+template <int GW>
+__device__ __forceinline__ unsigned group_mask() {
+    if constexpr (GW == 32) return FULL;
+    else return 0xffffu << (threadIdx.x & 16);
+}
+
 // Metropolis thresholds kept per replica for objective increases 1..kThrTable.
 constexpr uint32_t kThrTable = 64;
 
@@ -404,13 +416,13 @@ __device__ __forceinline__ int pair_new(const Update& u, int op, const int8_t* W
 
 // evaluate_move_warp (xweigh_cuda.cu:449-599): lane-partial deltas over the
 // lane's own rows; the caller reduces them across the warp.
-template <int OPL, typename GT, bool GEN>
+template <int OPL, typename GT, bool GEN, int GW = 32>
 __device__ __forceinline__ Deltas eval_lane(const Update& u, const int8_t* W, const GT* G, int n, int ld,
                                             int lane) {
     Deltas d = {0, 0, 0, 0};
 #pragma unroll
     for (int k = 0; k < OPL; ++k) {
-        const int o = lane + 32 * k;
+        const int o = lane + GW * k;
         if (o < n && o != u.R1 && o != u.R2) {
             const int o1 = G[u.R1 * ld + o];
             acc<GEN>(d, o1, o1 + u.A1 * W[u.X1 * n + o] + u.B1 * W[u.Y1 * n + o]);
@@ -429,13 +441,14 @@ __device__ __forceinline__ Deltas eval_lane(const Update& u, const int8_t* W, co
 
 // commit_sign_flip / commit_support_switch / commit_double_sign_flip
 // (xweigh_cuda.cu:607-877) and the within-row swap, in the two-row form.
-template <int OPL, int MW, typename GT, bool GEN>
+template <int OPL, int MW, typename GT, bool GEN, int GW = 32>
 __device__ void commit(uint32_t d0, uint32_t d1, const Update& u, int ds, int8_t* W, GT* G, int32_t* res,
                        uint8_t* mino, uint64_t* mask, int n, int ld, int m, int sparse, int lane) {
+    const unsigned gm = group_mask<GW>();
     int s1 = 0;
 #pragma unroll
     for (int k = 0; k < OPL; ++k) {
-        const int o = lane + 32 * k;
+        const int o = lane + GW * k;
         if (o < n && o != u.R1 && o != u.R2) {
             const int o1 = G[u.R1 * ld + o];
             const int n1 = o1 + u.A1 * W[u.X1 * n + o] + u.B1 * W[u.Y1 * n + o];
@@ -454,8 +467,8 @@ __device__ void commit(uint32_t d0, uint32_t d1, const Update& u, int ds, int8_t
             s1 += e1;
         }
     }
-    const int S1 = __reduce_add_sync(FULL, s1);
-    __syncwarp();
+    const int S1 = __reduce_add_sync(gm, s1);
+    __syncwarp(gm);
     if (lane == 0) {
         const int kind = (d0 >> 1) & 3, r1 = (d0 >> 3) & 255, r2 = (d0 >> 11) & 255;
         const int c1 = (d0 >> 19) & 255, c2 = d1 & 255;
@@ -499,7 +512,7 @@ __device__ void commit(uint32_t d0, uint32_t d1, const Update& u, int ds, int8_t
             mask[MW * r1 + (c2 >> 6)] |= 1ull << (c2 & 63);
         }
     }
-    __syncwarp();
+    __syncwarp(gm);
 }
 
 // tab[d-1] = ceil(exp(-d/T) * 2^32), computed with the same division and
@@ -507,20 +520,22 @@ __device__ void commit(uint32_t d0, uint32_t d1, const Update& u, int ds, int8_t
 //   u * 2^-32 < exp(-d/T)  <=>  u < tab[d-1]
 // exactly (both sides scaled by 2^32 without rounding; u is an integer).
 // Rebuilt whenever the replica's temperature changes.
+template <int GW = 32>
 __device__ __noinline__ void build_thresholds(uint64_t* tab, double T, int lane) {
     const double t = T > 1.0e-12 ? T : 1.0e-12;
-    for (uint32_t d = lane + 1; d <= kThrTable; d += 32) {
+    for (uint32_t d = lane + 1; d <= kThrTable; d += GW) {
         const double e = acceptance_exp(__ddiv_rn(-(double)d, t));
         tab[d - 1] = (uint64_t)ceil(__dmul_rn(e, 0x1p32));
     }
-    __syncwarp();
+    __syncwarp(group_mask<GW>());
 }
 
+template <int GW = 32>
 __device__ __forceinline__ void copy16(void* dst, const void* src, uint32_t bytes, int lane) {
     const uint32_t chunks = xw_pad16(bytes) / 16u;
     uint4* d = reinterpret_cast<uint4*>(dst);
     const uint4* s = reinterpret_cast<const uint4*>(src);
-    for (uint32_t i = lane; i < chunks; i += 32) d[i] = s[i];
+    for (uint32_t i = lane; i < chunks; i += GW) d[i] = s[i];
 }
 
 __device__ __forceinline__ uint64_t globaltimer() {
@@ -529,18 +544,49 @@ __device__ __forceinline__ uint64_t globaltimer() {
     return t;
 }
 
-template <int OPL, bool GEN>
-__device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int lane, uint64_t chunk_iters) {
+// A loaded replica: its shared-memory structures, the job's constants the
+// iteration reads, and the scalar state the loop carries.
+template <int OPL, int GW>
+struct Replica {
+    static constexpr int MW = OPL > 4 ? 4 : 2;
+    using GT = typename std::conditional<(OPL > 4), int16_t, int32_t>::type;
+    uint8_t* rec;
+    RepHeader* H;
+    XwJob* J;
+    int8_t* sW;
+    GT* sG;
+    int32_t* sRes;
+    uint8_t* sMino;
+    uint64_t* sMask;
+    uint64_t* sThr;
+    int n, w, m, sparse, ld, obj_kind;
+    uint32_t nn, status0;
+    // scalar state
+    uint64_t it, iters, moves, cand_evals;
+    uint32_t accepted, accepted_rows, two_row_evals;
+    int score, conflicts, best_s, best_c, msi, cool;
+    int64_t obj_total;
+    double T, reheat_T;
+};
+
+// Loads replica `rid` into the slot: W and the minority lists, the masks,
+// Gram and residuals rebuilt from W and checked against the header.  False
+// when the replica does not run (job done or solved, budget spent, or a
+// failed self-check, which flags the header).  The group's lanes call it.
+template <int OPL, bool GEN, int GW>
+__device__ __forceinline__ bool load_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int lane,
+                                             uint64_t chunk_iters, Replica<OPL, GW>& R) {
+    constexpr int MW = Replica<OPL, GW>::MW;
+    using GT = typename Replica<OPL, GW>::GT;
+    const unsigned gm = group_mask<GW>();
     uint8_t* rec = a.arena + a.rec_off[rid];
     RepHeader* H = reinterpret_cast<RepHeader*>(rec);
     const uint32_t jid = H->job;
     XwJob* J = a.jobs + jid;
-    if (*(volatile int32_t*)&J->done) return;
-    if (a.stop_on_solve == 1 && *(volatile int32_t*)&J->solved) return;
+    if (*(volatile int32_t*)&J->done) return false;
+    if (a.stop_on_solve == 1 && *(volatile int32_t*)&J->solved) return false;
 
     // eight rows per lane: int16 Gram and 256-bit row masks (slot_layout)
-    constexpr int MW = OPL > 4 ? 4 : 2;
-    using GT = typename std::conditional<(OPL > 4), int16_t, int32_t>::type;
     const int n = J->n, w = J->w, m = J->m, sparse = J->sparse;
     const SlotLayout L = slot_layout(n, m, OPL > 4);
     const int ld = L.ld;
@@ -549,28 +595,24 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
     int32_t* sRes = reinterpret_cast<int32_t*>(slot + L.off_res);
     uint8_t* sMino = slot + L.off_mino;
     uint64_t* sMask = reinterpret_cast<uint64_t*>(slot + L.off_mask);
-    uint4* sDraw = reinterpret_cast<uint4*>(slot + L.off_draws);
-    const uint32_t* sDw = reinterpret_cast<const uint32_t*>(sDraw);
-    View* sView = reinterpret_cast<View*>(slot + L.off_view);
-    uint64_t* sThr = reinterpret_cast<uint64_t*>(slot + L.off_thr);
 
     uint64_t it = H->it;
     uint64_t iters = chunk_iters;
     if (J->budget_iters) {
-        if (it >= J->budget_iters) return;
+        if (it >= J->budget_iters) return false;
         if (iters > J->budget_iters - it) iters = J->budget_iters - it;
     }
 
     // ---- load W and the minority lists; rebuild masks, Gram, residuals ----
     const uint32_t nn = (uint32_t)(n * n);
-    copy16(sW, rec + J->off_w, nn, lane);
+    copy16<GW>(sW, rec + J->off_w, nn, lane);
     const uint32_t status0 = H->status;
-    if (m > 0 && (status0 & XW_STATUS_INIT)) copy16(sMino, rec + J->off_mino, (uint32_t)(n * m), lane);
-    __syncwarp();
+    if (m > 0 && (status0 & XW_STATUS_INIT)) copy16<GW>(sMino, rec + J->off_mino, (uint32_t)(n * m), lane);
+    __syncwarp(gm);
     int bad_rows = 0;
 #pragma unroll
     for (int k = 0; k < OPL; ++k) {
-        const int o = lane + 32 * k;
+        const int o = lane + GW * k;
         if (o < n) {
             int pos = 0, weight = 0;
 #pragma unroll
@@ -592,16 +634,16 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
             if (m > 0 && !(status0 & XW_STATUS_INIT) && pos != m) bad_rows = 1;
         }
     }
-    if (__any_sync(FULL, bad_rows)) {
+    if (__any_sync(gm, bad_rows)) {
         if (lane == 0) H->err |= XW_ERR_MINORITY;
-        return;
+        return false;
     }
-    __syncwarp();
+    __syncwarp(gm);
     int p_score = 0, p_conf = 0, p_par = 0;
     long long p_sq = 0;
 #pragma unroll
     for (int k = 0; k < OPL; ++k) {
-        const int o = lane + 32 * k;
+        const int o = lane + GW * k;
         if (o < n) {
             int r_sum = 0;
 #pragma unroll 1
@@ -622,62 +664,139 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
             p_score += r_sum;
         }
     }
-    const int score0 = __reduce_add_sync(FULL, p_score) / 2;
-    const int conf0 = __reduce_add_sync(FULL, p_conf) / 2;
+    const int score0 = __reduce_add_sync(gm, p_score) / 2;
+    const int conf0 = __reduce_add_sync(gm, p_conf) / 2;
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) p_sq += __shfl_xor_sync(FULL, p_sq, off);
+    for (int off = GW / 2; off > 0; off >>= 1) p_sq += __shfl_xor_sync(gm, p_sq, off, GW);
     const long long sq0 = p_sq / 2;
-    const int par0 = __reduce_add_sync(FULL, p_par) / 2;
-    __syncwarp();
+    const int par0 = __reduce_add_sync(gm, p_par) / 2;
+    __syncwarp(gm);
 
     const int obj_kind = GEN ? H->obj_kind : 0;
     if (!GEN && (H->obj_kind != 0 || J->move_set != 0)) {
         // the lean kernel was launched for a replica that needs the general one
         if (lane == 0) H->err |= XW_ERR_KERNEL;
-        return;
+        return false;
     }
     const int64_t obj0 = obj_kind == 1 ? sq0 : obj_kind == 2 ? par0 : score0;
-    int score, conflicts, best_s, best_c, msi, cool;
-    int64_t obj_total;
-    uint64_t moves, cand_evals;
-    double T = H->temperature;
-    const double reheat_T = H->reheat_temperature;
+    R.T = H->temperature;
+    R.reheat_T = H->reheat_temperature;
     if (status0 & XW_STATUS_INIT) {
         if (H->score != score0 || H->conflicts != conf0 || H->obj_total != obj0) {
             if (lane == 0) H->err |= XW_ERR_SCORE;
-            return;
+            return false;
         }
-        best_s = H->best_score;
-        best_c = H->best_conflicts;
-        msi = H->msi;
-        cool = H->cool_ctr;
-        moves = H->moves;
-        cand_evals = H->cand_evals;
+        R.best_s = H->best_score;
+        R.best_c = H->best_conflicts;
+        R.msi = H->msi;
+        R.cool = H->cool_ctr;
+        R.moves = H->moves;
+        R.cand_evals = H->cand_evals;
+        R.accepted = H->accepted;
+        R.accepted_rows = H->accepted_rows;
+        R.two_row_evals = H->two_row_evals;
     } else {
-        best_s = score0;
-        best_c = conf0;
-        msi = 0;
-        cool = 0;
-        moves = 0;
-        cand_evals = 0;
-        copy16(rec + J->off_best, sW, nn, lane);
+        R.best_s = score0;
+        R.best_c = conf0;
+        R.msi = 0;
+        R.cool = 0;
+        R.moves = 0;
+        R.cand_evals = 0;
+        R.accepted = 0;
+        R.accepted_rows = 0;
+        R.two_row_evals = 0;
+        copy16<GW>(rec + J->off_best, sW, nn, lane);
     }
-    score = score0;
-    conflicts = conf0;
-    obj_total = obj0;
+    R.score = score0;
+    R.conflicts = conf0;
+    R.obj_total = obj0;
+    R.rec = rec;
+    R.H = H;
+    R.J = J;
+    R.sW = sW;
+    R.sG = sG;
+    R.sRes = sRes;
+    R.sMino = sMino;
+    R.sMask = sMask;
+    R.sThr = reinterpret_cast<uint64_t*>(slot + L.off_thr);
+    R.n = n;
+    R.w = w;
+    R.m = m;
+    R.sparse = sparse;
+    R.ld = ld;
+    R.obj_kind = obj_kind;
+    R.nn = nn;
+    R.status0 = status0;
+    R.it = it;
+    R.iters = iters;
+    return true;
+}
 
-    // ---- job constants ----
-    const int tempering = J->tempering;
-    const int cs = J->candidate_samples, ts = J->target_samples;
-    const int mpc = J->moves_per_cool, stuck = J->stuck_threshold;
-    const uint32_t k0 = J->key0, k1 = J->key1, stream = H->stream;
-    const uint64_t thr_greedy = J->thr_greedy;
-    const double t_min = J->t_min, cooling = J->cooling, reheat = J->reheat;
-    const int bpc = 4 + (ts <= 4 ? 1 : 2);          // cached blocks per candidate
-    const bool coop = ts <= 8;                      // cooperative hot-row tournament
+// Writes the replica's W, minority lists and scalar state back to its record.
+template <int OPL, int GW>
+__device__ __forceinline__ void store_replica(const Replica<OPL, GW>& R, int lane) {
+    const unsigned gm = group_mask<GW>();
+    __syncwarp(gm);
+    copy16<GW>(R.rec + R.J->off_w, R.sW, R.nn, lane);
+    if (R.m > 0) copy16<GW>(R.rec + R.J->off_mino, R.sMino, (uint32_t)(R.n * R.m), lane);
+    if (lane == 0) {
+        RepHeader* H = R.H;
+        H->it = R.it;
+        H->moves = R.moves;
+        H->cand_evals = R.cand_evals;
+        H->accepted = R.accepted;
+        H->accepted_rows = R.accepted_rows;
+        H->two_row_evals = R.two_row_evals;
+        H->score = R.score;
+        H->conflicts = R.conflicts;
+        H->best_score = R.best_s;
+        H->best_conflicts = R.best_c;
+        H->obj_total = R.obj_total;
+        H->temperature = R.T;
+        H->msi = R.msi;
+        H->cool_ctr = R.cool;
+        H->status = R.status0 | XW_STATUS_INIT | (R.best_s == 0 ? XW_STATUS_SOLVED : 0u);
+    }
+    __syncwarp(gm);
+}
+
+// The proposing side of an iteration: the job constants the draws and
+// proposals read, this group's draw buffer and View, and the lane's
+// cached-block slots and register context.
+template <int GW>
+struct Proposer {
+    uint4* sDraw;
+    const uint32_t* sDw;
+    View* sView;
+    Reg rg;
+    uint32_t my_slot, my_slot2;
+    uint32_t k0, k1, stream;
+    uint64_t thr_greedy;
+    int cs, ts, bpc;
+    bool coop;
+};
+
+// Sets up the proposer of a loaded replica with the draw buffer and View at
+// `draws` and `view` (the group's own).  The group's lanes call it.
+template <int OPL, int GW>
+__device__ __forceinline__ void setup_proposer(const Replica<OPL, GW>& R, uint4* draws, View* view, int lane,
+                                               Proposer<GW>& P) {
+    const XwJob* J = R.J;
+    const int n = R.n;
+    P.sDraw = draws;
+    P.sDw = reinterpret_cast<const uint32_t*>(draws);
+    P.sView = view;
+    P.cs = J->candidate_samples;
+    P.ts = J->target_samples;
+    P.k0 = J->key0;
+    P.k1 = J->key1;
+    P.stream = R.H->stream;
+    P.thr_greedy = J->thr_greedy;
+    P.bpc = 4 + (P.ts <= 4 ? 1 : 2);          // cached blocks per candidate
+    P.coop = P.ts <= 8;                       // cooperative hot-row tournament
     if (lane == 0) {
         View v;
-        v.W = sW; v.mino = sMino; v.res = sRes; v.mask = sMask; v.dw = sDw;
+        v.W = R.sW; v.mino = R.sMino; v.res = R.sRes; v.mask = R.sMask; v.dw = P.sDw;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int lo = 64 * q;
@@ -685,173 +804,399 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
         }
         v.thr_target = J->thr_target; v.thr_dbl = J->thr_double; v.thr_sign = J->thr_sign;
         v.thr_swsign = J->thr_swsign;
-        v.n = n; v.w = w; v.m = m; v.sparse = sparse; v.ts = ts; v.bpc = bpc; v.cc = 31 / bpc;
+        v.n = n; v.w = R.w; v.m = R.m; v.sparse = R.sparse; v.ts = P.ts; v.bpc = P.bpc; v.cc = 31 / P.bpc;
         v.move_set = J->move_set;
-        v.stream = stream; v.k0 = k0; v.k1 = k1; v.pad = 0;
-        *sView = v;
+        v.stream = P.stream; v.k0 = P.k0; v.k1 = P.k1; v.pad = 0;
+        *view = v;
     }
-    __syncwarp();
+    __syncwarp(group_mask<GW>());
 
-    build_thresholds(sThr, T, lane);
-
-    // lane -> cached Philox block of this iteration
-    uint32_t my_slot = 0;
+    // lane -> cached Philox blocks of an iteration (block 0 is the
+    // move-level block, 1 + c*bpc + b block b of candidate c); a half-warp
+    // group computes two blocks per lane
+    const int bpc = P.bpc;
+    P.my_slot = 0;
+    P.my_slot2 = 0;
     if (lane > 0) {
         const int q = lane - 1, c = q / bpc, b = q - c * bpc;
-        my_slot = cand_slot(c, b);
+        P.my_slot = cand_slot(c, b);
+    }
+    if constexpr (GW == 16) {
+        const int q = lane + 15, c = q / bpc, b = q - c * bpc;
+        P.my_slot2 = cand_slot(c, b);
     }
     // register context of candidate `lane` for the inlined proposal path
-    Reg rg;
-    rg.W = sW; rg.mino = sMino; rg.mask = sMask;
-    rg.cw = sDw + (1 + lane * bpc) * 4;
+    Reg& rg = P.rg;
+    rg.W = R.sW; rg.mino = R.sMino; rg.mask = R.sMask;
+    rg.cw = P.sDw + (1 + lane * bpc) * 4;
     rg.cached = lane < 31 / bpc;
     rg.thr_target = J->thr_target; rg.thr_dbl = J->thr_double; rg.thr_sign = J->thr_sign;
     rg.thr_swsign = J->thr_swsign;
-    rg.n = n; rg.w = w; rg.m = m; rg.sparse = sparse; rg.move_set = J->move_set;
-    rg.stream = stream; rg.k0 = k0; rg.k1 = k1;
+    rg.n = n; rg.w = R.w; rg.m = R.m; rg.sparse = R.sparse; rg.move_set = J->move_set;
+    rg.stream = P.stream; rg.k0 = P.k0; rg.k1 = P.k1;
+}
 
-    uint64_t done = 0;
-#pragma unroll 1
-    for (; done < iters; ++done) {
-        // 1: every replica of the job stops soon after any solve;
-        // 2: a replica stops at its own solve only, so that each replica's
-        //    trajectory is independent of how the launches are scheduled
-        if (a.stop_on_solve) {
-            if (best_s == 0) break;
-            if (a.stop_on_solve == 1 && (done & 63) == 63 && *(volatile int32_t*)&J->solved) break;
-        }
-        // A: draws
-        sDraw[lane] = draw_block(my_slot, it, stream, k0, k1);
-        __syncwarp();
-        const uint4 mblk = sDraw[0];
-        const int count = (uint64_t)mblk.x < thr_greedy ? cs : 1;
+// The move an iteration puts to the Metropolis test: the first best of its
+// candidates (b0 = 0: none was valid), its deltas, the iteration's
+// acceptance draw and the number of candidates evaluated.
+struct Choice {
+    uint32_t b0, b1;
+    int bds, bdc, bprim;
+    uint32_t u;
+    uint32_t evals, evals2;   // candidates evaluated; those changing two rows
+};
 
-        // C: cooperative hot-row tournaments for candidates 0..3
+// Phases A-E of iteration `it` against the replica's current state: draws,
+// hot-row tournaments, proposals, and the evaluation of the candidates in
+// order.  Reads the state and writes only the group's draw buffer.
+template <int OPL, bool GEN, int GW>
+__device__ __forceinline__ Choice choose_move(const Replica<OPL, GW>& R, Proposer<GW>& P, uint64_t it, int lane) {
+    constexpr int MW = Replica<OPL, GW>::MW;
+    using GT = typename Replica<OPL, GW>::GT;
+    const unsigned gm = group_mask<GW>();
+    const int n = R.n, ts = P.ts, bpc = P.bpc;
+    const uint32_t k0 = P.k0, k1 = P.k1, stream = P.stream;
+    const uint32_t* sDw = P.sDw;
+    const int32_t* sRes = R.sRes;
+    // A: draws
+    P.sDraw[lane] = draw_block(P.my_slot, it, stream, k0, k1);
+    if constexpr (GW == 16) P.sDraw[lane + 16] = draw_block(P.my_slot2, it, stream, k0, k1);
+    __syncwarp(gm);
+    const uint4 mblk = P.sDraw[0];
+    const int count = (uint64_t)mblk.x < P.thr_greedy ? P.cs : 1;
+
+    // C: cooperative hot-row tournaments for candidates 0..3, 8 lanes
+    // (samples) per candidate: one pass of the warp, two of a half-warp
+    int coop_row = 0;
+    if constexpr (GW == 32) {
         int hot_key = 0;
-        if (coop) {
+        if (P.coop) {
             const int c = lane >> 3, s = lane & 7;
             if (c < count && s < ts) {
                 const uint32_t wd = sDw[(1 + c * bpc + 4 + (s >> 2)) * 4 + (s & 3)];
-                const uint32_t row = draw_index(wd, (uint32_t)n, cand_slot(c, 4 + (s >> 2)), it, stream, k0, k1, s & 3);
+                const uint32_t row =
+                    draw_index(wd, (uint32_t)n, cand_slot(c, 4 + (s >> 2)), it, stream, k0, k1, s & 3);
                 hot_key = (sRes[row] << 13) | ((31 - s) << 8) | (int)row;
             }
             hot_key = max(hot_key, __shfl_xor_sync(FULL, hot_key, 1));
             hot_key = max(hot_key, __shfl_xor_sync(FULL, hot_key, 2));
             hot_key = max(hot_key, __shfl_xor_sync(FULL, hot_key, 4));
         }
-        const int coop_row = __shfl_sync(FULL, hot_key, (lane & 3) << 3) & 0xff;
+        coop_row = __shfl_sync(FULL, hot_key, (lane & 3) << 3) & 0xff;
+    } else {
+        int keys[2] = {0, 0};
+        if (P.coop) {
+#pragma unroll
+            for (int pass = 0; pass < 2; ++pass) {
+                const int c = 2 * pass + (lane >> 3), s = lane & 7;
+                int hot_key = 0;
+                if (c < count && s < ts) {
+                    const uint32_t wd = sDw[(1 + c * bpc + 4 + (s >> 2)) * 4 + (s & 3)];
+                    const uint32_t row =
+                        draw_index(wd, (uint32_t)n, cand_slot(c, 4 + (s >> 2)), it, stream, k0, k1, s & 3);
+                    hot_key = (sRes[row] << 13) | ((31 - s) << 8) | (int)row;
+                }
+                hot_key = max(hot_key, __shfl_xor_sync(gm, hot_key, 1, 16));
+                hot_key = max(hot_key, __shfl_xor_sync(gm, hot_key, 2, 16));
+                hot_key = max(hot_key, __shfl_xor_sync(gm, hot_key, 4, 16));
+                keys[pass] = hot_key;
+            }
+        }
+        // candidate c's winner sits in pass c/2 at lane (c%2)*8
+        const int k0v = __shfl_sync(gm, keys[0], (lane & 1) << 3, 16);
+        const int k1v = __shfl_sync(gm, keys[1], (lane & 1) << 3, 16);
+        coop_row = ((lane >> 1) & 1 ? k1v : k0v) & 0xff;
+    }
 
-        // D: proposals, lane c proposes candidate c
-        uint2 desc = make_uint2(0u, 0u);
-        rg.it = it;
-        if (lane < count) desc = d_propose<MW, GEN>(rg, sView, lane, coop && lane < 4, coop_row);
-        __syncwarp();
+    // D: proposals, lane c proposes candidate c
+    uint2 desc = make_uint2(0u, 0u);
+    P.rg.it = it;
+    if (lane < count) desc = d_propose<MW, GEN>(P.rg, P.sView, lane, P.coop && lane < 4, coop_row);
+    __syncwarp(gm);
 
-        // E: evaluate in candidate order, keep the first best
-        bool have = false;
-        uint32_t b0 = 0, b1 = 0;
-        int bds = 0, bdc = 0, bprim = 0;
+    // E: evaluate in candidate order, keep the first best
+    Choice ch;
+    ch.b0 = 0; ch.b1 = 0; ch.bds = 0; ch.bdc = 0; ch.bprim = 0;
+    ch.u = mblk.y;
+    ch.evals = 0;
+    ch.evals2 = 0;
 #pragma unroll 1
-        for (int c = 0; c < count; ++c) {
-            const uint32_t e0 = __shfl_sync(FULL, desc.x, c);
-            const uint32_t e1 = __shfl_sync(FULL, desc.y, c);
-            if (!(e0 & 1u)) continue;
-            const Update u = decode(e0, e1, sW, n);
-            const Deltas d = eval_lane<OPL, GT, GEN>(u, sW, sG, n, ld, lane);
-            const int packed = __reduce_add_sync(FULL, d.ds * 4096 + d.dc);
-            const int dc = ((packed + 2048) & 4095) - 2048;
-            const int ds = (packed - dc) >> 12;
-            int prim = ds;
-            if (GEN) {
-                if (obj_kind == 1) prim = __reduce_add_sync(FULL, d.dsq);
-                else if (obj_kind == 2) prim = __reduce_add_sync(FULL, d.dpar);
-            }
-            ++cand_evals;
-            bool better = !have;
-            if (!better) {
-                if (prim != bprim) better = prim < bprim;
-                else if (ds != bds) better = ds < bds;
-                else better = dc < bdc;
-            }
-            if (better) {
-                have = true; b0 = e0; b1 = e1; bds = ds; bdc = dc; bprim = prim;
+    for (int c = 0; c < count; ++c) {
+        const uint32_t e0 = __shfl_sync(gm, desc.x, c, GW);
+        const uint32_t e1 = __shfl_sync(gm, desc.y, c, GW);
+        if (!(e0 & 1u)) continue;
+        const Update u = decode(e0, e1, R.sW, n);
+        const Deltas d = eval_lane<OPL, GT, GEN, GW>(u, R.sW, R.sG, n, R.ld, lane);
+        const int packed = __reduce_add_sync(gm, d.ds * 4096 + d.dc);
+        const int dc = ((packed + 2048) & 4095) - 2048;
+        const int ds = (packed - dc) >> 12;
+        int prim = ds;
+        if (GEN) {
+            if (R.obj_kind == 1) prim = __reduce_add_sync(gm, d.dsq);
+            else if (R.obj_kind == 2) prim = __reduce_add_sync(gm, d.dpar);
+        }
+        ++ch.evals;
+        ch.evals2 += u.R2 >= 0;
+        bool better = ch.b0 == 0;
+        if (!better) {
+            if (prim != ch.bprim) better = prim < ch.bprim;
+            else if (ds != ch.bds) better = ds < ch.bds;
+            else better = dc < ch.bdc;
+        }
+        if (better) {
+            ch.b0 = e0; ch.b1 = e1; ch.bds = ds; ch.bdc = dc; ch.bprim = prim;
+        }
+    }
+    return ch;
+}
+
+// Phases F-H of an iteration whose choice is valid: Metropolis on the
+// replica's objective, the commit of an accepted move, best tracking
+// (the best W copied to the record on improvement, the job's solve flag),
+// cooling and reheat.  Returns whether the move was accepted.  The group's
+// lanes call it.
+template <int OPL, bool GEN, int GW>
+__device__ __forceinline__ bool apply_move(Replica<OPL, GW>& R, const Choice& ch, int tempering, int mpc, int stuck,
+                                           double t_min, double cooling, double reheat, int lane) {
+    constexpr int MW = Replica<OPL, GW>::MW;
+    using GT = typename Replica<OPL, GW>::GT;
+    ++R.moves;
+    // F: Metropolis
+    bool accept = ch.bprim <= 0;
+    if (!accept)
+        accept = ch.bprim <= (int64_t)kThrTable ? (uint64_t)ch.u < R.sThr[ch.bprim - 1]
+                                                : metropolis_accept(ch.bprim, R.T, ch.u);
+
+    // G: commit
+    if (accept) {
+        const Update u = decode(ch.b0, ch.b1, R.sW, R.n);
+        commit<OPL, MW, GT, GEN, GW>(ch.b0, ch.b1, u, ch.bds, R.sW, R.sG, R.sRes, R.sMino, R.sMask, R.n, R.ld,
+                                     R.m, R.sparse, lane);
+        R.score += ch.bds;
+        R.conflicts += ch.bdc;
+        R.obj_total += ch.bprim;
+        ++R.accepted;
+        R.accepted_rows += u.R2 >= 0 ? 2u : 1u;
+    }
+
+    // H: best tracking, cooling, reheat
+    if (R.score < R.best_s || (R.score == R.best_s && R.conflicts < R.best_c)) {
+        R.best_s = R.score;
+        R.best_c = R.conflicts;
+        R.msi = 0;
+        copy16<GW>(R.rec + R.J->off_best, R.sW, R.nn, lane);
+        if (R.best_s == 0 && lane == 0) {
+            RepHeader* H = R.H;
+            XwJob* J = R.J;
+            H->solve_it = R.it;
+            H->solve_ns = globaltimer();
+            if (atomicCAS(&J->solved, 0, 1) == 0) {
+                J->solved_replica = (int32_t)H->stream;
+                J->solved_it = R.it;
+                J->solve_ns = H->solve_ns;
             }
         }
-        if (!have) {
-            ++it;
-            continue;
+    } else {
+        ++R.msi;
+    }
+    if (!tempering) {
+        const double T0 = R.T;
+        if (++R.cool >= mpc) {
+            R.cool = 0;
+            R.T = __dmul_rn(R.T, cooling);
+            if (R.T < t_min) R.T = t_min;
         }
-        ++moves;
-
-        // F: Metropolis
-        bool accept = bprim <= 0;
-        if (!accept)
-            accept = bprim <= (int64_t)kThrTable ? (uint64_t)mblk.y < sThr[bprim - 1]
-                                                 : metropolis_accept(bprim, T, mblk.y);
-
-        // G: commit
-        if (accept) {
-            const Update u = decode(b0, b1, sW, n);
-            commit<OPL, MW, GT, GEN>(b0, b1, u, bds, sW, sG, sRes, sMino, sMask, n, ld, m, sparse, lane);
-            score += bds;
-            conflicts += bdc;
-            obj_total += bprim;
+        if (R.msi >= stuck) {
+            R.msi = 0;
+            R.T = __dmul_rn(R.reheat_T, reheat);
+            if (R.T < t_min) R.T = t_min;
         }
+        if (R.T != T0) build_thresholds<GW>(R.sThr, R.T, lane);
+    }
+    return accept;
+}
 
-        // H: best tracking, cooling, reheat
-        if (score < best_s || (score == best_s && conflicts < best_c)) {
-            best_s = score;
-            best_c = conflicts;
-            msi = 0;
-            copy16(rec + J->off_best, sW, nn, lane);
-            if (best_s == 0 && lane == 0) {
-                H->solve_it = it;
-                H->solve_ns = globaltimer();
-                if (atomicCAS(&J->solved, 0, 1) == 0) {
-                    J->solved_replica = (int32_t)H->stream;
-                    J->solved_it = it;
-                    J->solve_ns = H->solve_ns;
+template <int OPL, bool GEN, int GW = 32>
+__device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int lane, uint64_t chunk_iters) {
+    Replica<OPL, GW> R;
+    if (!load_replica<OPL, GEN, GW>(a, rid, slot, lane, chunk_iters, R)) return;
+    const SlotLayout L = slot_layout(R.n, R.m, OPL > 4);
+    Proposer<GW> P;
+    setup_proposer<OPL, GW>(R, reinterpret_cast<uint4*>(slot + L.off_draws),
+                            reinterpret_cast<View*>(slot + L.off_view), lane, P);
+    build_thresholds<GW>(R.sThr, R.T, lane);
+    const XwJob* J = R.J;
+    const int tempering = J->tempering;
+    const int mpc = J->moves_per_cool, stuck = J->stuck_threshold;
+    const double t_min = J->t_min, cooling = J->cooling, reheat = J->reheat;
+
+    uint64_t done = 0;
+#pragma unroll 1
+    for (; done < R.iters; ++done) {
+        // 1: every replica of the job stops soon after any solve;
+        // 2: a replica stops at its own solve only, so that each replica's
+        //    trajectory is independent of how the launches are scheduled
+        if (a.stop_on_solve) {
+            if (R.best_s == 0) break;
+            if (a.stop_on_solve == 1 && (done & 63) == 63 && *(volatile int32_t*)&J->solved) break;
+        }
+        const Choice ch = choose_move<OPL, GEN, GW>(R, P, R.it, lane);
+        R.cand_evals += ch.evals;
+        R.two_row_evals += ch.evals2;
+        if (ch.b0) apply_move<OPL, GEN, GW>(R, ch, tempering, mpc, stuck, t_min, cooling, reheat, lane);
+        ++R.it;
+    }
+    store_replica<OPL, GW>(R, lane);
+}
+
+// ---------------------------------------------------------------------------
+// Latency mode: one replica per CTA of K warps, speculating K iterations at
+// a time.  Warp k computes iteration it + k (phases A-E) against the
+// replica's current state, each with its own draw buffer: the draws of an
+// iteration depend only on its number, and its proposals and deltas only on
+// the state, which no iteration changes before one is accepted.  Warp 0
+// then takes the iterations in order through phases F-H until the first
+// accepted one, commits it, and discards the iterations after it, whose
+// proposals read the state it changed; the next round starts after the
+// accepted iteration.  The trajectory is the one-warp kernel's, move for
+// move; a round advances by the run of rejections up to the next accept
+// (about 2-4 iterations at the acceptance rates of cooling runs) in about
+// the time of one iteration, so a lone search runs that much faster.
+
+// Per-warp results and the round's control word, after the slot's own
+// (warp 0's) structures and the other warps' draw buffers and Views.
+struct SpecOut {
+    Choice ch;
+};
+struct SpecCtl {
+    uint64_t it;        // first iteration of the round
+    int32_t count;      // iterations of the round (0: the replica stops)
+    int32_t pad;
+};
+
+struct SpecLayout {
+    SlotLayout L;
+    uint32_t off_extra, per_warp, off_out, off_ctl, bytes;
+};
+
+// the latency-mode regions after a slot of `slot_bytes` (the one-warp
+// layout of the replica, or the largest of a launch's replicas)
+__host__ __device__ inline void spec_regions(uint32_t slot_bytes, int K, SpecLayout& S) {
+    S.per_warp = 32u * 16u + xw_pad16((uint32_t)sizeof(View));
+    S.off_extra = xw_pad16(slot_bytes);
+    S.off_out = S.off_extra + (uint32_t)(K - 1) * S.per_warp;
+    S.off_ctl = xw_pad16(S.off_out + (uint32_t)K * (uint32_t)sizeof(SpecOut));
+    S.bytes = S.off_ctl + (uint32_t)sizeof(SpecCtl);
+}
+
+__host__ __device__ inline SpecLayout spec_layout(int n, int m, int K) {
+    SpecLayout S;
+    S.L = slot_layout(n, m, false);
+    spec_regions(S.L.bytes, K, S);
+    return S;
+}
+
+template <bool GEN>
+__device__ void run_replica_spec(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int warp, int K, int lane) {
+    SpecCtl* ctl = nullptr;
+    Replica<1, 32> R;
+    bool ok = false;
+    // warp 0 loads the replica; the round size goes to the others through
+    // shared memory
+    if (warp == 0) ok = load_replica<1, GEN, 32>(a, rid, slot, lane, a.iters, R);
+    // every warp reads the order to find the layout
+    const XwJob* J = a.jobs + reinterpret_cast<const RepHeader*>(a.arena + a.rec_off[rid])->job;
+    const SpecLayout S = spec_layout(J->n, J->m, K);
+    ctl = reinterpret_cast<SpecCtl*>(slot + S.off_ctl);
+    SpecOut* outs = reinterpret_cast<SpecOut*>(slot + S.off_out);
+    const int tempering = J->tempering;
+    const int mpc = J->moves_per_cool, stuck = J->stuck_threshold;
+    const double t_min = J->t_min, cooling = J->cooling, reheat = J->reheat;
+    uint64_t done = 0;
+    if (warp == 0) {
+        if (ok) build_thresholds<32>(R.sThr, R.T, lane);
+        if (lane == 0) {
+            ctl->it = ok ? R.it : 0;
+            const bool stop = !ok || R.iters == 0 || (a.stop_on_solve && R.best_s == 0);
+            ctl->count = stop ? 0 : (int32_t)(R.iters < (uint64_t)K ? R.iters : (uint64_t)K);
+        }
+    }
+    __syncthreads();
+    if (ctl->count == 0) {
+        // nothing to run: the loaded replica's record still gets its
+        // rebuilt state, as the one-warp kernel writes it
+        if (warp == 0 && ok) store_replica<1, 32>(R, lane);
+        return;
+    }
+    // every warp: the replica's structures (read-only until warp 0 commits)
+    // and its own proposer
+    if (warp != 0) {
+        const SlotLayout& L = S.L;
+        R.J = const_cast<XwJob*>(J);
+        R.rec = a.arena + a.rec_off[rid];
+        R.H = reinterpret_cast<RepHeader*>(R.rec);
+        R.n = J->n; R.w = J->w; R.m = J->m; R.sparse = J->sparse; R.ld = L.ld;
+        R.obj_kind = GEN ? R.H->obj_kind : 0;
+        R.sW = reinterpret_cast<int8_t*>(slot);
+        R.sG = reinterpret_cast<int32_t*>(slot + L.off_g);
+        R.sRes = reinterpret_cast<int32_t*>(slot + L.off_res);
+        R.sMino = slot + L.off_mino;
+        R.sMask = reinterpret_cast<uint64_t*>(slot + L.off_mask);
+        R.sThr = reinterpret_cast<uint64_t*>(slot + L.off_thr);
+    }
+    uint8_t* mine = warp == 0 ? slot + S.L.off_draws : slot + S.off_extra + (uint32_t)(warp - 1) * S.per_warp;
+    View* view = warp == 0 ? reinterpret_cast<View*>(slot + S.L.off_view)
+                           : reinterpret_cast<View*>(mine + 32u * 16u);
+    Proposer<32> P;
+    setup_proposer<1, 32>(R, reinterpret_cast<uint4*>(mine), view, lane, P);
+
+#pragma unroll 1
+    for (;;) {
+        const uint64_t it0 = ctl->it;
+        const int cnt = ctl->count;
+        if (warp < cnt) {
+            const Choice ch = choose_move<1, GEN, 32>(R, P, it0 + (uint64_t)warp, lane);
+            if (lane == 0) outs[warp].ch = ch;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            // iterations in order until the first accepted move
+            int j = 0;
+            bool stop = false;
+#pragma unroll 1
+            for (; j < cnt; ++j) {
+                if (a.stop_on_solve == 1 && ((done + (uint64_t)j) & 63) == 63 &&
+                    *(volatile int32_t*)&R.J->solved) {
+                    stop = true;
+                    break;
+                }
+                const Choice ch = outs[j].ch;
+                R.cand_evals += ch.evals;
+                R.two_row_evals += ch.evals2;
+                if (!ch.b0) {
+                    ++R.it;
+                    continue;
+                }
+                const bool accept =
+                    apply_move<1, GEN, 32>(R, ch, tempering, mpc, stuck, t_min, cooling, reheat, lane);
+                ++R.it;
+                if (accept) {
+                    ++j;
+                    break;
                 }
             }
-        } else {
-            ++msi;
-        }
-        if (!tempering) {
-            const double T0 = T;
-            if (++cool >= mpc) {
-                cool = 0;
-                T = __dmul_rn(T, cooling);
-                if (T < t_min) T = t_min;
+            done += (uint64_t)j;
+            if (a.stop_on_solve && R.best_s == 0) stop = true;
+            if (lane == 0) {
+                ctl->it = R.it;
+                const uint64_t left = R.iters - done;
+                ctl->count = stop || left == 0 ? 0 : (int32_t)(left < (uint64_t)K ? left : (uint64_t)K);
             }
-            if (msi >= stuck) {
-                msi = 0;
-                T = __dmul_rn(reheat_T, reheat);
-                if (T < t_min) T = t_min;
-            }
-            if (T != T0) build_thresholds(sThr, T, lane);
         }
-        ++it;
+        __syncthreads();
+        if (ctl->count == 0) break;
     }
-
-    // ---- write back ----
-    __syncwarp();
-    copy16(rec + J->off_w, sW, nn, lane);
-    if (m > 0) copy16(rec + J->off_mino, sMino, (uint32_t)(n * m), lane);
-    if (lane == 0) {
-        H->it = it;
-        H->moves = moves;
-        H->cand_evals = cand_evals;
-        H->score = score;
-        H->conflicts = conflicts;
-        H->best_score = best_s;
-        H->best_conflicts = best_c;
-        H->obj_total = obj_total;
-        H->temperature = T;
-        H->msi = msi;
-        H->cool_ctr = cool;
-        H->status = status0 | XW_STATUS_INIT | (best_s == 0 ? XW_STATUS_SOLVED : 0u);
-    }
-    __syncwarp();
+    if (warp == 0) store_replica<1, 32>(R, lane);
 }
 
 // Register budget per thread; it sets how many replica warps an SM holds.
@@ -867,38 +1212,58 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
 #ifndef XW_ANNEAL_MAXNREG_LEAN1
 #define XW_ANNEAL_MAXNREG_LEAN1 96
 #endif
-constexpr int anneal_maxnreg(int opl, bool general) {
-    return opl == 1 && !general ? XW_ANNEAL_MAXNREG_LEAN1 : XW_ANNEAL_MAXNREG;
+#ifndef XW_ANNEAL_MAXNREG_PAIR
+#define XW_ANNEAL_MAXNREG_PAIR 96
+#endif
+constexpr int anneal_maxnreg(int opl, bool general, int gw) {
+    return gw == 16 ? XW_ANNEAL_MAXNREG_PAIR
+                    : opl == 1 && !general ? XW_ANNEAL_MAXNREG_LEAN1 : XW_ANNEAL_MAXNREG;
 }
-template <int OPL, bool GEN>
-__global__ void __maxnreg__(anneal_maxnreg(OPL, GEN)) anneal_kernel(AnnealArgs a) {
+// Each lane group (the warp, or each half of it) takes work items from the
+// launch's counter on its own: a replica (all of its launch iterations) or
+// one chunk of them.
+template <int OPL, bool GEN, int GW>
+__global__ void __maxnreg__(anneal_maxnreg(OPL, GEN, GW)) anneal_kernel(AnnealArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    uint8_t* slot = smem + (size_t)warp * a.slot_bytes;
+    const int lane = threadIdx.x & (GW - 1);
+    const int group = threadIdx.x / GW;
+    const unsigned gm = group_mask<GW>();
+    uint8_t* slot = smem + (size_t)group * a.slot_bytes;
     const uint64_t total = (uint64_t)a.n_items * a.chunks;
     for (;;) {
         uint32_t item = 0;
         if (lane == 0) item = atomicAdd(a.counter, 1u);
-        item = __shfl_sync(FULL, item, 0);
+        item = __shfl_sync(gm, item, 0, GW);
         if (item >= total) break;
         if (a.chunks == 1) {
-            run_replica<OPL, GEN>(a, a.items[item], slot, lane, a.iters);
+            run_replica<OPL, GEN, GW>(a, a.items[item], slot, lane, a.iters);
             continue;
         }
         const uint32_t c = item / a.n_items;
         const uint32_t rid = a.items[item - c * a.n_items];
         const uint64_t lo = a.iters * c / a.chunks, hi = a.iters * (c + 1) / a.chunks;
-        bool ok = true;
-        if (c > 0) ok = __all_sync(FULL, wait_chunk(a.chunk_done + rid, c));
-        __syncwarp();
-        if (ok) {
-            run_replica<OPL, GEN>(a, rid, slot, lane, hi - lo);
-        } else if (lane == 0) {
-            RepHeader* H = reinterpret_cast<RepHeader*>(a.arena + a.rec_off[rid]);
-            atomicOr(&H->err, XW_ERR_CHUNK);
-        }
-        release_chunk(a.chunk_done + rid, c + 1, lane);
+        RepHeader* H = reinterpret_cast<RepHeader*>(a.arena + a.rec_off[rid]);
+        run_chunk(
+            a.chunk_done + rid, c, a.chunk_wait_ns, &H->err, lane,
+            [&]() { run_replica<OPL, GEN, GW>(a, rid, slot, lane, hi - lo); }, gm);
+    }
+}
+
+// Latency mode: each CTA of K warps owns one replica at a time (orders up
+// to 32), taken from the launch's counter.
+template <bool GEN>
+__global__ void __launch_bounds__(512, 1) anneal_spec_kernel(AnnealArgs a, int K) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    __shared__ uint32_t s_item;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(a.counter, 1u);
+        __syncthreads();
+        const uint32_t item = s_item;
+        if (item >= a.n_items) break;
+        run_replica_spec<GEN>(a, a.items[item], smem, warp, K, lane);
+        __syncthreads();
     }
 }
 
@@ -966,7 +1331,7 @@ __global__ void collect_kernel(const XwJob* jobs, int njobs, const uint8_t* aren
     const XwJob& J = jobs[warp];
     int64_t bs = INT64_MAX, bc = INT64_MAX;
     int br = 0x7fffffff;
-    uint64_t moves = 0, evals = 0, iters = 0;
+    uint64_t moves = 0, evals = 0, iters = 0, acc = 0, acc_rows = 0, evals2 = 0;
     uint64_t fs_it = UINT64_MAX, fs_ns = 0;
     int fs = 0x7fffffff;
     uint32_t err = 0;
@@ -979,6 +1344,9 @@ __global__ void collect_kernel(const XwJob* jobs, int njobs, const uint8_t* aren
         }
         moves += H->moves;
         evals += H->cand_evals;
+        acc += H->accepted;
+        acc_rows += H->accepted_rows;
+        evals2 += H->two_row_evals;
         iters = iters > H->it ? iters : H->it;
         err |= H->err;
     }
@@ -988,6 +1356,9 @@ __global__ void collect_kernel(const XwJob* jobs, int njobs, const uint8_t* aren
         if (s2 < bs || (s2 == bs && (c2 < bc || (c2 == bc && r2 < br)))) { bs = s2; bc = c2; br = r2; }
         moves += __shfl_xor_sync(FULL, moves, off);
         evals += __shfl_xor_sync(FULL, evals, off);
+        acc += __shfl_xor_sync(FULL, acc, off);
+        acc_rows += __shfl_xor_sync(FULL, acc_rows, off);
+        evals2 += __shfl_xor_sync(FULL, evals2, off);
         const uint64_t i2 = __shfl_xor_sync(FULL, iters, off);
         iters = iters > i2 ? iters : i2;
         err |= __shfl_xor_sync(FULL, err, off);
@@ -1002,6 +1373,7 @@ __global__ void collect_kernel(const XwJob* jobs, int njobs, const uint8_t* aren
         o.solved = J.solved; o.err = (int32_t)err;
         o.first_solver = fs < J.replicas ? fs : -1;
         o.moves = moves; o.cand_evals = evals; o.iters = iters;
+        o.accepted = acc; o.accepted_rows = acc_rows; o.two_row_evals = evals2;
         o.solved_it = fs < J.replicas ? fs_it : 0;
         o.solve_ns = fs < J.replicas ? fs_ns : 0;
         out[warp] = o;
@@ -1026,25 +1398,49 @@ uint32_t anneal_slot_bytes(int n, int m, int opl) { return slot_layout(n, m, opl
 
 int anneal_opl(int n) { return n <= 32 ? 1 : n <= 64 ? 2 : n <= 128 ? 4 : 8; }
 
-const void* anneal_kernel_fn(int opl, bool general) {
-    if (general) {
-        if (opl == 1) return reinterpret_cast<const void*>(&anneal_kernel<1, true>);
-        if (opl == 2) return reinterpret_cast<const void*>(&anneal_kernel<2, true>);
-        if (opl == 4) return reinterpret_cast<const void*>(&anneal_kernel<4, true>);
-        return reinterpret_cast<const void*>(&anneal_kernel<8, true>);
+const void* anneal_kernel_fn(int opl, bool general, int rpw) {
+    if (rpw == 2) {
+        return general ? reinterpret_cast<const void*>(&anneal_kernel<1, true, 16>)
+                       : reinterpret_cast<const void*>(&anneal_kernel<1, false, 16>);
     }
-    if (opl == 1) return reinterpret_cast<const void*>(&anneal_kernel<1, false>);
-    if (opl == 2) return reinterpret_cast<const void*>(&anneal_kernel<2, false>);
-    if (opl == 4) return reinterpret_cast<const void*>(&anneal_kernel<4, false>);
-    return reinterpret_cast<const void*>(&anneal_kernel<8, false>);
+    if (general) {
+        if (opl == 1) return reinterpret_cast<const void*>(&anneal_kernel<1, true, 32>);
+        if (opl == 2) return reinterpret_cast<const void*>(&anneal_kernel<2, true, 32>);
+        if (opl == 4) return reinterpret_cast<const void*>(&anneal_kernel<4, true, 32>);
+        return reinterpret_cast<const void*>(&anneal_kernel<8, true, 32>);
+    }
+    if (opl == 1) return reinterpret_cast<const void*>(&anneal_kernel<1, false, 32>);
+    if (opl == 2) return reinterpret_cast<const void*>(&anneal_kernel<2, false, 32>);
+    if (opl == 4) return reinterpret_cast<const void*>(&anneal_kernel<4, false, 32>);
+    return reinterpret_cast<const void*>(&anneal_kernel<8, false, 32>);
 }
 
 cudaError_t launch_anneal(const AnnealArgs& args, int opl, bool general, int warps_per_block, int blocks,
-                          cudaStream_t stream) {
-    const size_t smem = (size_t)warps_per_block * args.slot_bytes;
+                          cudaStream_t stream, int rpw) {
+    if (rpw != 1 && (rpw != 2 || opl != 1)) return cudaErrorInvalidValue;
+    const size_t smem = (size_t)warps_per_block * rpw * args.slot_bytes;
     const dim3 grid(blocks), block(32 * warps_per_block);
     void* kargs[] = {const_cast<AnnealArgs*>(&args)};
-    return cudaLaunchKernel(anneal_kernel_fn(opl, general), grid, block, kargs, smem, stream);
+    return cudaLaunchKernel(anneal_kernel_fn(opl, general, rpw), grid, block, kargs, smem, stream);
+}
+
+uint32_t anneal_spec_cta_bytes(uint32_t slot_bytes, int K) {
+    SpecLayout S;
+    spec_regions(slot_bytes, K, S);
+    return S.bytes;
+}
+
+const void* anneal_spec_kernel_fn(bool general) {
+    return general ? reinterpret_cast<const void*>(&anneal_spec_kernel<true>)
+                   : reinterpret_cast<const void*>(&anneal_spec_kernel<false>);
+}
+
+cudaError_t launch_anneal_spec(const AnnealArgs& args, bool general, int K, int blocks, cudaStream_t stream) {
+    if (K < 2 || K > 16 || args.chunks != 1) return cudaErrorInvalidValue;
+    const dim3 grid(blocks), block(32 * K);
+    int k = K;
+    void* kargs[] = {const_cast<AnnealArgs*>(&args), &k};
+    return cudaLaunchKernel(anneal_spec_kernel_fn(general), grid, block, kargs, args.slot_bytes, stream);
 }
 
 cudaError_t launch_exchange(XwJob* jobs, int njobs, uint8_t* arena, const uint64_t* rec_off, const double* ladder,

@@ -641,6 +641,7 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
     int score, conflicts, best_s, best_c, msi, cool;
     int64_t obj_total;
     uint64_t moves, cand_evals;
+    uint32_t accepted = H->accepted, accepted_rows = H->accepted_rows, two_row_evals = H->two_row_evals;
     double T = H->temperature;
     const double reheat_T = H->reheat_temperature;
     bool at_best;  // W equals the best state and the best copy is pending
@@ -663,6 +664,7 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
         cool = 0;
         moves = 0;
         cand_evals = 0;
+        accepted = accepted_rows = two_row_evals = 0;
         at_best = true;
     }
     score = score0;
@@ -753,6 +755,7 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
                 else if (obj_kind == 2) prim = __reduce_add_sync(FULL, d.dpar);
             }
             ++cand_evals;
+            two_row_evals += u.R2 >= 0;
             bool better = !have;
             if (!better) {
                 if (prim != bprim) better = prim < bprim;
@@ -786,6 +789,8 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
             score += bds;
             conflicts += bdc;
             obj_total += bprim;
+            ++accepted;
+            accepted_rows += u.R2 >= 0 ? 2u : 1u;
         }
 
         if (score < best_s || (score == best_s && conflicts < best_c)) {
@@ -828,6 +833,9 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
         H->it = it;
         H->moves = moves;
         H->cand_evals = cand_evals;
+        H->accepted = accepted;
+        H->accepted_rows = accepted_rows;
+        H->two_row_evals = two_row_evals;
         H->score = score;
         H->conflicts = conflicts;
         H->best_score = best_s;
@@ -866,16 +874,9 @@ __global__ void __launch_bounds__(128, XW_LARGE_MIN_BLOCKS) anneal_large_kernel(
         const uint32_t c = item / a.n_items;
         const uint32_t rid = a.items[item - c * a.n_items];
         const uint64_t lo = a.iters * c / a.chunks, hi = a.iters * (c + 1) / a.chunks;
-        bool ok = true;
-        if (c > 0) ok = __all_sync(FULL, wait_chunk(a.chunk_done + rid, c));
-        __syncwarp();
-        if (ok) {
-            run_large<GEN>(a, rid, slot, lane, hi - lo);
-        } else if (lane == 0) {
-            RepHeader* H = reinterpret_cast<RepHeader*>(a.arena + a.rec_off[rid]);
-            atomicOr(&H->err, XW_ERR_CHUNK);
-        }
-        release_chunk(a.chunk_done + rid, c + 1, lane);
+        RepHeader* H = reinterpret_cast<RepHeader*>(a.arena + a.rec_off[rid]);
+        run_chunk(a.chunk_done + rid, c, a.chunk_wait_ns, &H->err, lane,
+                  [&]() { run_large<GEN>(a, rid, slot, lane, hi - lo); });
     }
 }
 

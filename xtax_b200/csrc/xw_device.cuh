@@ -119,32 +119,63 @@ __device__ __forceinline__ double acceptance_exp(double x) {
 // ends; how long it lasts is at most that chunk's own run time, which can be
 // long when the queue runs ahead of a slow replica (a mixed batch, or
 // replicas that finished early).  So the wait is bounded by elapsed device
-// time, kChunkWaitNs (%globaltimer), with an iteration cap behind it, and the
-// replica is flagged (XW_ERR_CHUNK) if it gives up.
+// time (%globaltimer; kChunkWaitNs unless the launch sets its own limit),
+// with an iteration cap behind it.  A chunk that gives up flags the replica
+// (XW_ERR_CHUNK), runs nothing, and publishes the count with kChunkPoison
+// set: the count is raised with an atomic maximum, so the predecessor that
+// is still running cannot clear the mark when it finishes, and every later
+// chunk of the replica sees it and skips too instead of running beside that
+// predecessor on the same record.
 constexpr uint64_t kChunkWaitNs = 30ull * 1000000000ull;
 constexpr uint32_t kChunkSpinLimit = 1u << 28;
+constexpr uint32_t kChunkPoison = 0x80000000u;
 
-static __device__ __noinline__ bool wait_chunk(const uint32_t* flag, uint32_t want) {
+// The replica's chunk count once it reaches `want` (kChunkPoison set when a
+// chunk before gave up), or 0 when the wait ran out.
+static __device__ __noinline__ uint32_t wait_chunk(const uint32_t* flag, uint32_t want, uint64_t limit_ns) {
     uint32_t v = 0;
     uint64_t t0, t;
+    if (limit_ns == 0) limit_ns = kChunkWaitNs;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
 #pragma unroll 1
     for (uint32_t spin = 0; spin < kChunkSpinLimit; ++spin) {
         asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
-        if (v >= want) return true;
+        if (v >= want) return v;
         __nanosleep(256);
         asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-        if (t - t0 > kChunkWaitNs) return false;
+        if (t - t0 > limit_ns) return 0;
     }
-    return false;
+    return 0;
 }
 
-// every lane's record writes are made visible device-wide before lane 0
-// publishes the chunk count
-__device__ __forceinline__ void release_chunk(uint32_t* flag, uint32_t value, int lane) {
+// Every lane's record writes are made visible device-wide before lane 0
+// publishes the chunk count (a release-ordered atomic maximum, so that a
+// poisoned count stays poisoned).  `gm`: the lanes that own the replica.
+__device__ __forceinline__ void release_chunk(uint32_t* flag, uint32_t value, int lane, unsigned gm = 0xffffffffu) {
     __threadfence();
-    __syncwarp();
-    if (lane == 0) asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(flag), "r"(value) : "memory");
+    __syncwarp(gm);
+    if (lane == 0) asm volatile("red.release.gpu.global.max.u32 [%0], %1;" ::"l"(flag), "r"(value) : "memory");
+}
+
+// One chunk of a chunked launch: wait for the replica's previous chunk, run
+// `body` when it finished normally, flag the replica and skip otherwise, and
+// publish this chunk's count.  Every lane of the replica's lane group `gm`
+// calls it.
+template <typename Body>
+__device__ __forceinline__ void run_chunk(uint32_t* done, uint32_t c, uint64_t limit_ns, uint32_t* err, int lane,
+                                          Body body, unsigned gm = 0xffffffffu) {
+    bool ok = true;
+    if (c > 0) {
+        const uint32_t seen = wait_chunk(done, c, limit_ns);
+        ok = __all_sync(gm, seen != 0 && !(seen & kChunkPoison));
+    }
+    __syncwarp(gm);
+    if (ok) {
+        body();
+    } else if (lane == 0) {
+        atomicOr(err, XW_ERR_CHUNK);
+    }
+    release_chunk(done, ok ? c + 1 : (kChunkPoison | (c + 1)), lane, gm);
 }
 
 // Metropolis test u*2^-32 < exp(-delta/T), delta > 0.

@@ -116,6 +116,20 @@ void check_cuda(cudaError_t e, const char* what) { check(e, what); }
 static_assert(XW_MAX_ORDER_CUDA == XW_MAX_ORDER_LARGE, "public and device order limits agree");
 static_assert(XW_MAX_ORDER_SHARED == XW_MAX_N, "public and shared-memory order limits agree");
 
+uint64_t chunk_wait_limit_ns() {
+    const char* e = std::getenv("XW_CHUNK_WAIT_NS");
+    if (!e || !*e) return 0;
+    return std::strtoull(e, nullptr, 10);
+}
+
+void raise_smem_limit(const void* fn, int device) {
+    int optin = 0;
+    check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device),
+          "cudaDeviceGetAttribute max opt-in shared memory");
+    check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin),
+          "cudaFuncSetAttribute max dynamic shared memory");
+}
+
 int large_min_order() {
     const char* e = std::getenv("XW_LARGE_MIN_ORDER");
     if (!e || !*e) return XW_MAX_N + 1;
@@ -161,6 +175,9 @@ std::string validate(int n, int w, const xw_params& p) {
     if (p.move_set < 0 || p.move_set > 1) return "CUDA move set must be 0 or 1";
     if (p.start_kind < 0 || p.start_kind > 1) return "CUDA start kind must be 0 or 1";
     if (p.warps_per_block < 0 || p.warps_per_block > 16) return "CUDA warps per block must be in [0, 16]";
+    if (p.replicas_per_warp < 0 || p.replicas_per_warp > 2) return "CUDA replicas per warp must be 0, 1 or 2";
+    if (p.warps_per_replica < 0 || p.warps_per_replica > 16) return "CUDA warps per replica must be in [0, 16]";
+    if (p.restart_kicks < 0 || p.restart_kicks > 1) return "CUDA restart kicks must be 0 (host) or 1 (device)";
     if (p.stop_on_solve < 0 || p.stop_on_solve > 2) return "CUDA stop-on-solve mode must be 0, 1 or 2";
     return {};
 }
@@ -199,11 +216,13 @@ void Batch::dalloc(void** ptr, size_t bytes, const char* what) {
 Batch::~Batch() {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     for (auto e : events) cudaEventDestroy(e);
+    for (auto e : side_events) cudaEventDestroy(e);
     if (stream) cudaStreamSynchronize(stream);
     for (void* ptr : {d_jobs, d_jobs0, d_arena, d_arena0, d_rec_off, d_items, d_counters, d_ladder,
                       d_out, d_best_off, d_best, d_t0, d_gram, d_gram_off, d_chunk_done})
         if (ptr) cudaFreeAsync(ptr, stream);
     if (stream) cudaStreamSynchronize(stream);
+    for (auto st : side_streams) cudaStreamDestroy(st);
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
@@ -374,16 +393,13 @@ void Batch::build(const xw_job_spec* specs, int njobs, const xw_params& p, const
     upload(host);
 }
 
-// Work list, result offsets, launch class and shared-memory slot from the
-// job table.
+// Work list, result offsets, launch classes and shared-memory slots from
+// the job table.
 void Batch::derive_layout() {
     const int njobs = (int)jobs.size();
     total_replicas = 0;
     best_offsets.assign(njobs, 0);
     size_t best_off = 0;
-    opl = 1;
-    general = false;
-    slot_bytes = 0;
     n_large = 0;
     general_large = false;
     large_slot_bytes = 0;
@@ -396,18 +412,12 @@ void Batch::derive_layout() {
             n_large += (uint32_t)J.replicas;
             general_large = general_large || J.general != 0;
             large_slot_bytes = std::max(large_slot_bytes, anneal_large_slot_bytes(J.n));
-        } else {
-            opl = std::max(opl, anneal_opl(J.n));
-            general = general || J.general != 0;
         }
     }
-    // one launch runs every shared-memory replica with the widest class's
-    // kernel and layout, another every HBM-resident one
-    for (int j = 0; j < njobs; ++j)
-        if (!jobs[j].large) slot_bytes = std::max(slot_bytes, anneal_slot_bytes(jobs[j].n, jobs[j].m, opl));
     best_bytes = best_off;
     // work items: the HBM-resident replicas, then the others; longest
-    // replicas first within each (cost grows with n)
+    // replicas first within each (cost grows with n), so that each launch
+    // class is one range of items
     items.resize(total_replicas);
     std::vector<int> job_of(total_replicas);
     for (int j = 0; j < njobs; ++j)
@@ -418,6 +428,25 @@ void Batch::derive_layout() {
         if (A.large != B.large) return A.large > B.large;
         return A.n > B.n;
     });
+    // launch classes over the shared-memory items
+    classes.clear();
+    for (uint32_t i = n_large; i < total_replicas; ++i) {
+        const XwJob& J = jobs[job_of[items[i]]];
+        const int kind = tune_kind(J.n, J.candidate_samples);
+        if (classes.empty() || classes.back().kind != kind) {
+            LaunchClass c;
+            c.kind = kind;
+            c.opl = anneal_opl(J.n);
+            c.min_n = c.max_n = J.n;
+            c.item_begin = i;
+            classes.push_back(c);
+        }
+        LaunchClass& c = classes.back();
+        c.item_count += 1;
+        c.min_n = std::min(c.min_n, J.n);
+        c.general = c.general || J.general != 0;
+        c.slot_bytes = std::max(c.slot_bytes, anneal_slot_bytes(J.n, J.m, c.opl));
+    }
     // Gram arena offsets of the HBM-resident replicas
     gram_off.assign(total_replicas, 0);
     gram_bytes = 0;
@@ -484,7 +513,19 @@ void Batch::upload(const std::vector<uint8_t>& host) {
           "upload result offsets");
     reset();
     check(cudaStreamSynchronize(stream), "cudaStreamSynchronize upload");
-    configure_shape(params.warps_per_block);
+    // streams and fork/join events for side-by-side launches of a round
+    const int launches = launches_per_round();
+    while ((int)side_streams.size() < launches - 1) {
+        cudaStream_t st;
+        check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
+        side_streams.push_back(st);
+    }
+    while ((int)side_events.size() < (launches > 1 ? launches + 1 : 0)) {
+        cudaEvent_t e;
+        check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+        side_events.push_back(e);
+    }
+    configure_shape();
 }
 
 // Population snapshots (the format is described with Snapshot): a batch
@@ -600,6 +641,8 @@ void Batch::load(const std::string& path, const xw_params* over) {
         params.moves_per_launch = over->moves_per_launch;
         params.stop_on_solve = over->stop_on_solve;
         params.warps_per_block = over->warps_per_block;
+        params.replicas_per_warp = over->replicas_per_warp;
+        params.warps_per_replica = over->warps_per_replica;
         params.max_seconds = over->max_seconds;
     }
     tempering = params.tempering != 0;
@@ -625,7 +668,7 @@ uint32_t choose_chunks(uint32_t replicas, uint32_t slots) {
     return best;
 }
 
-void Batch::configure_shape(int wpb) {
+void Batch::configure_shape() {
     if (graph_exec) {
         cudaGraphExecDestroy(graph_exec);
         graph_exec = nullptr;
@@ -634,8 +677,7 @@ void Batch::configure_shape(int wpb) {
         // four warps per CTA, as many CTAs as the SMs hold
         const void* lfn = anneal_large_kernel_fn(general_large);
         const size_t lsmem = (size_t)large_wpb * large_slot_bytes;
-        check(cudaFuncSetAttribute(lfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem),
-              "cudaFuncSetAttribute max dynamic shared memory");
+        raise_smem_limit(lfn, params.device);
         int per_sm = 0;
         check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lfn, 32 * large_wpb, lsmem),
               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
@@ -643,39 +685,96 @@ void Batch::configure_shape(int wpb) {
         const int want = (int)((n_large + large_wpb - 1) / large_wpb);
         large_blocks = std::max(1, std::min(want, per_sm * props.multiProcessorCount));
         large_chunks = choose_chunks(n_large, (uint32_t)(large_blocks * large_wpb));
-        if (large_chunks > 1 && !d_chunk_done)
-            dalloc(&d_chunk_done, sizeof(uint32_t) * std::max<uint32_t>(total_replicas, 1), "cudaMalloc chunk counters");
     }
-    if (n_large == total_replicas) return;
-    const void* fn = anneal_kernel_fn(opl, general);
     int optin = 0;
     check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, params.device),
           "cudaDeviceGetAttribute max opt-in shared memory");
-    if (slot_bytes > (uint32_t)optin)
-        throw std::length_error(fmt("CUDA replica requires %.2f KiB of shared memory, but device %d permits "
-                                    "%.2f KiB per opt-in block",
-                                    slot_bytes / 1024.0, params.device, optin / 1024.0));
-    if (wpb <= 0) wpb = tuned_warps_per_block(opl, slot_bytes, params.device);
-    wpb = std::max(1, std::min(wpb, std::min(16, (int)(optin / slot_bytes))));
-    const size_t smem = (size_t)wpb * slot_bytes;
-    check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-          "cudaFuncSetAttribute max dynamic shared memory");
+    for (size_t k = 0; k < classes.size(); ++k) {
+        const LaunchClass& c = classes[k];
+        if (c.slot_bytes > (uint32_t)optin)
+            throw std::length_error(fmt("CUDA replica requires %.2f KiB of shared memory, but device %d permits "
+                                        "%.2f KiB per opt-in block",
+                                        c.slot_bytes / 1024.0, params.device, optin / 1024.0));
+        // the latency mode: orders up to 32, and (unless set) classes of at
+        // most one replica per SM, where a replica's speed is its latency
+        if (c.max_n <= 32) {
+            int wpr = params.warps_per_replica;
+            if (wpr == 0 && c.item_count <= (uint32_t)props.multiProcessorCount)
+                wpr = tuned_warps_per_replica(c.slot_bytes, params.device);
+            if (wpr > 1 && configure_latency(k, wpr)) continue;
+        }
+        TunedShape t = tuned_shape(c.kind, c.slot_bytes, params.device);
+        if (params.warps_per_block > 0) t.wpb = params.warps_per_block;
+        if (params.replicas_per_warp > 0) t.rpw = params.replicas_per_warp;
+        if (c.kind != kTunePairKind) t.rpw = 1;
+        // the widest shape that fits the opt-in shared memory
+        t.wpb = std::max(1, std::min(t.wpb, std::min(16, (int)(optin / (c.slot_bytes * (uint32_t)t.rpw)))));
+        if (!configure_class(k, t.wpb, t.rpw) && !configure_class(k, 1, 1))
+            throw std::length_error("CUDA anneal kernel has zero occupancy on the selected device");
+    }
+    uint32_t most_chunks = n_large ? large_chunks : 1;
+    for (const LaunchClass& c : classes) most_chunks = std::max(most_chunks, c.chunks);
+    if (most_chunks > 1 && !d_chunk_done)
+        dalloc(&d_chunk_done, sizeof(uint32_t) * std::max<uint32_t>(total_replicas, 1), "cudaMalloc chunk counters");
+}
+
+bool Batch::configure_latency(size_t k, int wpr) {
+    if (graph_exec) {
+        cudaGraphExecDestroy(graph_exec);
+        graph_exec = nullptr;
+    }
+    LaunchClass& c = classes.at(k);
+    if (c.max_n > 32 || wpr < 2 || wpr > 16) return false;
+    const void* fn = anneal_spec_kernel_fn(c.general);
+    raise_smem_limit(fn, params.device);
+    const uint32_t bytes = anneal_spec_cta_bytes(c.slot_bytes, wpr);
     int per_sm = 0;
-    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * wpb, smem),
-          "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-    if (per_sm < 1) throw std::length_error("CUDA anneal kernel has zero occupancy on the selected device");
-    warps_per_block = wpb;
-    blocks_per_sm = per_sm;
-    const uint32_t small = total_replicas - n_large;
-    const int want = (int)((small + wpb - 1) / wpb);
-    blocks = std::max(1, std::min(want, per_sm * props.multiProcessorCount));
-    // More replicas than resident warps: a launch of whole replicas ends in a
-    // part-filled wave (4096 replicas on 2368 warps run 2 waves for 1.73
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * wpr, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if (per_sm < 1) return false;
+    c.wpr = wpr;
+    c.spec_bytes = bytes;
+    c.rpw = 1;
+    c.wpb = wpr;
+    c.blocks_per_sm = per_sm;
+    c.blocks = std::max(1, std::min((int)c.item_count, per_sm * props.multiProcessorCount));
+    c.chunks = 1;
+    return true;
+}
+
+bool Batch::configure_class(size_t k, int wpb, int rpw) {
+    if (graph_exec) {
+        cudaGraphExecDestroy(graph_exec);
+        graph_exec = nullptr;
+    }
+    LaunchClass& c = classes.at(k);
+    if (rpw == 2 && c.kind != kTunePairKind) return false;
+    c.wpr = 1;
+    const void* fn = anneal_kernel_fn(c.opl, c.general, rpw);
+    raise_smem_limit(fn, params.device);
+    const size_t smem = (size_t)wpb * rpw * c.slot_bytes;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * wpb, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if (per_sm < 1) return false;
+    c.wpb = wpb;
+    c.rpw = rpw;
+    c.blocks_per_sm = per_sm;
+    const uint32_t groups = (uint32_t)(wpb * rpw);
+    const int want = (int)((c.item_count + groups - 1) / groups);
+    c.blocks = std::max(1, std::min(want, per_sm * props.multiProcessorCount));
+    // More replicas than resident groups: a launch of whole replicas ends in
+    // a part-filled wave (4096 replicas on 2368 warps run 2 waves for 1.73
     // waves of work).  Split each replica's iterations into k chunks, k in
     // [1, 8] with the fewest waves per unit of work, the least k on ties.
-    chunks = choose_chunks(small, (uint32_t)(blocks * wpb));
-    if ((chunks > 1 || large_chunks > 1) && !d_chunk_done)
+    c.chunks = choose_chunks(c.item_count, (uint32_t)c.blocks * groups);
+    if (c.chunks > 1 && !d_chunk_done)
         dalloc(&d_chunk_done, sizeof(uint32_t) * std::max<uint32_t>(total_replicas, 1), "cudaMalloc chunk counters");
+    return true;
 }
 
 void Batch::reset() {
@@ -697,23 +796,28 @@ void Batch::reserve_rounds(int rounds) {
         check(cudaEventCreate(&e), "cudaEventCreate");
         events.push_back(e);
     }
-    if (counters_cap < rounds) {
+    if (counters_cap < rounds || counters_per_round != launches_per_round()) {
         if (d_counters) check(cudaFreeAsync(d_counters, stream), "cudaFreeAsync counters");
         d_counters = nullptr;
-        // one counter per round for each of the two kernels
-        dalloc(&d_counters, sizeof(uint32_t) * 2 * rounds, "cudaMalloc counters");
+        // one counter per round for each launch of the round
+        dalloc(&d_counters, sizeof(uint32_t) * (size_t)launches_per_round() * rounds, "cudaMalloc counters");
         check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
         counters_cap = rounds;
+        counters_per_round = launches_per_round();
     }
 }
 
 void Batch::enqueue_rounds(uint64_t iters, bool timed) {
     const uint64_t per = round_iters();
     const int rounds = (int)((iters + per - 1) / per);
-    if ((int)events.size() < 2 * rounds || counters_cap < rounds)
+    const int launches = launches_per_round();
+    if ((int)events.size() < 2 * rounds || counters_cap < rounds || counters_per_round != launches)
         throw std::logic_error("round resources not reserved");
+    uint32_t most_chunks = n_large ? large_chunks : 1;
+    for (const LaunchClass& c : classes) most_chunks = std::max(most_chunks, c.chunks);
     check(launch_mark_t0(static_cast<uint64_t*>(d_t0), stream), "launch mark_t0");
-    check(cudaMemsetAsync(d_counters, 0, sizeof(uint32_t) * 2 * rounds, stream), "cudaMemsetAsync counters");
+    check(cudaMemsetAsync(d_counters, 0, sizeof(uint32_t) * (size_t)launches * rounds, stream),
+          "cudaMemsetAsync counters");
     uint64_t left = iters;
     for (int k = 0; k < rounds; ++k) {
         AnnealArgs a;
@@ -723,38 +827,66 @@ void Batch::enqueue_rounds(uint64_t iters, bool timed) {
         a.iters = std::min(left, per);
         a.stop_on_solve = params.stop_on_solve;
         a.pad = 0;
+        a.chunk_wait_ns = chunk_wait_limit_ns();
         left -= a.iters;
+        uint32_t* counters = static_cast<uint32_t*>(d_counters) + (size_t)launches * k;
         if (timed) check(cudaEventRecord(events[2 * k], stream), "cudaEventRecord");
+        // one chunk-counter reset for all of the round's launches (their
+        // replicas are disjoint), before they fork
+        if (a.iters >= 2 && most_chunks > 1)
+            check(cudaMemsetAsync(d_chunk_done, 0, sizeof(uint32_t) * total_replicas, stream),
+                  "cudaMemsetAsync chunk counters");
+        // launch l runs on the batch's stream when it is alone, else on side
+        // stream l, forked from and joined back into the batch's stream
+        if (launches > 1) check(cudaEventRecord(side_events[0], stream), "cudaEventRecord");
+        int l = 0;
+        auto on = [&](int idx) {
+            if (launches == 1) return stream;
+            cudaStream_t st = idx == 0 ? stream : side_streams[idx - 1];
+            if (idx > 0) check(cudaStreamWaitEvent(st, side_events[0], 0), "cudaStreamWaitEvent");
+            return st;
+        };
+        auto join = [&](int idx, cudaStream_t st) {
+            if (launches == 1 || idx == 0) return;
+            check(cudaEventRecord(side_events[idx], st), "cudaEventRecord");
+        };
         if (n_large) {
-            AnnealArgs l = a;
-            l.items = static_cast<const uint32_t*>(d_items);
-            l.n_items = n_large;
-            l.slot_bytes = large_slot_bytes;
-            l.counter = static_cast<uint32_t*>(d_counters) + 2 * k + 1;
-            l.gram = static_cast<uint8_t*>(d_gram);
-            l.gram_off = static_cast<const uint64_t*>(d_gram_off);
-            l.chunks = l.iters >= large_chunks ? large_chunks : 1;
-            if (l.chunks > 1) {
-                l.chunk_done = static_cast<uint32_t*>(d_chunk_done);
-                check(cudaMemsetAsync(d_chunk_done, 0, sizeof(uint32_t) * total_replicas, stream),
-                      "cudaMemsetAsync chunk counters");
-            }
-            check(launch_anneal_large(l, general_large, large_wpb, large_blocks, stream),
-                  "launch anneal_large_kernel");
+            AnnealArgs la = a;
+            la.items = static_cast<const uint32_t*>(d_items);
+            la.n_items = n_large;
+            la.slot_bytes = large_slot_bytes;
+            la.counter = counters + l;
+            la.gram = static_cast<uint8_t*>(d_gram);
+            la.gram_off = static_cast<const uint64_t*>(d_gram_off);
+            la.chunks = la.iters >= large_chunks ? large_chunks : 1;
+            if (la.chunks > 1) la.chunk_done = static_cast<uint32_t*>(d_chunk_done);
+            cudaStream_t st = on(l);
+            check(launch_anneal_large(la, general_large, large_wpb, large_blocks, st), "launch anneal_large_kernel");
+            join(l, st);
+            ++l;
         }
-        if (n_large < total_replicas) {
-            a.items = static_cast<const uint32_t*>(d_items) + n_large;
-            a.n_items = total_replicas - n_large;
-            a.slot_bytes = slot_bytes;
-            a.counter = static_cast<uint32_t*>(d_counters) + 2 * k;
-            a.chunks = a.iters >= chunks ? chunks : 1;
-            if (a.chunks > 1) {
-                a.chunk_done = static_cast<uint32_t*>(d_chunk_done);
-                check(cudaMemsetAsync(d_chunk_done, 0, sizeof(uint32_t) * total_replicas, stream),
-                      "cudaMemsetAsync chunk counters");
+        for (const LaunchClass& c : classes) {
+            AnnealArgs ca = a;
+            ca.items = static_cast<const uint32_t*>(d_items) + c.item_begin;
+            ca.n_items = c.item_count;
+            ca.slot_bytes = c.slot_bytes;
+            ca.counter = counters + l;
+            ca.chunks = ca.iters >= c.chunks ? c.chunks : 1;
+            if (ca.chunks > 1) ca.chunk_done = static_cast<uint32_t*>(d_chunk_done);
+            cudaStream_t st = on(l);
+            if (c.wpr > 1) {
+                ca.slot_bytes = c.spec_bytes;
+                ca.chunks = 1;
+                ca.chunk_done = nullptr;
+                check(launch_anneal_spec(ca, c.general, c.wpr, c.blocks, st), "launch anneal_spec_kernel");
+            } else {
+                check(launch_anneal(ca, c.opl, c.general, c.wpb, c.blocks, st, c.rpw), "launch anneal_kernel");
             }
-            check(launch_anneal(a, opl, general, warps_per_block, blocks, stream), "launch anneal_kernel");
+            join(l, st);
+            ++l;
         }
+        for (int idx = 1; idx < launches; ++idx)
+            check(cudaStreamWaitEvent(stream, side_events[idx], 0), "cudaStreamWaitEvent");
         if (timed) check(cudaEventRecord(events[2 * k + 1], stream), "cudaEventRecord");
         if (tempering)
             check(launch_exchange(static_cast<XwJob*>(d_jobs), (int)jobs.size(), static_cast<uint8_t*>(d_arena),
@@ -813,6 +945,25 @@ void Batch::collect(std::vector<JobOut>& out, int8_t* best_host, bool want_best)
               "cudaMemcpy best states to host");
     check(cudaMemcpyAsync(&t0_host, d_t0, sizeof(uint64_t), cudaMemcpyDeviceToHost, stream), "cudaMemcpy clock");
     check(cudaStreamSynchronize(stream), "cudaStreamSynchronize results");
+    vstats.assign(jobs.size(), VerifyStats{});
+    vstats_valid.assign(jobs.size(), 0);
+    if (want_best) {
+        // every job's best W (orders up to 256) rescored and checked exactly
+        // on the device, in one batch
+        std::vector<VerifyItem> items;
+        std::vector<size_t> of;
+        for (size_t j = 0; j < jobs.size(); ++j) {
+            if (jobs[j].n > XW_MAX_ORDER_SHARED) continue;
+            items.push_back({static_cast<const int8_t*>(d_best) + best_offsets[j], jobs[j].n, jobs[j].w});
+            of.push_back(j);
+        }
+        std::vector<VerifyStats> vs;
+        verifier.run(items, stream, vs);
+        for (size_t k = 0; k < of.size(); ++k) {
+            vstats[of[k]] = vs[k];
+            vstats_valid[of[k]] = 1;
+        }
+    }
 }
 
 void Batch::fill_results(const std::vector<JobOut>& out, const int8_t* best_host, xw_job_result* res) const {
@@ -827,16 +978,25 @@ void Batch::fill_results(const std::vector<JobOut>& out, const int8_t* best_host
         r.error = o.err;
         r.moves = o.moves;
         r.candidate_evaluations = o.cand_evals;
+        r.accepted_moves = o.accepted;
+        r.accepted_rows = o.accepted_rows;
+        r.two_row_evaluations = o.two_row_evals;
         r.iterations = o.iters;
         r.solved_iteration = o.solved_it;
         r.time_to_solution_seconds = (o.solved && o.solve_ns >= t0_host) ? (o.solve_ns - t0_host) * 1e-9 : -1.0;
         if (best_host && r.solved) {
             const int n = jobs[j].n;
-            std::vector<int8_t> e(best_host + best_offsets[j], best_host + best_offsets[j] + (size_t)n * n);
-            try {
-                r.verified = CpuState::from_entries(n, jobs[j].w, e).verify_weighing() ? 1 : 0;
-            } catch (const std::exception&) {
-                r.verified = 0;
+            if (j < vstats_valid.size() && vstats_valid[j]) {
+                // the device check of this best W (collect)
+                r.verified = vstats[j].exact == 1 && vstats[j].score == 0 ? 1 : 0;
+            } else {
+                // orders above 256: the int64 check on the host
+                std::vector<int8_t> e(best_host + best_offsets[j], best_host + best_offsets[j] + (size_t)n * n);
+                try {
+                    r.verified = CpuState::from_entries(n, jobs[j].w, e).verify_weighing() ? 1 : 0;
+                } catch (const std::exception&) {
+                    r.verified = 0;
+                }
             }
         }
     }
@@ -888,9 +1048,9 @@ int restart_population(Batch& b, int j, const std::vector<int8_t>& elite_best, i
     // (W(256,128), 0.3 s); above them, with weights near n/2, it grows as
     // n^5 (W(300,150) ~3e11, W(1024,512) ~5e14).  Past kEscapeScanBudget
     // the restart kicks without an escape move rather than stall the run.
-    std::vector<EscapeMove> escapes;
-    if (escape_scan_work(n, elite_best) <= kEscapeScanBudget)
-        escapes = escape_moves_from(elite, escape_scan(n, elite_best.data(), eg.data(), limit));
+    std::vector<ScanResult> scan;
+    if (escape_scan_work(n, elite_best) <= kEscapeScanBudget) scan = escape_scan(n, elite_best.data(), eg.data(), limit);
+    const std::vector<EscapeMove> escapes = escape_moves_from(elite, scan);
     std::vector<int> selected;
     size_t scanned = 0;
     while ((int)selected.size() < count && scanned < (size_t)R * 2) {
@@ -900,6 +1060,64 @@ int restart_population(Batch& b, int j, const std::vector<int8_t>& elite_best, i
         selected.push_back(r);
     }
     rs.cursor = (rs.cursor + scanned) % (size_t)R;
+    auto kick_of = [&](size_t idx) {
+        return selected.size() > 1 ? p.restart_kick_min + (int)(idx * (size_t)(p.restart_kick_max - p.restart_kick_min) /
+                                                                (selected.size() - 1))
+                                   : p.restart_kick_min;
+    };
+    auto done_line = [&]() {
+        ++rs.round;
+        rs.restarted += selected.size();
+        line = fmt("[restart] seconds=%g elite_score=%lld replicas=%zu kicks=%d..%d min_escape_delta=%lld", elapsed,
+                   (long long)gbest, selected.size(), p.restart_kick_min, p.restart_kick_max,
+                   (long long)(escapes.empty() ? 0 : escapes.front().score_delta));
+        return (int)selected.size();
+    };
+
+    if (p.restart_kicks == 1) {
+        // device kicks: the records are rewritten in place by one CTA per
+        // restarted replica (xw_restart.cu); only the job's small tables
+        // cross to the device, no record comes back
+        const size_t pool = std::min(scan.size(), std::max<size_t>(selected.size() * 4, 1));
+        std::vector<int32_t> esc;
+        for (size_t k = 0; k < pool; ++k) {
+            const ScanResult& x = scan[k];
+            esc.insert(esc.end(), {x.row1, x.row2, x.col1, x.col2, x.new1, x.new2});
+        }
+        std::vector<KickJob> kicks(selected.size());
+        for (size_t idx = 0; idx < selected.size(); ++idx) {
+            kicks[idx].rid = J.rep_begin + (uint32_t)selected[idx];
+            kicks[idx].index = (uint32_t)idx;
+            kicks[idx].kick = kick_of(idx);
+            kicks[idx].esc = pool ? (int32_t)((idx + (size_t)rs.round * selected.size()) % pool) : -1;
+        }
+        void *d_kicks = nullptr, *d_esc = nullptr, *d_scratch = nullptr;
+        b.dalloc(&d_kicks, sizeof(KickJob) * kicks.size(), "cudaMalloc kicks");
+        b.dalloc(&d_esc, sizeof(int32_t) * std::max<size_t>(esc.size(), 1), "cudaMalloc escape moves");
+        b.dalloc(&d_scratch, sizeof(uint16_t) * XW_MAX_ORDER_LARGE * kicks.size(), "cudaMalloc kick scratch");
+        check(cudaMemcpyAsync(d_kicks, kicks.data(), sizeof(KickJob) * kicks.size(), cudaMemcpyHostToDevice, b.stream),
+              "upload kicks");
+        if (!esc.empty())
+            check(cudaMemcpyAsync(d_esc, esc.data(), sizeof(int32_t) * esc.size(), cudaMemcpyHostToDevice, b.stream),
+                  "upload escape moves");
+        KickArgs ka;
+        ka.job = static_cast<const XwJob*>(b.d_jobs) + j;
+        ka.arena = static_cast<uint8_t*>(b.d_arena);
+        ka.rec_off = static_cast<const uint64_t*>(b.d_rec_off);
+        ka.elite = static_cast<const int8_t*>(b.d_best) + b.best_offsets[j];
+        ka.escapes = static_cast<const int32_t*>(d_esc);
+        ka.kicks = static_cast<const KickJob*>(d_kicks);
+        ka.scratch = static_cast<uint16_t*>(d_scratch);
+        ka.round = rs.round;
+        ka.gbest = (int32_t)gbest;
+        ka.gconf = (int32_t)gconf;
+        ka.t_min = p.t_min;
+        ka.reheat = p.reheat;
+        launch_kicks(ka, (int)kicks.size(), b.stream);
+        for (void* ptr : {d_kicks, d_esc, d_scratch}) check(cudaFreeAsync(ptr, b.stream), "cudaFreeAsync");
+        check(cudaStreamSynchronize(b.stream), "cudaStreamSynchronize kicks");
+        return done_line();
+    }
 
     const size_t rb = J.record_bytes, base = b.rec_off[J.rep_begin];
     std::vector<uint8_t> host((size_t)R * rb);
@@ -914,10 +1132,7 @@ int restart_population(Batch& b, int j, const std::vector<int8_t>& elite_best, i
     const uint32_t base_seed = (uint32_t)p.seed;
     parallel_for((int)selected.size(), [&](int idx) {
         const int r = selected[(size_t)idx];
-        const int kick = selected.size() > 1
-            ? p.restart_kick_min + (int)((size_t)idx * (size_t)(p.restart_kick_max - p.restart_kick_min) /
-                                         (selected.size() - 1))
-            : p.restart_kick_min;
+        const int kick = kick_of((size_t)idx);
         const CpuState k = kick_elite(elite, escapes, (size_t)idx, selected.size(), rs.round, r, base_seed, kick, cp);
         uint8_t* rec = host.data() + (size_t)r * rb;
         RepHeader* H = reinterpret_cast<RepHeader*>(rec);
@@ -943,12 +1158,7 @@ int restart_population(Batch& b, int j, const std::vector<int8_t>& elite_best, i
     });
     check(cudaMemcpyAsync(dev, host.data(), host.size(), cudaMemcpyHostToDevice, b.stream), "write restart records");
     check(cudaStreamSynchronize(b.stream), "cudaStreamSynchronize");
-    ++rs.round;
-    rs.restarted += selected.size();
-    line = fmt("[restart] seconds=%g elite_score=%lld replicas=%zu kicks=%d..%d min_escape_delta=%lld", elapsed,
-               (long long)gbest, selected.size(), p.restart_kick_min, p.restart_kick_max,
-               (long long)(escapes.empty() ? 0 : escapes.front().score_delta));
-    return (int)selected.size();
+    return done_line();
 }
 
 }  // namespace xw
@@ -994,6 +1204,9 @@ void xw_params_default(xw_params* p) {
     p->start_kind = 0;
     p->stop_on_solve = 1;
     p->warps_per_block = 0;
+    p->replicas_per_warp = 0;
+    p->warps_per_replica = 0;
+    p->restart_kicks = 0;
 }
 
 const char* xw_last_error(void) { return g_last_error.c_str(); }
@@ -1163,6 +1376,7 @@ double xw_calibrate(int32_t n, int32_t w, const int8_t* W, const xw_params* p, u
 
 struct xw_batch {
     std::unique_ptr<Batch> b;
+    std::vector<RestartState> restarts;   // per job, for xw_batch_restart
 };
 
 #define XW_GUARD(...)                                                         \
@@ -1290,38 +1504,99 @@ int32_t xw_autotune(const xw_job_spec* jobs, int32_t njobs, const xw_params* pin
         }
         Batch b;
         b.build(jobs, njobs, *pin, nullptr);
-        if (b.n_large == b.total_replicas)
+        if (b.classes.empty())
             return fail(XW_ERR_INVALID, "autotune covers the shared-memory kernel; every job here is of larger order");
         int optin = 0;
         check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, pin->device),
               "cudaDeviceGetAttribute max opt-in shared memory");
-        int best = 0;
-        float best_t = 0.0f;
-        for (int wpb : {1, 2, 4, 8, 16}) {
-            if ((size_t)wpb * b.slot_bytes > (size_t)optin) break;
-            b.configure_shape(wpb);
-            if (b.warps_per_block != wpb) continue;
-            float total = 0.0f;
-            for (int rep = 0; rep < 2; ++rep) {   // the first pass warms up, the second is timed
-                b.reset();
-                b.run(iters, false);
-                check(cudaStreamSynchronize(b.stream), "cudaStreamSynchronize");
-                total = 0.0f;
-                for (int k = 0; k < b.last_rounds; ++k) {
-                    float ms = 0.0f;
-                    check(cudaEventElapsedTime(&ms, b.events[2 * k], b.events[2 * k + 1]), "cudaEventElapsedTime");
-                    total += ms;
+        // each class alone: the batch's other classes are left out of the
+        // trial launches by timing only this class's items
+        const std::vector<Batch::LaunchClass> all = b.classes;
+        const uint32_t n_large = b.n_large;
+        b.n_large = 0;   // the trials launch no large-order replicas
+        float total_best = 0.0f;
+        int first_wpb = 0;
+        for (size_t k = 0; k < all.size(); ++k) {
+            b.classes.assign(1, all[k]);
+            int best = 0, best_rpw = 1;
+            float best_t = 0.0f;
+            auto time_trial = [&]() {
+                b.reserve_rounds((int)((iters + b.round_iters() - 1) / b.round_iters()));
+                float total = 0.0f;
+                for (int rep = 0; rep < 2; ++rep) {   // the first pass warms up, the second is timed
+                    b.reset();
+                    b.run(iters, false);
+                    check(cudaStreamSynchronize(b.stream), "cudaStreamSynchronize");
+                    total = 0.0f;
+                    for (int r = 0; r < b.last_rounds; ++r) {
+                        float ms = 0.0f;
+                        check(cudaEventElapsedTime(&ms, b.events[2 * r], b.events[2 * r + 1]), "cudaEventElapsedTime");
+                        total += ms;
+                    }
+                }
+                return total;
+            };
+            // the latency mode, for classes of at most one replica per SM
+            int best_wpr = 1;
+            float best_lat = 0.0f;
+            if (all[k].max_n <= 32 && all[k].item_count <= (uint32_t)b.props.multiProcessorCount) {
+                for (int wpr : {2, 4, 8, 16}) {
+                    if (!b.configure_latency(0, wpr)) continue;
+                    const float t = time_trial();
+                    if (best_wpr == 1 || t < best_lat) {
+                        best_wpr = wpr;
+                        best_lat = t;
+                    }
                 }
             }
-            if (best == 0 || total < best_t) {
-                best = wpb;
-                best_t = total;
+            for (int rpw : {1, 2}) {
+                if (rpw == 2 && all[k].kind != kTunePairKind) continue;
+                for (int wpb : {1, 2, 4, 8, 16}) {
+                    if ((size_t)wpb * rpw * all[k].slot_bytes > (size_t)optin) break;
+                    if (!b.configure_class(0, wpb, rpw)) continue;
+                    const float total = time_trial();
+                    if (best == 0 || total < best_t) {
+                        best = wpb;
+                        best_rpw = rpw;
+                        best_t = total;
+                    }
+                }
             }
+            if (best == 0) return fail(XW_ERR_CAPACITY, "no launch shape fits the device's shared memory");
+            record_tuned(all[k].kind, all[k].slot_bytes, best, best_rpw);
+            if (best_wpr > 1) {
+                // the latency mode against the best one-warp shape
+                const bool lat = best_lat < best_t;
+                record_tuned(kTuneLatencyKind, all[k].slot_bytes, lat ? best_wpr : 1, 1);
+                if (lat) best_t = best_lat;
+            }
+            if (k == 0) first_wpb = best;
+            total_best += best_t;
         }
-        if (best == 0) return fail(XW_ERR_CAPACITY, "no launch shape fits the device's shared memory");
-        record_tuned(b.opl, b.slot_bytes, best);
-        *best_wpb = best;
-        if (best_ms) *best_ms = best_t;
+        b.classes = all;
+        b.n_large = n_large;
+        *best_wpb = first_wpb;
+        if (best_ms) *best_ms = total_best;
+        return XW_OK;
+    })
+}
+
+int32_t xw_batch_restart(xw_batch* h, int32_t job, int32_t* restarted) {
+    if (!h || !restarted) return fail(XW_ERR_INVALID, "null argument");
+    XW_GUARD({
+        Batch& b = *h->b;
+        if (job < 0 || job >= (int)b.jobs.size()) return fail(XW_ERR_INVALID, "job index out of range");
+        if (h->restarts.size() != b.jobs.size()) h->restarts.assign(b.jobs.size(), RestartState{});
+        std::vector<JobOut> out;
+        std::vector<int8_t> best(b.best_bytes);
+        b.collect(out, best.data(), true);
+        const XwJob& J = b.jobs[job];
+        const std::vector<int8_t> elite(best.begin() + b.best_offsets[job],
+                                        best.begin() + b.best_offsets[job] + (size_t)J.n * J.n);
+        RestartState& rs = h->restarts[job];
+        rs.elite = out[job].best_replica;
+        std::string line;
+        *restarted = restart_population(b, job, elite, out[job].score, out[job].conflicts, rs, 0.0, line);
         return XW_OK;
     })
 }
@@ -1374,6 +1649,10 @@ int32_t xw_batch_read_replica(xw_batch* h, int32_t job, int32_t replica, xw_repl
             st->objective_kind = H->obj_kind;
             st->status = H->status;
             st->error = H->err;
+            st->accepted_moves = H->accepted;
+            st->accepted_rows = H->accepted_rows;
+            st->two_row_evaluations = H->two_row_evals;
+            st->reserved = 0;
         }
         const size_t nn = (size_t)J.n * J.n;
         if (W) std::memcpy(W, rec.data() + J.off_w, nn);
@@ -1406,9 +1685,59 @@ int32_t xw_batch_bytes(xw_batch* h, uint64_t* h2d, uint64_t* d2h) {
 
 int32_t xw_batch_shape(xw_batch* h, int32_t* wpb, int32_t* blocks, int32_t* slot) {
     if (!h) return fail(XW_ERR_INVALID, "null batch");
-    if (wpb) *wpb = h->b->warps_per_block;
-    if (blocks) *blocks = h->b->blocks;
-    if (slot) *slot = (int32_t)h->b->slot_bytes;
+    // the class with the most replicas
+    const Batch& b = *h->b;
+    const Batch::LaunchClass* c = nullptr;
+    for (const auto& k : b.classes)
+        if (!c || k.item_count > c->item_count) c = &k;
+    if (wpb) *wpb = c ? c->wpb : b.large_wpb;
+    if (blocks) *blocks = c ? c->blocks : b.large_blocks;
+    if (slot) *slot = (int32_t)(c ? c->slot_bytes : b.large_slot_bytes);
+    return XW_OK;
+}
+
+int32_t xw_batch_classes(xw_batch* h, xw_launch_class* out, int32_t cap, int32_t* count) {
+    if (!h || !count || (cap > 0 && !out)) return fail(XW_ERR_INVALID, "null argument");
+    const Batch& b = *h->b;
+    std::vector<xw_launch_class> all;
+    if (b.n_large) {
+        xw_launch_class c{};
+        c.large = 1;
+        c.min_order = 0x7fffffff;
+        for (const XwJob& J : b.jobs)
+            if (J.large) {
+                c.min_order = std::min(c.min_order, J.n);
+                c.max_order = std::max(c.max_order, J.n);
+                c.general = c.general || J.general;
+            }
+        c.rows_per_lane = 0;
+        c.replicas_per_warp = 1;
+        c.warps_per_block = b.large_wpb;
+        c.blocks = b.large_blocks;
+        c.slot_bytes = (int32_t)b.large_slot_bytes;
+        c.chunks = (int32_t)b.large_chunks;
+        c.replicas = (int32_t)b.n_large;
+        c.warps_per_replica = 1;
+        all.push_back(c);
+    }
+    for (const auto& k : b.classes) {
+        xw_launch_class c{};
+        c.min_order = k.min_n;
+        c.max_order = k.max_n;
+        c.rows_per_lane = k.opl;
+        c.replicas_per_warp = k.rpw;
+        c.warps_per_block = k.wpb;
+        c.blocks = k.blocks;
+        c.slot_bytes = (int32_t)k.slot_bytes;
+        c.chunks = (int32_t)k.chunks;
+        c.replicas = (int32_t)k.item_count;
+        c.general = k.general ? 1 : 0;
+        c.warps_per_replica = k.wpr;
+        if (k.wpr > 1) c.slot_bytes = (int32_t)k.spec_bytes;
+        all.push_back(c);
+    }
+    *count = (int32_t)all.size();
+    for (int32_t i = 0; i < cap && i < (int32_t)all.size(); ++i) out[i] = all[i];
     return XW_OK;
 }
 
@@ -1487,7 +1816,7 @@ int32_t xw_run(int32_t n, int32_t w, const xw_params* pin, const int8_t* start, 
             int per_sm = 0;
             const void* fn = large ? anneal_large_kernel_fn(needs_general_kernel(p))
                                    : anneal_kernel_fn(anneal_opl(n), needs_general_kernel(p));
-            cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(wpb * slot));
+            raise_smem_limit(fn, p.device);
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * wpb, (size_t)wpb * slot);
             replicas = std::max(1, per_sm * wpb * out->device.multiprocessors);
         }
@@ -1561,8 +1890,21 @@ int32_t xw_run(int32_t n, int32_t w, const xw_params* pin, const int8_t* start, 
         }
         b.collect(res, best.data(), true);
         const double search_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-        const CpuState fin = CpuState::from_entries(n, w, best);
-        if (fin.score() != res[0].score || fin.conflicts() != res[0].conflicts)
+        // the final best W: rescored and checked exactly on the device
+        // (tensor cores), or on the host above the shared-memory orders
+        int64_t fin_score = 0, fin_conf = 0;
+        bool fin_exact = false;
+        if (!b.vstats_valid.empty() && b.vstats_valid[0]) {
+            fin_score = b.vstats[0].score;
+            fin_conf = b.vstats[0].conflicts;
+            fin_exact = b.vstats[0].exact == 1;
+        } else {
+            const CpuState fin = CpuState::from_entries(n, w, best);
+            fin_score = fin.score();
+            fin_conf = fin.conflicts();
+            fin_exact = fin.verify_weighing();
+        }
+        if (fin_score != res[0].score || fin_conf != res[0].conflicts)
             throw std::runtime_error("CUDA final best snapshot score mismatch");
         const uint64_t moves = res[0].moves, evals = res[0].cand_evals;
         say(fmt("done moves=%llu candidate_evaluations=%llu seconds=%g moves_per_sec=%g "
@@ -1574,7 +1916,7 @@ int32_t xw_run(int32_t n, int32_t w, const xw_params* pin, const int8_t* start, 
         out->conflicts = res[0].conflicts;
         out->replicas = replicas;
         out->solved = res[0].score == 0;
-        out->verified = out->solved ? (fin.verify_weighing() ? 1 : 0) : 0;
+        out->verified = out->solved ? (fin_exact ? 1 : 0) : 0;
         out->best_replica = res[0].best_replica;
         out->moves = moves;
         out->candidate_evaluations = evals;

@@ -29,6 +29,8 @@ struct AnnealArgs {
     // chunk_done[rid] (zeroed per launch) counts a replica's finished chunks.
     uint32_t chunks = 1;
     uint32_t* chunk_done = nullptr;
+    // device-time limit of a chunk's wait for its predecessor, 0 = 30 s
+    uint64_t chunk_wait_ns = 0;
 };
 
 // shared-memory bytes one warp needs for a replica of order n, minority m,
@@ -38,10 +40,22 @@ uint32_t anneal_slot_bytes(int n, int m, int opl);
 int anneal_opl(int n);
 // `general`: some replica of the launch uses the squared or parity objective
 // or the within-row swap move set; otherwise the lean kernel (L1 score,
-// the reference's moves) runs, which drops that work from the hot loop
-const void* anneal_kernel_fn(int opl, bool general);
+// the reference's moves) runs, which drops that work from the hot loop.
+// `rpw`: replicas per warp, 1, or 2 for orders up to 16 (opl 1; each half
+// of a warp owns a replica and a shared-memory slot of args.slot_bytes, so
+// a CTA holds warps_per_block * rpw slots).
+const void* anneal_kernel_fn(int opl, bool general, int rpw = 1);
 cudaError_t launch_anneal(const AnnealArgs& args, int opl, bool general, int warps_per_block, int blocks,
-                          cudaStream_t stream);
+                          cudaStream_t stream, int rpw = 1);
+// Latency mode (orders up to 32): one replica per CTA of K warps (2..16),
+// which speculate K iterations at a time and keep the first accepted one;
+// the trajectory is the one-warp kernel's.  Shared memory per CTA for
+// replicas whose one-warp slot (anneal_slot_bytes at one row per lane) is
+// at most slot_bytes; the kernel and its launch (a.slot_bytes: the CTA's
+// dynamic shared memory; a.chunks must be 1).
+uint32_t anneal_spec_cta_bytes(uint32_t slot_bytes, int K);
+const void* anneal_spec_kernel_fn(bool general);
+cudaError_t launch_anneal_spec(const AnnealArgs& args, bool general, int K, int blocks, cudaStream_t stream);
 // Orders above XW_MAX_N: the kernel whose replica state lives in HBM
 // (xw_anneal_large.cu).  Shared memory per warp, Gram-arena bytes per
 // replica (a multiple of 256), the kernel, and its launch.
@@ -63,6 +77,7 @@ struct JobOut {
     int32_t first_solver;           // least (solve iteration, index) with score 0, or -1
     uint64_t moves, cand_evals, iters;
     uint64_t solved_it, solve_ns;   // the first solver's solve iteration and %globaltimer
+    uint64_t accepted, accepted_rows, two_row_evals;   // sums of the replicas' statistics
 };
 
 // One warp per job: results and (best_out nonnull) the chosen replica's best

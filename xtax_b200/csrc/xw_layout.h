@@ -33,6 +33,7 @@
 #define XW_ERR_MINORITY 2u     // W row weights disagree with the minority lists
 #define XW_ERR_KERNEL 4u       // a lean launch met a replica that needs the general kernel
 #define XW_ERR_CHUNK 8u        // a chunk's wait for its replica's previous chunk timed out
+// (the same values as XW_DEVERR_* of include/xw.h)
 
 struct XwJob {
     int32_t n, w, m, sparse;        // m = min(w, n-w); sparse = (w <= n-w)
@@ -76,7 +77,10 @@ struct RepHeader {
     uint32_t status, err;
     uint64_t solve_it;
     uint64_t solve_ns;
-    uint32_t pad[4];
+    // move statistics (32-bit, wrapping): accepted moves, rows those moves
+    // changed (1 or 2 each), and candidates evaluated that change two rows
+    uint32_t accepted, accepted_rows, two_row_evals;
+    uint32_t pad;
 };
 
 #ifdef __cplusplus

@@ -92,6 +92,10 @@ __global__ void noalloc_init_kernel(unsigned char* scratch, XwJob job, NoallocLa
         items[r] = (uint32_t)r;
         RepHeader* H = reinterpret_cast<RepHeader*>(scratch + off);
         memset(H, 0, sizeof(RepHeader));
+        // no score yet (the kernel computes it from W when it loads the
+        // replica): a replica the kernel refuses cannot read as solved
+        H->score = H->best_score = INT32_MAX;
+        H->conflicts = H->best_conflicts = INT32_MAX;
         H->job = 0;
         H->stream = (uint32_t)r;
         H->temperature = ladder[r];
@@ -115,7 +119,9 @@ __global__ void noalloc_init_kernel(unsigned char* scratch, XwJob job, NoallocLa
 }
 
 // Copies each replica's best W and {best score, best conflicts, score,
-// moves} into the caller's buffers.
+// moves} into the caller's buffers.  A replica the kernel flagged (a start
+// row whose weight is not w, a failed self-check) reports best score -1 and
+// best conflicts -err instead, so that it cannot read as solved.
 __global__ void noalloc_output_kernel(const unsigned char* scratch, NoallocLayout L, int n, int R, int8_t* best,
                                       int64_t* stats, uint32_t off_best) {
     const int r = blockIdx.x;
@@ -125,9 +131,10 @@ __global__ void noalloc_output_kernel(const unsigned char* scratch, NoallocLayou
     const int8_t* src = reinterpret_cast<const int8_t*>(scratch + off + off_best);
     for (int i = threadIdx.x; i < n * n; i += blockDim.x) best[(size_t)r * n * n + i] = src[i];
     if (threadIdx.x == 0) {
-        stats[4 * r + 0] = H->best_score;
-        stats[4 * r + 1] = H->best_conflicts;
-        stats[4 * r + 2] = H->score;
+        const bool bad = H->err != 0;
+        stats[4 * r + 0] = bad ? -1 : H->best_score;
+        stats[4 * r + 1] = bad ? -(int64_t)H->err : H->best_conflicts;
+        stats[4 * r + 2] = bad ? -1 : H->score;
         stats[4 * r + 3] = (int64_t)H->moves;
     }
 }
@@ -201,7 +208,14 @@ extern "C" int32_t xw_anneal_noalloc(int32_t n, int32_t w, const xw_params* p, i
         }
         scratch = g_scratch_ptr[dev];
     }
-    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(wpb * slot));
+    // the kernel's shared-memory limit goes to the device's opt-in maximum,
+    // as every other launcher of it sets it, so that no call lowers the
+    // limit a batch or server launch of a larger order relies on
+    int optin = 0;
+    e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e == cudaSuccess && (size_t)wpb * slot > (size_t)optin)
+        return nfail(XW_ERR_CAPACITY, "xw_anneal_noalloc: the replicas' shared memory exceeds the device's limit");
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
     if (e != cudaSuccess) return nfail(XW_ERR_CAPACITY, std::string("cudaFuncSetAttribute failed: ") + cudaGetErrorString(e));
     int per_sm = 0, sms = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * wpb, (size_t)wpb * slot);

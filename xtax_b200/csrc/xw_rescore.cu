@@ -28,11 +28,14 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "../../include/xw.h"
 #include "xw_host_internal.h"
@@ -56,6 +59,7 @@ struct RescoreParams {
     int4* stats;        // per matrix {score, conflicts, squared, exact}
     int32_t* gram;      // nullable: per matrix n*n row-major
     int* error;         // nonzero after a timed-out wait
+    const int2* dims;   // nullable: per matrix {order, weight} of a matrix zero-padded to n
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -284,7 +288,15 @@ __global__ void __launch_bounds__(128, 4) rescore_tc_kernel(const __grid_constan
             s_abs += 2 * o_abs - abs(dg);
             s_nz += 2 * o_nz - min(abs(dg), 1);
             s_sq += 2 * o_sq - dg * dg;
-            diag_ok = dg == p.w;
+            // a zero-padded matrix: its own rows carry w on the diagonal,
+            // the padding rows 0 (their off-diagonal entries are 0 anyway)
+            int nv = p.n, wv = p.w;
+            if (p.dims && mat < p.count) {
+                const int2 d = p.dims[mat];
+                nv = d.x;
+                wv = d.y;
+            }
+            diag_ok = i < nv ? dg == wv : dg == 0;
             part.x = __reduce_add_sync(0xffffffffu, s_abs);
             part.y = __reduce_add_sync(0xffffffffu, s_nz);
             part.z = __reduce_add_sync(0xffffffffu, s_sq);
@@ -332,9 +344,12 @@ __global__ void __launch_bounds__(128, 4) rescore_tc_kernel(const __grid_constan
 
 // SIMT path for orders that do not fill 32-row tensor-core blocks: one warp
 // per matrix, lane o accumulates column o of G.
-__global__ void rescore_simt_kernel(const int8_t* W, int count, int n, int w, int4* stats, int32_t* gram) {
+__global__ void rescore_simt_kernel(const int8_t* W, int count, int n, int w, int4* stats, int32_t* gram,
+                                    const int2* dims) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (warp >= count) return;
+    const int nv = dims ? dims[warp].x : n;
+    if (dims) w = dims[warp].y;
     const int8_t* M = W + (size_t)warp * n * n;
     int s_abs = 0, s_nz = 0, s_sq = 0, diag_ok = 1;
     for (int o = lane; o < n; o += 32) {
@@ -343,7 +358,7 @@ __global__ void rescore_simt_kernel(const int8_t* W, int count, int n, int w, in
             for (int c = 0; c < n; ++c) dot += M[r * n + c] * M[o * n + c];
             if (gram) gram[(size_t)warp * n * n + (size_t)r * n + o] = dot;
             if (r == o) {
-                diag_ok &= dot == w;
+                diag_ok &= dot == (o < nv ? w : 0);
             } else {
                 const int a = dot < 0 ? -dot : dot;
                 s_abs += a;
@@ -402,7 +417,7 @@ int* error_flag_ptr() {
 
 // Enqueue the rescoring of `count` row-major n x n matrices at W (device).
 int32_t rescore_device(const int8_t* W, int64_t count, int n, int w, int32_t* stats, int32_t* gram,
-                       cudaStream_t stream, int* err_flag, bool force_simt) {
+                       cudaStream_t stream, int* err_flag, bool force_simt, const int2* dims) {
     if (count < 0 || count > INT32_MAX / 4) return rfail(XW_ERR_INVALID, "rescore: count out of range");
     if (n < 1 || n > XW_MAX_ORDER_SHARED) return rfail(XW_ERR_INVALID, "rescore: order must be in [1, 256]");
     if (count == 0) return XW_OK;
@@ -411,7 +426,8 @@ int32_t rescore_device(const int8_t* W, int64_t count, int n, int w, int32_t* st
     const bool tc = !force_simt && n % 32 == 0 && n <= 128 && ((uintptr_t)W % 16) == 0;
     if (!tc) {
         const int blocks = (int)((count * 32 + 255) / 256);
-        rescore_simt_kernel<<<blocks, 256, 0, stream>>>(W, (int)count, n, w, reinterpret_cast<int4*>(stats), gram);
+        rescore_simt_kernel<<<blocks, 256, 0, stream>>>(W, (int)count, n, w, reinterpret_cast<int4*>(stats), gram,
+                                                        dims);
         e = cudaGetLastError();
         return e == cudaSuccess ? XW_OK : rfail(XW_ERR_CUDA, std::string("rescore launch: ") + cudaGetErrorString(e));
     }
@@ -427,12 +443,13 @@ int32_t rescore_device(const int8_t* W, int64_t count, int n, int w, int32_t* st
     p.stats = reinterpret_cast<int4*>(stats);
     p.gram = gram;
     p.error = err_flag;
+    p.dims = dims;
     CUtensorMap map;
-    const cuuint64_t dims[2] = {(cuuint64_t)n, (cuuint64_t)count * n};
+    const cuuint64_t extent[2] = {(cuuint64_t)n, (cuuint64_t)count * n};
     const cuuint64_t strides[1] = {(cuuint64_t)n};
     const cuuint32_t box[2] = {128u, (cuuint32_t)p.rows_per_tile};
     const cuuint32_t estr[2] = {1u, 1u};
-    const CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t*>(W), dims, strides, box, estr,
+    const CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t*>(W), extent, strides, box, estr,
                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return rfail(XW_ERR_CUDA, "rescore: cuTensorMapEncodeTiled failed");
@@ -454,6 +471,104 @@ int32_t rescore_device(const int8_t* W, int64_t count, int n, int w, int32_t* st
     return e == cudaSuccess ? XW_OK : rfail(XW_ERR_CUDA, std::string("rescore launch: ") + cudaGetErrorString(e));
 }
 
+// Copies each matrix of a verification batch into its zero-padded
+// row-major slot (block b: matrix b of the group; the source is the
+// column-major W of the search) and writes its {order, weight}.
+__global__ void verify_gather_kernel(const VerifyItem* items, const int32_t* index, int N, int8_t* dst, int2* dims) {
+    const VerifyItem it = items[index[blockIdx.x]];
+    int8_t* out = dst + (size_t)blockIdx.x * N * N;
+    for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
+        const int r = e / N, c = e - r * N;
+        out[e] = r < it.n && c < it.n ? it.W[(size_t)c * it.n + r] : (int8_t)0;
+    }
+    if (threadIdx.x == 0) dims[blockIdx.x] = make_int2(it.n, it.w);
+}
+
+DeviceVerifier::~DeviceVerifier() {
+    for (void* ptr : {(void*)d_items, (void*)d_index, (void*)d_stage, (void*)d_dims, (void*)d_stats})
+        if (ptr) cudaFree(ptr);
+    if (h_stats) cudaFreeHost(h_stats);
+    if (h_table) cudaFreeHost(h_table);
+}
+
+void DeviceVerifier::reserve(size_t items, size_t stage_bytes) {
+    if (items > cap_items) {
+        for (void* ptr : {(void*)d_items, (void*)d_index, (void*)d_dims, (void*)d_stats})
+            if (ptr) check_cuda(cudaFree(ptr), "cudaFree");
+        if (h_stats) check_cuda(cudaFreeHost(h_stats), "cudaFreeHost");
+        if (h_table) check_cuda(cudaFreeHost(h_table), "cudaFreeHost");
+        const size_t cap = std::max<size_t>(items, 64);
+        check_cuda(cudaMalloc(&d_items, sizeof(VerifyItem) * cap), "cudaMalloc verification items");
+        check_cuda(cudaMalloc(&d_index, sizeof(int32_t) * cap), "cudaMalloc verification index");
+        check_cuda(cudaMalloc(&d_dims, sizeof(int2) * cap), "cudaMalloc verification dims");
+        check_cuda(cudaMalloc(&d_stats, sizeof(int4) * cap), "cudaMalloc verification stats");
+        check_cuda(cudaMallocHost(&h_stats, sizeof(int4) * cap), "cudaMallocHost verification stats");
+        check_cuda(cudaMallocHost(&h_table, (sizeof(VerifyItem) + sizeof(int32_t)) * cap),
+                   "cudaMallocHost verification table");
+        cap_items = cap;
+    }
+    if (stage_bytes > cap_stage) {
+        if (d_stage) check_cuda(cudaFree(d_stage), "cudaFree");
+        check_cuda(cudaMalloc(&d_stage, stage_bytes), "cudaMalloc verification staging");
+        cap_stage = stage_bytes;
+    }
+}
+
+void DeviceVerifier::run(const std::vector<VerifyItem>& items, cudaStream_t stream, std::vector<VerifyStats>& out) {
+    out.assign(items.size(), VerifyStats{});
+    if (items.empty()) return;
+    // groups of one padded order: a multiple of 32 up to 128 (tensor cores),
+    // the order itself above (SIMT)
+    auto padded = [](int n) { return n <= 128 ? 32 * ((n + 31) / 32) : n; };
+    std::vector<int32_t> index(items.size());
+    for (size_t k = 0; k < items.size(); ++k) {
+        if (items[k].n < 1 || items[k].n > XW_MAX_ORDER_SHARED)
+            throw std::invalid_argument("device verification covers orders 1..256");
+        index[k] = (int32_t)k;
+    }
+    std::stable_sort(index.begin(), index.end(),
+                     [&](int32_t a, int32_t b) { return padded(items[a].n) < padded(items[b].n); });
+    size_t stage = 0;
+    for (size_t k = 0; k < items.size(); ++k) {
+        const size_t N = (size_t)padded(items[index[k]].n);
+        stage = (stage + N * N + 127) & ~size_t(127);
+    }
+    reserve(items.size(), stage);
+    VerifyItem* hi = reinterpret_cast<VerifyItem*>(h_table);
+    int32_t* hx = reinterpret_cast<int32_t*>(hi + items.size());
+    std::memcpy(hi, items.data(), sizeof(VerifyItem) * items.size());
+    std::memcpy(hx, index.data(), sizeof(int32_t) * items.size());
+    check_cuda(cudaMemcpyAsync(d_items, hi, sizeof(VerifyItem) * items.size(), cudaMemcpyHostToDevice, stream),
+               "upload verification items");
+    check_cuda(cudaMemcpyAsync(d_index, hx, sizeof(int32_t) * items.size(), cudaMemcpyHostToDevice, stream),
+               "upload verification index");
+    int* flag = error_flag_ptr();
+    if (!flag) throw std::runtime_error("rescore: cannot resolve the error flag");
+    size_t off = 0;
+    for (size_t g0 = 0; g0 < index.size();) {
+        const int N = padded(items[index[g0]].n);
+        size_t g1 = g0;
+        while (g1 < index.size() && padded(items[index[g1]].n) == N) ++g1;
+        const int cnt = (int)(g1 - g0);
+        int8_t* dst = d_stage + off;
+        verify_gather_kernel<<<cnt, 256, 0, stream>>>(d_items, d_index + g0, N, dst, d_dims + g0);
+        check_cuda(cudaGetLastError(), "launch verify_gather_kernel");
+        const int32_t rc = rescore_device(dst, cnt, N, 0, reinterpret_cast<int32_t*>(d_stats + g0), nullptr, stream,
+                                          flag, false, d_dims + g0);
+        if (rc != XW_OK) throw std::runtime_error("device verification launch failed");
+        off = (off + (size_t)cnt * N * N + 127) & ~size_t(127);
+        g0 = g1;
+    }
+    check_cuda(cudaMemcpyAsync(h_stats, d_stats, sizeof(int4) * items.size(), cudaMemcpyDeviceToHost, stream),
+               "read verification stats");
+    check_cuda(cudaStreamSynchronize(stream), "cudaStreamSynchronize verification");
+    if (xw_rescore_status() != XW_OK) throw std::runtime_error("device verification: a rescoring wait expired");
+    for (size_t k = 0; k < items.size(); ++k) {
+        const int4 v = reinterpret_cast<const int4*>(h_stats)[k];
+        out[index[k]] = VerifyStats{v.x, v.y, v.z, v.w};
+    }
+}
+
 }  // namespace xw
 
 using namespace xw;
@@ -463,7 +578,7 @@ extern "C" int32_t xw_rescore_device(const int8_t* W, int64_t count, int32_t n, 
     if (!W || !stats) return rfail(XW_ERR_INVALID, "rescore: null argument");
     int* flag = error_flag_ptr();
     if (!flag) return rfail(XW_ERR_CUDA, "rescore: cannot resolve the error flag");
-    return rescore_device(W, count, n, w, stats, gram, static_cast<cudaStream_t>(stream), flag, simt != 0);
+    return rescore_device(W, count, n, w, stats, gram, static_cast<cudaStream_t>(stream), flag, simt != 0, nullptr);
 }
 
 extern "C" int32_t xw_rescore_status(void) {

@@ -30,6 +30,7 @@
 
 #include "../../include/xw.h"
 #include "xw_cpu.h"
+#include "xw_device.cuh"
 #include "xw_host_internal.h"
 
 namespace xw {
@@ -146,7 +147,196 @@ struct DevBuf {
     }
 };
 
+// ---------------------------------------------------------------------------
+// Device kicks (restart mode 1).  The reference kicks the elite's copies on
+// the host with std::mt19937 (xweigh_cuda.cu:2089-2193) after reading the
+// population back; here one CTA per restarted replica rewrites its record
+// in place: the elite's best W, the escape move, then by (index + round) % 3
+// nothing more, row kicks (2..max(2, w/2) distinct nonzeros of 1..4 random
+// rows flip, then kick/4 random moves) or kick random moves that are all
+// support switches; a random move is a sign flip of a random nonzero (a
+// coin under the job's sign threshold, or no zeros at all) or a
+// value-preserving 2x2 support switch, `steps` of them within 8*steps
+// attempts.  Draw k is word k%4 of Philox({k/4, round_lo, round_hi,
+// 0x20000000 | replica}, job key); an index in [0,count) is Lemire's
+// multiply-shift with a rejected word replaced by the next (at most 64
+// tries).  Then the record gets the kicked W's scores, minority lists
+// (rebuilt in column order), best W, the reheat temperature and cleared
+// stagnation counters.
+
+__device__ __forceinline__ uint32_t kick_word(uint32_t& k, uint32_t k0, uint32_t k1, uint32_t r_lo, uint32_t r_hi,
+                                              uint32_t tag) {
+    const uint4 b = philox4x32_10(make_uint4(k >> 2, r_lo, r_hi, tag), k0, k1);
+    const uint32_t v = pick(b, (int)(k & 3u));
+    ++k;
+    return v;
+}
+
+struct KickRng {
+    uint32_t k, k0, k1, r_lo, r_hi, tag;
+    __device__ uint32_t word() { return kick_word(k, k0, k1, r_lo, r_hi, tag); }
+    __device__ uint32_t index(uint32_t count) {
+        uint64_t prod = 0;
+        for (int t = 0; t < 64; ++t) {
+            prod = (uint64_t)word() * count;
+            const uint32_t low = (uint32_t)prod;
+            if (low >= count || low >= (0u - count) % count) break;
+        }
+        return (uint32_t)(prod >> 32);
+    }
+};
+
+__device__ int kick_nonzero(const int8_t* K, int n, int row, int k) {
+    for (int c = 0; c < n; ++c)
+        if (K[(size_t)c * n + row] != 0 && k-- == 0) return c;
+    return -1;
+}
+
+constexpr int kKickThreads = 128;
+
+__global__ void __launch_bounds__(kKickThreads) kick_kernel(KickArgs a) {
+    const KickJob kj = a.kicks[blockIdx.x];
+    const XwJob& J = *a.job;
+    const int n = J.n, w = J.w, m = J.m;
+    uint8_t* rec = a.arena + a.rec_off[kj.rid];
+    RepHeader* H = reinterpret_cast<RepHeader*>(rec);
+    int8_t* K = reinterpret_cast<int8_t*>(rec + J.off_w);
+    const int tid = threadIdx.x;
+    for (int i = tid; i < n * n; i += kKickThreads) K[i] = a.elite[i];
+    __syncthreads();
+    if (tid == 0) {
+        auto at = [&](int r, int c) -> int8_t& { return K[(size_t)c * n + r]; };
+        if (kj.esc >= 0) {
+            const int* e = a.escapes + 6 * kj.esc;
+            at(e[0], e[2]) = 0;
+            at(e[1], e[3]) = 0;
+            at(e[0], e[3]) = (int8_t)e[4];
+            at(e[1], e[2]) = (int8_t)e[5];
+        }
+        KickRng g{0u, J.key0, J.key1, (uint32_t)a.round, (uint32_t)(a.round >> 32), 0x20000000u | H->stream};
+        const int mode = (int)(((uint64_t)kj.index + a.round) % 3ull);
+        int steps = kj.kick;
+        uint64_t thr = J.thr_sign;
+        if (mode == 0) {
+            steps = 0;
+        } else if (mode == 1 && kj.kick > 0 && w >= 3) {
+            int rows = 1 + kj.kick / (w > 1 ? w : 1);
+            if (rows > 4) rows = 4;
+            const int maxf = w / 2 > 2 ? w / 2 : 2;
+            for (int rk = 0; rk < rows; ++rk) {
+                const int row = (int)g.index((uint32_t)n);
+                int cnt = 0;
+                for (int c = 0; c < n; ++c) cnt += at(row, c) != 0;
+                const int flips = 2 + (int)g.index((uint32_t)(maxf - 1));
+                // a partial Fisher-Yates shuffle of the row's nonzero
+                // columns, kept as a permutation of ranks in column order
+                // (the k-th nonzero column is found by a scan)
+                uint16_t* perm = a.scratch + (size_t)blockIdx.x * XW_MAX_ORDER_LARGE;
+                for (int q = 0; q < cnt; ++q) perm[q] = (uint16_t)q;
+                for (int f = 0; f < flips && f < cnt; ++f) {
+                    const int j = f + (int)g.index((uint32_t)(cnt - f));
+                    const uint16_t t = perm[f];
+                    perm[f] = perm[j];
+                    perm[j] = t;
+                }
+                for (int f = 0; f < flips && f < cnt; ++f) {
+                    const int col = kick_nonzero(K, n, row, perm[f]);
+                    at(row, col) = (int8_t)-at(row, col);
+                }
+            }
+            steps = kj.kick / 4;
+        } else if (mode == 2) {
+            thr = 0;
+        }
+        int applied = 0;
+        for (int t = 0; t < 8 * steps && applied < steps; ++t) {
+            const uint32_t u = g.word();
+            if (w == n || (uint64_t)u < thr) {
+                const int row = (int)g.index((uint32_t)n);
+                const int col = kick_nonzero(K, n, row, (int)g.index((uint32_t)w));
+                at(row, col) = (int8_t)-at(row, col);
+                ++applied;
+                continue;
+            }
+            if (n < 2) continue;
+            const int r1 = (int)g.index((uint32_t)n);
+            int r2 = (int)g.index((uint32_t)(n - 1));
+            if (r2 >= r1) ++r2;
+            const int c1 = kick_nonzero(K, n, r1, (int)g.index((uint32_t)w));
+            const int c2 = kick_nonzero(K, n, r2, (int)g.index((uint32_t)w));
+            if (c1 == c2 || at(r1, c2) != 0 || at(r2, c1) != 0) continue;
+            const int8_t v1 = at(r1, c1), v2 = at(r2, c2);
+            at(r1, c1) = 0;
+            at(r2, c2) = 0;
+            at(r1, c2) = v1;
+            at(r2, c1) = v2;
+            ++applied;
+        }
+    }
+    __syncthreads();
+    // scores of the kicked W: thread t takes rows t, t + 128, ...
+    __shared__ unsigned long long s_sq;
+    __shared__ int s_score, s_conf, s_par;
+    if (tid == 0) {
+        s_sq = 0;
+        s_score = s_conf = s_par = 0;
+    }
+    __syncthreads();
+    int p_score = 0, p_conf = 0, p_par = 0;
+    unsigned long long p_sq = 0;
+    for (int r = tid; r < n; r += kKickThreads) {
+        for (int o = r + 1; o < n; ++o) {
+            int dot = 0;
+            for (int c = 0; c < n; ++c) dot += K[(size_t)c * n + r] * K[(size_t)c * n + o];
+            const int ad = dot < 0 ? -dot : dot;
+            p_score += ad;
+            p_conf += dot != 0;
+            p_sq += (unsigned long long)(dot * dot);
+            p_par += ad & 1;
+        }
+        // the row's minority list, in column order (u16 entries above the
+        // shared-memory orders)
+        int pos = 0;
+        for (int c = 0; c < n && pos < m; ++c)
+            if ((K[(size_t)c * n + r] != 0) == (J.sparse != 0)) {
+                if (J.large)
+                    reinterpret_cast<uint16_t*>(rec + J.off_mino)[(size_t)r * m + pos] = (uint16_t)c;
+                else
+                    rec[J.off_mino + (size_t)r * m + pos] = (uint8_t)c;
+                ++pos;
+            }
+    }
+    atomicAdd(&s_score, p_score);
+    atomicAdd(&s_conf, p_conf);
+    atomicAdd(&s_par, p_par);
+    atomicAdd(&s_sq, p_sq);
+    __syncthreads();
+    const int score = s_score, conf = s_conf;
+    const bool better = score < a.gbest || (score == a.gbest && conf < a.gconf);
+    int8_t* B = reinterpret_cast<int8_t*>(rec + J.off_best);
+    for (int i = tid; i < n * n; i += kKickThreads) B[i] = better ? K[i] : a.elite[i];
+    if (tid == 0) {
+        H->score = score;
+        H->conflicts = conf;
+        H->best_score = better ? score : a.gbest;
+        H->best_conflicts = better ? conf : a.gconf;
+        H->obj_total = H->obj_kind == 1 ? (int64_t)s_sq : H->obj_kind == 2 ? (int64_t)s_par : (int64_t)score;
+        const double t = __dmul_rn(H->reheat_temperature, a.reheat);
+        H->temperature = t > a.t_min ? t : a.t_min;
+        H->msi = 0;
+        H->cool_ctr = 0;
+        H->status &= ~XW_STATUS_GRAM;   // the large-order kernel rebuilds G from the new W
+    }
+}
+
 }  // namespace
+
+void launch_kicks(const KickArgs& a, int count, cudaStream_t stream) {
+    if (count <= 0) return;
+    kick_kernel<<<count, kKickThreads, 0, stream>>>(a);
+    check_cuda(cudaGetLastError(), "launch kick_kernel");
+}
+
 
 std::vector<ScanResult> escape_scan(int n, const int8_t* W, const int32_t* G, size_t limit) {
     std::vector<ScanResult> out;

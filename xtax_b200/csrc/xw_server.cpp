@@ -49,11 +49,18 @@
 namespace xw {
 namespace {
 
-constexpr int kClasses = 4;                      // rows per lane 1, 2, 4, 8
+// Launch classes of a round: 0 holds the orders up to 16 (at most 16
+// candidates per move), which may run two replicas per warp; 1..4 the other
+// orders by rows per lane 1, 2, 4, 8.
+constexpr int kClasses = 5;
 constexpr size_t kBestStride = (size_t)XW_MAX_N * XW_MAX_N;
 
-int class_of(int n) { return n <= 32 ? 0 : n <= 64 ? 1 : n <= 128 ? 2 : 3; }
-int opl_of_class(int c) { return 1 << c; }
+int class_of(int n, int candidate_samples) {
+    if (n <= 16 && candidate_samples <= 16) return 0;
+    return n <= 32 ? 1 : n <= 64 ? 2 : n <= 128 ? 3 : 4;
+}
+int opl_of_class(int c) { return c == 0 ? 1 : 1 << (c - 1); }
+int kind_of_class(int c) { return c == 0 ? kTunePairKind : opl_of_class(c); }
 
 // First-fit allocator of [0, capacity) ranges with coalescing on release.
 struct RangeAlloc {
@@ -196,9 +203,10 @@ struct Server {
     void place(const ReqPtr& q);
     void select_round();
     void rebuild_items();
-    int blocks_for(int cls, bool general, uint32_t slot_bytes, int wpb, size_t items);
+    int blocks_for(int cls, bool general, uint32_t slot_bytes, int wpb, int rpw, size_t items);
     void round(bool& any_tempering);
-    void retire(const ReqPtr& q, const JobOut& o, double t_host, uint64_t stamp, int state);
+    void retire(const ReqPtr& q, const JobOut& o, double t_host, uint64_t stamp, int state, const VerifyStats& vs);
+    DeviceVerifier verifier;   // retiring requests' W, checked on the tensor cores
     void checkpoint(const ReqPtr& q, const JobOut& o, bool want_best, size_t nsaves);
     void finish_locked(const ReqPtr& q, int state);
     void fail_all(const std::string& msg);
@@ -402,7 +410,7 @@ void Server::rebuild_items() {
     }
     for (int s : order) {
         const ReqPtr& q = slot_req[s];
-        const int c = class_of(q->spec.n);
+        const int c = class_of(q->spec.n, q->job.candidate_samples);
         for (int r = 0; r < q->spec.replicas; ++r) items_host[c].push_back((uint32_t)(q->rep_begin + r));
         class_slot[c] = std::max(class_slot[c], anneal_slot_bytes(q->spec.n, q->job.m, opl_of_class(c)));
         class_general[c] = class_general[c] || q->job.general != 0;
@@ -415,20 +423,22 @@ void Server::rebuild_items() {
     items_dirty = false;
 }
 
-int Server::blocks_for(int cls, bool general, uint32_t slot_bytes, int wpb, size_t items) {
-    const auto key = std::make_pair((cls * 64 + wpb) * 2 + (general ? 1 : 0), slot_bytes);
+int Server::blocks_for(int cls, bool general, uint32_t slot_bytes, int wpb, int rpw, size_t items) {
+    const auto key = std::make_pair(((cls * 64 + wpb) * 2 + (general ? 1 : 0)) * 4 + rpw, slot_bytes);
     auto it = per_sm_cache.find(key);
     int per_sm = 0;
     if (it == per_sm_cache.end()) {
-        check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, anneal_kernel_fn(opl_of_class(cls), general),
-                                                                 32 * wpb, (size_t)wpb * slot_bytes),
+        check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                       &per_sm, anneal_kernel_fn(opl_of_class(cls), general, rpw), 32 * wpb,
+                       (size_t)wpb * rpw * slot_bytes),
                    "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
         per_sm_cache[key] = per_sm;
     } else {
         per_sm = it->second;
     }
     if (per_sm < 1) throw std::length_error("CUDA anneal kernel has zero occupancy for this request mix");
-    const int want = (int)((items + wpb - 1) / wpb);
+    const int groups = wpb * rpw;
+    const int want = (int)((items + groups - 1) / groups);
     return std::max(1, std::min(want, per_sm * sms));
 }
 
@@ -441,17 +451,20 @@ void Server::round(bool& any_tempering) {
     check_cuda(cudaMemsetAsync(d_counters, 0, sizeof(uint32_t) * kClasses, stream), "reset work counters");
     // per class: warps per block, CTAs, and chunks per replica (a class with
     // more replicas than its resident warps runs chunked, as batches do)
-    int cls_wpb[kClasses] = {}, cls_blocks[kClasses] = {};
+    int cls_wpb[kClasses] = {}, cls_blocks[kClasses] = {}, cls_rpw[kClasses] = {};
     uint32_t cls_chunks[kClasses] = {};
     bool any_chunked = false;
     for (int c = 0; c < kClasses; ++c) {
         if (items_host[c].empty()) continue;
-        int wpb = cfg.warps_per_block > 0 ? cfg.warps_per_block
-                                          : tuned_warps_per_block(opl_of_class(c), class_slot[c], cfg.device);
-        wpb = std::max(1, std::min(16, wpb));
+        TunedShape t = tuned_shape(kind_of_class(c), class_slot[c], cfg.device);
+        if (cfg.warps_per_block > 0) t.wpb = cfg.warps_per_block;
+        if (cfg.replicas_per_warp > 0) t.rpw = cfg.replicas_per_warp;
+        if (c != 0) t.rpw = 1;
+        const int wpb = std::max(1, std::min(16, t.wpb));
         cls_wpb[c] = wpb;
-        cls_blocks[c] = blocks_for(c, class_general[c], class_slot[c], wpb, items_host[c].size());
-        cls_chunks[c] = choose_chunks((uint32_t)items_host[c].size(), (uint32_t)(cls_blocks[c] * wpb));
+        cls_rpw[c] = t.rpw;
+        cls_blocks[c] = blocks_for(c, class_general[c], class_slot[c], wpb, t.rpw, items_host[c].size());
+        cls_chunks[c] = choose_chunks((uint32_t)items_host[c].size(), (uint32_t)(cls_blocks[c] * wpb * t.rpw));
         if (cls_chunks[c] > (uint32_t)cfg.quantum_iters) cls_chunks[c] = 1;
         any_chunked = any_chunked || cls_chunks[c] > 1;
     }
@@ -484,7 +497,9 @@ void Server::round(bool& any_tempering) {
         a.pad = 0;
         a.chunks = cls_chunks[c];
         if (a.chunks > 1) a.chunk_done = d_chunk_done;
-        check_cuda(launch_anneal(a, opl_of_class(c), class_general[c], wpb, cls_blocks[c], st), "launch anneal_kernel");
+        a.chunk_wait_ns = chunk_wait_limit_ns();
+        check_cuda(launch_anneal(a, opl_of_class(c), class_general[c], wpb, cls_blocks[c], st, cls_rpw[c]),
+                   "launch anneal_kernel");
         if (nclass > 1) {
             check_cuda(cudaEventRecord(join[c], st), "cudaEventRecord");
             check_cuda(cudaStreamWaitEvent(stream, join[c], 0), "cudaStreamWaitEvent");
@@ -509,17 +524,18 @@ void Server::round(bool& any_tempering) {
     ++stats.rounds;
 }
 
-// Engine thread: read back the chosen W, verify it, free the request's
-// device resources.
-void Server::retire(const ReqPtr& q, const JobOut& o, double t_host, uint64_t stamp, int state) {
-    const int n = q->spec.n, w = q->spec.w;
+// Engine thread: read back the chosen W, take its score and exact check
+// from the round's device verification (vs), free the request's device
+// resources.
+void Server::retire(const ReqPtr& q, const JobOut& o, double t_host, uint64_t stamp, int state,
+                    const VerifyStats& vs) {
+    const int n = q->spec.n;
     std::vector<int8_t> W((size_t)n * n);
     check_cuda(cudaMemcpy(W.data(), d_best + (size_t)q->slot * kBestStride, W.size(), cudaMemcpyDeviceToHost),
                "read request best state");
-    int64_t st[4] = {0, 0, 0, 0};
-    xw_score(n, w, W.data(), st);
+    const int64_t st[2] = {vs.score, vs.conflicts};
     const bool solved = o.first_solver >= 0;
-    const bool verified = solved && xw_verify(n, w, W.data()) == 3;
+    const bool verified = solved && vs.exact == 1;
     XwJob zero;
     std::memset(&zero, 0, sizeof zero);
     zero.done = 1;
@@ -706,20 +722,35 @@ void Server::engine_loop() {
             std::vector<int> keep;
             keep.reserve(active.size());
             const std::vector<int> current(active);
+            std::vector<std::pair<int, int>> leaving;   // slot, final state
             for (int s : current) {
-                const ReqPtr q = slot_req[s];
+                const ReqPtr& q = slot_req[s];
                 const JobOut& o = h_out[s];
                 const uint64_t budget = q->job.budget_iters;
                 const bool out_of_budget = budget && o.iters >= budget;
                 const bool out_of_time = q->params.max_seconds > 0.0 && t_host - q->t_admit >= q->params.max_seconds;
                 if (o.first_solver >= 0 || o.err) {
-                    retire(q, o, t_host, stamp, XW_REQ_DONE);
+                    leaving.push_back({s, XW_REQ_DONE});
                 } else if (cancel_flag[s]) {
-                    retire(q, o, t_host, stamp, XW_REQ_CANCELLED);
+                    leaving.push_back({s, XW_REQ_CANCELLED});
                 } else if (out_of_budget || out_of_time) {
-                    retire(q, o, t_host, stamp, XW_REQ_DONE);
+                    leaving.push_back({s, XW_REQ_DONE});
                 } else {
                     keep.push_back(s);
+                }
+            }
+            if (!leaving.empty()) {
+                // the round's retiring W, rescored and checked in one batch
+                std::vector<VerifyItem> items;
+                for (const auto& lv : leaving) {
+                    const ReqPtr& q = slot_req[lv.first];
+                    items.push_back({d_best + (size_t)q->slot * kBestStride, q->spec.n, q->spec.w});
+                }
+                std::vector<VerifyStats> vs;
+                verifier.run(items, stream, vs);
+                for (size_t k = 0; k < leaving.size(); ++k) {
+                    const ReqPtr q = slot_req[leaving[k].first];
+                    retire(q, h_out[leaving[k].first], t_host, stamp, leaving[k].second, vs[k]);
                 }
             }
             active.swap(keep);
@@ -734,14 +765,10 @@ void Server::start() {
     cudaDeviceProp props{};
     check_cuda(cudaGetDeviceProperties(&props, cfg.device), "cudaGetDeviceProperties");
     sms = props.multiProcessorCount;
-    int optin = 0;
-    check_cuda(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, cfg.device),
-               "cudaDeviceGetAttribute max opt-in shared memory");
     for (int c = 0; c < kClasses; ++c)
         for (bool general : {false, true})
-            check_cuda(cudaFuncSetAttribute(anneal_kernel_fn(opl_of_class(c), general),
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, optin),
-                       "cudaFuncSetAttribute max dynamic shared memory");
+            for (int rpw = 1; rpw <= (c == 0 ? 2 : 1); ++rpw)
+                raise_smem_limit(anneal_kernel_fn(opl_of_class(c), general, rpw), cfg.device);
     if (cfg.max_active_replicas <= 0) {
         // four waves of the resident warps at the order-32 slot: enough work
         // per round to keep every SM busy through the round's tail
@@ -901,6 +928,8 @@ int32_t xw_server_create(const xw_server_config* c, xw_server** out) {
     if (cfg.max_replica_ids < 1) return fail_with(XW_ERR_INVALID, "server replica ids must be positive");
     if (cfg.warps_per_block < 0 || cfg.warps_per_block > 16)
         return fail_with(XW_ERR_INVALID, "CUDA warps per block must be in [0, 16]");
+    if (cfg.replicas_per_warp < 0 || cfg.replicas_per_warp > 2)
+        return fail_with(XW_ERR_INVALID, "replicas per warp must be 0, 1 or 2");
     if (cfg.arena_bytes < 4096) return fail_with(XW_ERR_INVALID, "server arena must be at least 4 KiB");
     if (cfg.schedule != XW_SCHED_ALL && cfg.schedule != XW_SCHED_LEAST_ATTAINED)
         return fail_with(XW_ERR_INVALID, "server schedule must be XW_SCHED_ALL or XW_SCHED_LEAST_ATTAINED");
