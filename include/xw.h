@@ -514,6 +514,54 @@ int32_t xw_server_get_stats(xw_server* s, xw_server_stats* out);
  * device memory. */
 void xw_server_destroy(xw_server* s);
 
+/* ---- the CPU annealer ------------------------------------------------- */
+/* The reference's CPU tool xweigh (src/xweigh_main.cpp, engine
+ * src/xweigh_anneal.hpp:909-1291): one worker thread per core, each
+ * annealing its own state, a parallel-tempering ladder over the workers
+ * when there are two or more, the monitor's exchanges and best-matrix
+ * writes.  The fallback for hosts without a B200.  xw_cpu_params mirrors
+ * xweigh::Params (xweigh_anneal.hpp:42-67) field for field, without the
+ * Windows pinning switches. */
+typedef struct xw_cpu_params {
+    int32_t threads;              /* worker threads (default: hardware threads) */
+    int32_t tempering;            /* 1: parallel tempering for two or more workers */
+    uint64_t seed;                /* 0 = random_device */
+    double max_seconds;
+    double save_interval;
+    double sign_fraction;
+    double greedy_fraction;
+    int32_t candidate_samples;
+    double target_fraction;
+    int32_t target_samples;
+    int32_t exchange_interval;    /* moves per worker between exchanges */
+    double t_init;                /* 0 = calibrate */
+    double t_min;
+    double cooling;
+    int32_t moves_per_cool;
+    int32_t stuck_threshold;
+    double reheat;
+    double reseed_factor;
+} xw_cpu_params;
+
+typedef struct xw_cpu_result {
+    int64_t score, conflicts;     /* of the best W */
+    int32_t solved, verified;
+    uint64_t moves;
+    double seconds;               /* search time */
+    double t_init;                /* the (calibrated) initial temperature */
+    int32_t threads;
+    int32_t reserved;
+} xw_cpu_result;
+
+void xw_cpu_params_default(xw_cpu_params* p);
+/* run_annealer (xweigh_anneal.hpp:1106-1291) from `start` (nullable:
+ * State::random_start with the seed), with the reference's log lines through
+ * `log`, best-matrix writes through `checkpoint` every save_interval, and
+ * xw_request_stop as the stop flag.  best_out (nullable) receives the best
+ * W, column-major. */
+int32_t xw_cpu_run(int32_t n, int32_t w, const xw_cpu_params* p, const int8_t* start, xw_log_fn log,
+                   xw_checkpoint_fn checkpoint, void* user, xw_cpu_result* out, int8_t* best_out);
+
 /* ---- annealing without device allocation ------------------------------ */
 /* No counterpart in the reference: an entry point for callers that cannot
  * call cudaMalloc -- hosts whose device memory belongs to their own pool

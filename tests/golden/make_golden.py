@@ -3,7 +3,8 @@
 Run in a container that has the reference tree (read-only) after
 `make -C oracle` has built oracle/_ref/ from it:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            (every fixture)
+    python tests/golden/make_golden.py cpu_cli    (cpu_cli.json alone)
 
 Every fixture here comes from executing flinty-mathematics/xtax code:
 oracle/_ref/ref_harness (a driver around src/xweigh_anneal.hpp),
@@ -191,9 +192,63 @@ def cuda_cli_nogpu():
     return out
 
 
+def cpu_cli():
+    """The reference CPU xweigh CLI: option validation, existence checks,
+    the Sylvester construction and argument errors (no timing in their
+    output), and one-thread runs that solve, whose trajectories are
+    deterministic: the final W, the move count of the done line, the start
+    line and the closing lines."""
+    errors = [
+        ["10", "9", "--sign-fraction", "2"],
+        ["10", "9", "--threads", "0"],
+        ["10", "9", "--candidate-samples", "0"],
+        ["10", "9", "--target-samples", "0"],
+        ["10", "9", "--cooling", "1"],
+        ["10", "9", "--t-min", "0"],
+        ["10", "9", "--reseed-factor", "0.5"],
+        ["10", "9", "--exchange-interval", "0"],
+        ["9", "10"],
+        ["6", "6"],
+        ["7", "5"],
+        ["14", "7"],
+        ["10"],
+        ["10", "9", "--bogus", "3"],
+        ["abc", "9"],
+    ]
+    out = {"errors": [], "sylvester": [], "runs": []}
+    for args in errors:
+        r = subprocess.run([os.path.join(REF, "xweigh")] + args + ["-o", "/tmp/xw_golden_cpu.csv"],
+                           capture_output=True, text=True, timeout=60)
+        out["errors"].append({"args": args, "returncode": r.returncode, "stdout": r.stdout, "stderr": r.stderr})
+    for args in (["16", "4"], ["8", "8"], ["12", "4", "-t", "2"]):
+        outp = "/tmp/xw_golden_cpu_syl.csv"
+        r = subprocess.run([os.path.join(REF, "xweigh")] + args + ["-o", outp], capture_output=True, text=True,
+                           timeout=60)
+        lines = [l for l in r.stdout.splitlines() if not l.startswith("[init]")]
+        out["sylvester"].append({"args": args, "returncode": r.returncode, "stdout_lines": lines,
+                                 "csv": open(outp).read()})
+    for n, w, seed, extra in [(10, 9, 4, []), (10, 9, 5, []), (10, 9, 6, ["--no-tempering"]),
+                              (12, 11, 2, []), (10, 9, 7, ["--t-init", "3", "--sign-fraction", "0.3"])]:
+        outp = "/tmp/xw_golden_cpu_run.csv"
+        r = subprocess.run([os.path.join(REF, "xweigh"), str(n), str(w), "-t", "1", "--seed", str(seed),
+                            "-o", outp] + extra, capture_output=True, text=True, timeout=600)
+        lines = r.stdout.splitlines()
+        done = [l for l in lines if l.startswith("done moves=")][0]
+        start = [l for l in lines if l.startswith("[t=0s] start")][0]
+        out["runs"].append({"n": n, "w": w, "seed": seed, "extra": extra, "returncode": r.returncode,
+                            "moves": int(done.split()[1].split("=")[1]), "start_line": start,
+                            "csv": open(outp).read(),
+                            "final_lines": [l for l in lines if l.startswith(("Final", "Found", "No weighing", "W:"))
+                                            or (l and l[0] in "-01" and "," in l)]})
+    return out
+
+
 def main():
     if not os.path.exists(HARNESS):
         sys.exit("build oracle/_ref first: make -C oracle")
+    if sys.argv[1:] == ["cpu_cli"]:
+        dump("cpu_cli.json", cpu_cli())
+        return
     dump("starts.json", starts())
     dump("moves.json", moves())
     dump("compound.json", compound())
@@ -205,6 +260,7 @@ def main():
     dump("csv.json", csv_fixtures(solved))
     dump("cli_runs.json", cli_runs())
     dump("cuda_cli.json", cuda_cli_nogpu())
+    dump("cpu_cli.json", cpu_cli())
 
 
 if __name__ == "__main__":

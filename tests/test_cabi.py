@@ -159,7 +159,8 @@ def test_ctypes_structs_match_the_c_header(tmp_path):
                "xw_job_spec": X.JobSpec, "xw_job_result": X.JobResult, "xw_replica_state": X.ReplicaState,
                "xw_server_config": X.ServerConfig, "xw_request": X._Request,
                "xw_request_result": X.RequestResult, "xw_server_stats": X.ServerStats,
-               "xw_escape_move": X.EscapeMove, "xw_launch_class": X.LaunchClass}
+               "xw_escape_move": X.EscapeMove, "xw_launch_class": X.LaunchClass, "xw_cpu_params": X.CpuParams,
+               "xw_cpu_result": X.CpuResult}
     src = tmp_path / "sizes.c"
     src.write_text('#include <stdio.h>\n#include "xw.h"\nint main(void) {\n' +
                    "".join(f'    printf("%zu\\n", sizeof({k}));\n' for k in structs) + "    return 0;\n}\n")

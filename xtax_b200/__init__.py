@@ -108,6 +108,23 @@ class LaunchClass(C.Structure):
                 ("warps_per_replica", C.c_int32)]
 
 
+class CpuParams(C.Structure):
+    """xw_cpu_params: xweigh::Params of the CPU annealer."""
+    _fields_ = [("threads", C.c_int32), ("tempering", C.c_int32), ("seed", C.c_uint64),
+                ("max_seconds", C.c_double), ("save_interval", C.c_double), ("sign_fraction", C.c_double),
+                ("greedy_fraction", C.c_double), ("candidate_samples", C.c_int32),
+                ("target_fraction", C.c_double), ("target_samples", C.c_int32),
+                ("exchange_interval", C.c_int32), ("t_init", C.c_double), ("t_min", C.c_double),
+                ("cooling", C.c_double), ("moves_per_cool", C.c_int32), ("stuck_threshold", C.c_int32),
+                ("reheat", C.c_double), ("reseed_factor", C.c_double)]
+
+
+class CpuResult(C.Structure):
+    _fields_ = [("score", C.c_int64), ("conflicts", C.c_int64), ("solved", C.c_int32), ("verified", C.c_int32),
+                ("moves", C.c_uint64), ("seconds", C.c_double), ("t_init", C.c_double), ("threads", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
 class ServerConfig(C.Structure):
     """xw_server_config: the serving loop's device, round length and capacities."""
     _fields_ = [("device", C.c_int32), ("quantum_iters", C.c_int32), ("max_requests", C.c_int32),
@@ -203,6 +220,9 @@ def lib():
                                             P(C.c_uint8)]),
             "xw_batch_shape": (i32, [C.c_void_p, P(i32), P(i32), P(i32)]),
             "xw_batch_classes": (i32, [C.c_void_p, P(LaunchClass), i32, P(i32)]),
+            "xw_cpu_params_default": (None, [P(CpuParams)]),
+            "xw_cpu_run": (i32, [i32, i32, P(CpuParams), P(i8), LOG_FN, CHECKPOINT_FN, C.c_void_p, P(CpuResult),
+                                 P(i8)]),
             "xw_batch_restart": (i32, [C.c_void_p, i32, P(i32)]),
             "xw_batch_bytes": (i32, [C.c_void_p, P(u64), P(u64)]),
             "xw_batch_destroy": (None, [C.c_void_p]),
@@ -692,6 +712,24 @@ def autotune(jobs, params: Params, iters=2000):
     wpb, ms = C.c_int32(), C.c_float()
     _check(lib().xw_autotune(specs, len(jobs), C.byref(params.to_c()), iters, C.byref(wpb), C.byref(ms)))
     return wpb.value, ms.value
+
+
+def cpu_run(n, w, start=None, log=None, **params):
+    """xw_cpu_run: the CPU annealer (the reference's xweigh engine) with
+    xweigh::Params fields as keywords; returns (CpuResult, best W
+    column-major)."""
+    p = CpuParams()
+    lib().xw_cpu_params_default(C.byref(p))
+    for k, v in params.items():
+        setattr(p, k, v)
+    best = np.zeros(n * n, dtype=np.int8)
+    st = None if start is None else np.ascontiguousarray(start, dtype=np.int8).reshape(-1)
+    lines = []
+    cb = LOG_FN(lambda line, _u: (log or lines.append)(line.decode()))
+    res = CpuResult()
+    _check(lib().xw_cpu_run(n, w, C.byref(p), None if st is None else _i8(st), cb, CHECKPOINT_FN(0), None,
+                            C.byref(res), _i8(best)))
+    return res, best
 
 
 def escape_scan(n, w, W_colmajor, limit):

@@ -1,5 +1,6 @@
-// xw_cli.cpp -- the xweigh_cuda command line, a drop-in for
-// src/xweigh_cuda_main.cpp of flinty-mathematics/xtax on top of libxw.
+// xw_cli.cpp -- the command lines of libxw: xweigh_cuda, a drop-in for
+// src/xweigh_cuda_main.cpp of flinty-mathematics/xtax, and (built with
+// XW_CLI_CPU) xweigh, a drop-in for src/xweigh_main.cpp, the CPU annealer.
 //
 // Same positional arguments, options, defaults, validation messages,
 // existence checks (impossibility_reason), Sylvester short-circuit, output
@@ -8,8 +9,10 @@
 // same message and exits with the same code (105 validation, 106 missing
 // argument, 109 unexpected argument), followed by
 // "Run with --help for more information.".
+#include <algorithm>
 #include <atomic>
 #include <cctype>
+#include <chrono>
 #include <cerrno>
 #include <climits>
 #include <cmath>
@@ -84,7 +87,7 @@ struct Option {
     std::vector<std::string> names;
     std::string help;
     std::function<void(const std::string&)> set;
-    bool flag = false;
+    bool flag = false;   // takes no value (set is called with "")
 };
 
 bool file_exists(const std::string& p) {
@@ -174,6 +177,83 @@ struct CliState {
     std::string output = "best_W.csv";
 };
 
+// The shared parser: options by name (--name value, --name=value, flags),
+// then the positionals n and w.  False after printing --help.
+bool parse_args(int argc, char** argv, std::vector<Option>& opts, const char* title, long long& order,
+                long long& weight) {
+    std::vector<std::string> positional;
+    bool have_n = false, have_w = false;
+    std::map<std::string, Option*> by_name;
+    for (auto& o : opts)
+        for (auto& nm : o.names) by_name[nm] = &o;
+
+    std::vector<std::string> extras;
+    for (int i = 1; i < argc; ++i) {
+        std::string a = argv[i];
+        if (a == "-h" || a == "--help") {
+            std::printf("%s\nUsage: %s [OPTIONS] n w\n\n"
+                        "Positionals:\n  n INT:INT in [1 - 32767] REQUIRED\n                              Matrix order n\n"
+                        "  w INT:INT in [1 - 32767] REQUIRED\n                              Matrix weight w\n\nOptions:\n"
+                        "  -h,--help                   Print this help message and exit\n",
+                        title, argv[0]);
+            for (auto& o : opts) {
+                std::string names;
+                for (auto& nm : o.names) names += (names.empty() ? "" : ",") + nm;
+                std::printf("  %-27s %s\n", names.c_str(), o.help.c_str());
+            }
+            return false;
+        }
+        if (a.size() > 1 && a[0] == '-' && !(a.size() > 1 && (std::isdigit((unsigned char)a[1]) || a[1] == '.'))) {
+            std::string name = a, value;
+            bool inline_value = false;
+            const size_t eq = a.find('=');
+            if (a.rfind("--", 0) == 0 && eq != std::string::npos) {
+                name = a.substr(0, eq);
+                value = a.substr(eq + 1);
+                inline_value = true;
+            }
+            auto it = by_name.find(name);
+            if (it == by_name.end()) {
+                extras.push_back(a);
+                continue;
+            }
+            if (it->second->flag) {
+                if (inline_value) throw ArgError{107, name + ": flag does not take a value"};
+            } else if (!inline_value) {
+                if (i + 1 >= argc) throw ArgError{106, name + " requires 1 argument(s) but received 0"};
+                value = argv[++i];
+            }
+            it->second->set(value);
+            continue;
+        }
+        if (positional.size() < 2) positional.push_back(a);
+        else extras.push_back(a);
+    }
+    // positionals n then w, each checked against CLI::Range(1, MAX_ORDER)
+    for (size_t k = 0; k < positional.size(); ++k) {
+        const std::string& v = positional[k];
+        long long x;
+        const char* nm = k == 0 ? "n" : "w";
+        if (!parse_int(v, x) || x < 1 || x > 32767)
+            throw ArgError{105, std::string(nm) + ": Value " + v + " not in range [1 - 32767]"};
+        (k == 0 ? order : weight) = x;
+        (k == 0 ? have_n : have_w) = true;
+    }
+    if (!extras.empty()) {
+        // reported last-seen first
+        std::string msg = extras.size() == 1 ? "The following argument was not expected:"
+                                             : "The following arguments were not expected:";
+        for (auto it = extras.rbegin(); it != extras.rend(); ++it) msg += " " + *it;
+        throw ArgError{109, msg};
+    }
+    if (!have_n) throw ArgError{106, "n is required"};
+    if (!have_w) throw ArgError{106, "w is required"};
+    return true;
+
+}
+
+
+
 void log_line(const char* line, void*) {
     std::printf("%s\n", line);
     std::fflush(stdout);
@@ -185,13 +265,11 @@ void checkpoint(const int8_t* best, int32_t n, void* user) {
         std::fprintf(stderr, "Warning: %s\n", xw_last_error());
 }
 
-int run(int argc, char** argv) {
+[[maybe_unused]] int run(int argc, char** argv) {
     xw_params p;
     xw_params_default(&p);
     CliState state;
     std::string start_file;
-    std::vector<std::string> positional;
-    bool have_n = false, have_w = false;
     long long order = 0, weight = 0;
 
     std::vector<Option> opts;
@@ -280,70 +358,8 @@ int run(int argc, char** argv) {
     add({"--start-kind"}, "0 regular random start, 1 row-only random start", int_opt("--start-kind", &p.start_kind));
     add({"--warps-per-block"}, "Replica warps per CTA (0 = autotuned)", int_opt("--warps-per-block", &p.warps_per_block));
 
-    std::map<std::string, Option*> by_name;
-    for (auto& o : opts)
-        for (auto& nm : o.names) by_name[nm] = &o;
-
-    std::vector<std::string> extras;
-    for (int i = 1; i < argc; ++i) {
-        std::string a = argv[i];
-        if (a == "-h" || a == "--help") {
-            std::printf("xweigh_cuda shared-memory weighing-matrix annealer\nUsage: %s [OPTIONS] n w\n\n"
-                        "Positionals:\n  n INT:INT in [1 - 32767] REQUIRED\n                              Matrix order n\n"
-                        "  w INT:INT in [1 - 32767] REQUIRED\n                              Matrix weight w\n\nOptions:\n"
-                        "  -h,--help                   Print this help message and exit\n",
-                        argv[0]);
-            for (auto& o : opts) {
-                std::string names;
-                for (auto& nm : o.names) names += (names.empty() ? "" : ",") + nm;
-                std::printf("  %-27s %s\n", names.c_str(), o.help.c_str());
-            }
-            return 0;
-        }
-        if (a.size() > 1 && a[0] == '-' && !(a.size() > 1 && (std::isdigit((unsigned char)a[1]) || a[1] == '.'))) {
-            std::string name = a, value;
-            bool inline_value = false;
-            const size_t eq = a.find('=');
-            if (a.rfind("--", 0) == 0 && eq != std::string::npos) {
-                name = a.substr(0, eq);
-                value = a.substr(eq + 1);
-                inline_value = true;
-            }
-            auto it = by_name.find(name);
-            if (it == by_name.end()) {
-                extras.push_back(a);
-                continue;
-            }
-            if (!inline_value) {
-                if (i + 1 >= argc) throw ArgError{106, name + " requires 1 argument(s) but received 0"};
-                value = argv[++i];
-            }
-            it->second->set(value);
-            continue;
-        }
-        if (positional.size() < 2) positional.push_back(a);
-        else extras.push_back(a);
-    }
-    // positionals n then w, each checked against CLI::Range(1, MAX_ORDER)
-    for (size_t k = 0; k < positional.size(); ++k) {
-        const std::string& v = positional[k];
-        long long x;
-        const char* nm = k == 0 ? "n" : "w";
-        if (!parse_int(v, x) || x < 1 || x > 32767)
-            throw ArgError{105, std::string(nm) + ": Value " + v + " not in range [1 - 32767]"};
-        (k == 0 ? order : weight) = x;
-        (k == 0 ? have_n : have_w) = true;
-    }
-    if (!extras.empty()) {
-        // reported last-seen first
-        std::string msg = extras.size() == 1 ? "The following argument was not expected:"
-                                             : "The following arguments were not expected:";
-        for (auto it = extras.rbegin(); it != extras.rend(); ++it) msg += " " + *it;
-        throw ArgError{109, msg};
-    }
-    if (!have_n) throw ArgError{106, "n is required"};
-    if (!have_w) throw ArgError{106, "w is required"};
-
+    if (!parse_args(argc, argv, opts, "xweigh_cuda shared-memory weighing-matrix annealer", order, weight))
+        return 0;
     const int n = (int)order, w = (int)weight;
     if (w > n) {
         std::fprintf(stderr, "Error: w must not exceed n\n");
@@ -407,12 +423,178 @@ int run(int argc, char** argv) {
     return finish(best, n, w, state.output) ? 0 : 1;
 }
 
+// valid_params, xweigh_main.cpp:54-88
+std::string valid_cpu_params(const xw_cpu_params& p) {
+    if (p.threads < 1) return "--threads must be positive";
+    if (p.max_seconds < 0.0) return "--max-seconds must be nonnegative";
+    if (p.save_interval < 0.0) return "--save-interval must be nonnegative";
+    if (p.sign_fraction < 0.0 || p.sign_fraction > 1.0) return "--sign-fraction must be in [0, 1]";
+    if (p.greedy_fraction < 0.0 || p.greedy_fraction > 1.0) return "--greedy-fraction must be in [0, 1]";
+    if (p.target_fraction < 0.0 || p.target_fraction > 1.0) return "--target-fraction must be in [0, 1]";
+    if (p.candidate_samples < 1) return "--candidate-samples must be positive";
+    if (p.target_samples < 1) return "--target-samples must be positive";
+    if (p.exchange_interval < 1) return "--exchange-interval must be positive";
+    if (p.t_init < 0.0) return "--t-init must be nonnegative";
+    if (p.t_min <= 0.0) return "--t-min must be positive";
+    if (p.cooling <= 0.0 || p.cooling >= 1.0) return "--cooling must be in (0, 1)";
+    if (p.moves_per_cool < 1) return "--moves-per-cool must be positive";
+    if (p.stuck_threshold < 1) return "--stuck-threshold must be positive";
+    if (p.reheat <= 0.0) return "--reheat must be positive";
+    if (p.reseed_factor < 1.0) return "--reseed-factor must be at least 1";
+    return {};
+}
+
+// The xweigh command line (xweigh_main.cpp:88-270) over xw_cpu_run.
+[[maybe_unused]] int run_cpu(int argc, char** argv) {
+    xw_cpu_params p;
+    xw_cpu_params_default(&p);
+    CliState state;
+    std::string start_file;
+    long long order = 0, weight = 0;
+    std::vector<Option> opts;
+    auto add = [&](std::vector<std::string> names, std::string help, std::function<void(const std::string&)> set,
+                   bool flag = false) {
+        opts.push_back(Option{std::move(names), std::move(help), std::move(set), flag});
+    };
+    auto conv_err = [](const std::string& name, const std::string& v) {
+        return ArgError{107, name + ": Value " + v + " could not be converted"};
+    };
+    auto int_opt = [&](const std::string& name, int32_t* dst) {
+        return [=](const std::string& v) {
+            long long x;
+            if (!parse_int(v, x) || x < INT32_MIN || x > INT32_MAX) throw conv_err(name, v);
+            *dst = (int32_t)x;
+        };
+    };
+    auto dbl_opt = [&](const std::string& name, double* dst) {
+        return [=](const std::string& v) {
+            double x;
+            if (!parse_double(v, x)) throw conv_err(name, v);
+            *dst = x;
+        };
+    };
+    add({"-o", "--out"}, "Output CSV for the best matrix", [&](const std::string& v) { state.output = v; });
+    add({"--start"}, "Start from a complete fixed-weight ternary CSV", [&](const std::string& v) {
+        if (!file_exists(v)) throw ArgError{105, "--start: File does not exist: " + v};
+        start_file = v;
+    });
+    add({"-t", "--threads"}, "Number of worker threads (default: physical cores)", int_opt("--threads", &p.threads));
+    // physical and logical processors count alike on this host, and workers
+    // are not pinned: both switches are accepted for the reference's scripts
+    add({"--use-hyperthreads"}, "Default to all logical processors (ignored with --threads)",
+        [&](const std::string&) {}, true);
+    add({"--no-pin"}, "Do not pin workers to physical cores on Windows", [&](const std::string&) {}, true);
+    add({"--seed"}, "Base RNG seed (0 = random_device)", [&](const std::string& v) {
+        uint64_t x;
+        if (!parse_uint64(v, x)) throw conv_err("--seed", v);
+        p.seed = x;
+    });
+    add({"--max-seconds"}, "Wall-clock search budget (0 = until solved or interrupted)",
+        dbl_opt("--max-seconds", &p.max_seconds));
+    add({"--save-interval"}, "Minimum seconds between best-matrix writes", dbl_opt("--save-interval", &p.save_interval));
+    add({"--sign-fraction"}, "Probability of proposing a sign flip instead of a support switch",
+        dbl_opt("--sign-fraction", &p.sign_fraction));
+    add({"--greedy-fraction"}, "Probability of selecting the best of sampled candidate moves",
+        dbl_opt("--greedy-fraction", &p.greedy_fraction));
+    add({"--candidate-samples"}, "Candidate count for a sampled greedy move",
+        int_opt("--candidate-samples", &p.candidate_samples));
+    add({"--target-fraction"}, "Probability of targeting a high-residual row",
+        dbl_opt("--target-fraction", &p.target_fraction));
+    add({"--target-samples"}, "Tournament size for high-residual row selection",
+        int_opt("--target-samples", &p.target_samples));
+    add({"--tempering"}, "Parallel tempering for two or more workers", [&](const std::string&) { p.tempering = 1; },
+        true);
+    add({"--no-tempering"}, "Independent annealing workers", [&](const std::string&) { p.tempering = 0; }, true);
+    add({"--exchange-interval"}, "Approximate moves per worker between replica exchanges",
+        int_opt("--exchange-interval", &p.exchange_interval));
+    add({"--t-init"}, "Initial temperature (0 = auto-calibrate)", dbl_opt("--t-init", &p.t_init));
+    add({"--t-min"}, "Minimum temperature", dbl_opt("--t-min", &p.t_min));
+    add({"--cooling"}, "Single-worker geometric cooling factor", dbl_opt("--cooling", &p.cooling));
+    add({"--moves-per-cool"}, "Single-worker moves between cooling steps",
+        int_opt("--moves-per-cool", &p.moves_per_cool));
+    add({"--stuck-threshold"}, "Single-worker moves without improvement before reheating",
+        int_opt("--stuck-threshold", &p.stuck_threshold));
+    add({"--reheat"}, "Fraction of initial temperature restored when stuck", dbl_opt("--reheat", &p.reheat));
+    add({"--reseed-factor"}, "Reseed from the best when this factor behind it",
+        dbl_opt("--reseed-factor", &p.reseed_factor));
+    if (!parse_args(argc, argv, opts, "xweigh unrestricted weighing-matrix annealer", order, weight)) return 0;
+
+    const int n = (int)order, w = (int)weight;
+    if (w > n) {
+        std::fprintf(stderr, "Error: w must not exceed n\n");
+        return 1;
+    }
+    const std::string err = valid_cpu_params(p);
+    if (!err.empty()) {
+        std::fprintf(stderr, "Error: %s\n", err.c_str());
+        return 1;
+    }
+    const std::string impossible = xw_impossibility_reason(n, w);
+    if (!impossible.empty()) {
+        std::fprintf(stderr, "Error: W(%d,%d) cannot exist: %s\n", n, w, impossible.c_str());
+        return 1;
+    }
+    if (n > XW_MAX_ORDER_CUDA) {
+        std::fprintf(stderr, "Error: orders above %d are outside this build\n", XW_MAX_ORDER_CUDA);
+        return 1;
+    }
+    if (p.seed == 0) p.seed = (uint64_t)std::random_device{}();
+    const auto t_init0 = std::chrono::steady_clock::now();
+    std::vector<int8_t> start((size_t)n * n);
+    const bool loaded = !start_file.empty();
+    const bool sylvester = !loaded && is_power_of_two(w) && n % w == 0;
+    if (loaded) {
+        if (xw_read_csv(start_file.c_str(), n, w, start.data()) != XW_OK) {
+            std::fprintf(stderr, "Error: %s\n", xw_last_error());
+            return 1;
+        }
+    } else if (sylvester) {
+        xw_sylvester(n, w, start.data());
+    } else if (xw_random_start(n, w, (uint32_t)p.seed, start.data()) != XW_OK) {
+        std::fprintf(stderr, "Error: %s\n", xw_last_error());
+        return 1;
+    }
+    const double init_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_init0).count();
+    // a reference worker's state: W twice, int16 Gram, int64 residuals,
+    // u16 minority lists (xweigh_anneal.hpp:185-190)
+    const int m = std::min(w, n - w);
+    const double worker_bytes = (double)n * n * 4 + 8.0 * n + 2.0 * n * m;
+    std::printf("[init] seconds=%g worker_mib=%g total_worker_mib=%g\n", init_s, worker_bytes / 1048576.0,
+                worker_bytes * p.threads / 1048576.0);
+    int64_t st[4];
+    xw_score(n, w, start.data(), st);
+    if (loaded)
+        std::printf("[start] loaded %s score=%lld conflicts=%lld\n", start_file.c_str(), (long long)st[0],
+                    (long long)st[1]);
+    else if (sylvester)
+        std::printf("[construct] using direct sum of Sylvester blocks\n");
+    std::vector<int8_t> best = start;
+    if (st[0] != 0) {
+        std::fflush(stdout);
+        xw_cpu_result res;
+        const int rc = xw_cpu_run(n, w, &p, start.data(), log_line, checkpoint, &state, &res, best.data());
+        if (rc != XW_OK) {
+            std::fprintf(stderr, "Error: %s\n", xw_last_error());
+            return 1;
+        }
+    }
+    if (xw_write_csv(state.output.c_str(), n, best.data()) != XW_OK) {
+        std::fprintf(stderr, "Error: %s\n", xw_last_error());
+        return 1;
+    }
+    return finish(best, n, w, state.output) ? 0 : 1;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
     std::signal(SIGINT, on_interrupt);
     try {
+#ifdef XW_CLI_CPU
+        return run_cpu(argc, argv);
+#else
         return run(argc, argv);
+#endif
     } catch (const ArgError& e) {
         std::fprintf(stderr, "%s\nRun with --help for more information.\n", e.message.c_str());
         return e.code;

@@ -238,6 +238,47 @@ int64_t CpuState::evaluate_score(const CpuMove& mv) const {
     return d;
 }
 
+void CpuState::evaluate(const CpuMove& mv, int64_t& score_delta, int64_t& conflict_delta) const {
+    int64_t ds = 0, dc = 0;
+    auto ab = [](int v) { return (int64_t)(v < 0 ? -v : v); };
+    auto cd = [](int o, int nw) { return (int64_t)(nw != 0) - (int64_t)(o != 0); };
+    if (mv.kind == 0) {
+        const int ch = -2 * at(mv.row1, mv.col1);
+        for (int o = 0; o < n_; ++o) {
+            if (o == mv.row1) continue;
+            const int old = gram_[(size_t)mv.row1 * n_ + o];
+            const int nw = old + ch * at(o, mv.col1);
+            ds += ab(nw) - ab(old);
+            dc += cd(old, nw);
+        }
+    } else {
+        const int v1 = at(mv.row1, mv.col1), v2 = at(mv.row2, mv.col2);
+        for (int o = 0; o < n_; ++o) {
+            if (o == mv.row1 || o == mv.row2) continue;
+            const int o1 = gram_[(size_t)mv.row1 * n_ + o], o2 = gram_[(size_t)mv.row2 * n_ + o];
+            const int n1 = o1 + v1 * (at(o, mv.col2) - at(o, mv.col1));
+            const int n2 = o2 + v2 * (at(o, mv.col1) - at(o, mv.col2));
+            ds += ab(n1) - ab(o1) + ab(n2) - ab(o2);
+            dc += cd(o1, n1) + cd(o2, n2);
+        }
+    }
+    score_delta = ds;
+    conflict_delta = dc;
+}
+
+void CpuState::apply_to_entries(std::vector<int8_t>& e, int n, const CpuMove& mv) {
+    auto at = [&](int r, int c) -> int8_t& { return e[(size_t)c * n + r]; };
+    if (mv.kind == 0) {
+        at(mv.row1, mv.col1) = (int8_t)-at(mv.row1, mv.col1);
+        return;
+    }
+    const int8_t v1 = at(mv.row1, mv.col1), v2 = at(mv.row2, mv.col2);
+    at(mv.row1, mv.col1) = 0;
+    at(mv.row2, mv.col2) = 0;
+    at(mv.row1, mv.col2) = v1;
+    at(mv.row2, mv.col1) = v2;
+}
+
 void CpuState::commit(const CpuMove& mv) {
     auto ab = [](int v) { return (int64_t)(v < 0 ? -v : v); };
     int64_t ds = 0, dc = 0;

@@ -49,6 +49,10 @@ public:
 
     bool propose(std::mt19937& rng, const CpuParams& p, bool targeted, CpuMove& mv) const;
     int64_t evaluate_score(const CpuMove& mv) const;
+    // State::evaluate (anneal.hpp:542-596): exact (score delta, conflict delta)
+    void evaluate(const CpuMove& mv, int64_t& score_delta, int64_t& conflict_delta) const;
+    // State::apply_to_entries: the move on a bare column-major W
+    static void apply_to_entries(std::vector<int8_t>& entries, int n, const CpuMove& mv);
     // commit_sign_flip / commit_support_switch (anneal.hpp:598-666): apply
     // the move, update the Gram, residuals, minority list, score, conflicts
     void commit(const CpuMove& mv);

@@ -96,6 +96,8 @@ namespace xw {
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
+const std::atomic<int>& stop_flag() { return g_stop; }
+
 bool needs_general_kernel(const xw_params& p) {
     if (p.move_set != 0) return true;
     if (p.objective == 1 || p.objective == 2) return true;
@@ -126,7 +128,10 @@ void raise_smem_limit(const void* fn, int device) {
     int optin = 0;
     check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device),
           "cudaDeviceGetAttribute max opt-in shared memory");
-    check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin),
+    // the opt-in maximum covers static and dynamic shared memory together
+    cudaFuncAttributes attr{};
+    check(cudaFuncGetAttributes(&attr, fn), "cudaFuncGetAttributes");
+    check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)attr.sharedSizeBytes),
           "cudaFuncSetAttribute max dynamic shared memory");
 }
 

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -17,6 +18,8 @@ std::string validate(int n, int w, const xw_params& p);
 // objective on some replica, or the within-row swap move set
 bool needs_general_kernel(const xw_params& p);
 void set_last_error(const std::string& msg);
+// the flag xw_request_stop sets
+const std::atomic<int>& stop_flag();
 // The least order that runs on the HBM-resident kernel: XW_MAX_N + 1, or
 // the value of XW_LARGE_MIN_ORDER in [1, XW_MAX_N + 1] (tests run small
 // orders through that kernel to compare it with the shared-memory one).

@@ -215,7 +215,10 @@ extern "C" int32_t xw_anneal_noalloc(int32_t n, int32_t w, const xw_params* p, i
     e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (e == cudaSuccess && (size_t)wpb * slot > (size_t)optin)
         return nfail(XW_ERR_CAPACITY, "xw_anneal_noalloc: the replicas' shared memory exceeds the device's limit");
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    cudaFuncAttributes attr{};
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&attr, fn);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)attr.sharedSizeBytes);
     if (e != cudaSuccess) return nfail(XW_ERR_CAPACITY, std::string("cudaFuncSetAttribute failed: ") + cudaGetErrorString(e));
     int per_sm = 0, sms = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * wpb, (size_t)wpb * slot);
