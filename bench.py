@@ -206,15 +206,14 @@ def make_params():
                     squared_objective_fraction=0.0, parity_objective_fraction=0.0, stop_on_solve=0)
 
 
-def algorithmic_smem_bytes(moves, cand_evals, n=N_ORDER, g=4):
-    """Shared-memory bytes a move needs at minimum: each evaluated candidate
-    reads k rows of (n-1) Gram entries (g bytes) and (n-1) W entries per
-    changed row; an accepted move writes 2k(n-1) Gram entries.  k = 1.5 for
-    this move mix (flips 1 row; switches and double flips 2 rows, a quarter
-    of the double flips on one row)."""
-    k = 1.5
-    reads = cand_evals * k * (n - 1) * (g + 1)
-    writes = moves * 0.5 * 2 * k * (n - 1) * g   # about half of the moves are accepted
+def algorithmic_smem_bytes(cand_evals, two_row_evals, accepted_rows, n=N_ORDER, g=4):
+    """Shared-memory bytes the moves need at minimum, from the move
+    statistics the kernel counts: each evaluated candidate reads, per row it
+    changes (one, or two for the counted two-row candidates), (n-1) Gram
+    entries of g bytes and (n-1) W entries; each row an accepted move
+    changes writes 2(n-1) Gram entries (the row and its mirror column)."""
+    reads = (cand_evals + two_row_evals) * (n - 1) * (g + 1)
+    writes = accepted_rows * 2 * (n - 1) * g
     return reads + writes
 
 
@@ -260,7 +259,7 @@ def ours(args):
             torch.distributed.barrier()
 
     step_ms, launch_ms = [], []
-    moves = evals = 0
+    moves = evals = evals2 = acc = acc_rows = 0
     barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
@@ -276,10 +275,14 @@ def ours(args):
             res = batch.results()
             moves += sum(r.moves for r, _ in res)
             evals += sum(r.candidate_evaluations for r, _ in res)
+            evals2 += sum(r.two_row_evaluations for r, _ in res)
+            acc += sum(r.accepted_moves for r, _ in res)
+            acc_rows += sum(r.accepted_rows for r, _ in res)
     torch.cuda.synchronize()
     barrier()
     total_ms = sum(step_ms)
-    (total_ms,), (moves, evals) = reduce_over_ranks(world, "cuda", [total_ms], [float(moves), float(evals)])
+    (total_ms,), (moves, evals, evals2, acc, acc_rows) = reduce_over_ranks(
+        world, "cuda", [total_ms], [float(moves), float(evals), float(evals2), float(acc), float(acc_rows)])
     value = moves / (total_ms / 1e3)
 
     # end to end: the C ABI whole-batch call with host buffers
@@ -318,14 +321,20 @@ def ours(args):
 
     anneal_launches = [ms for ms in launch_ms if ms > 0]
     avg_launch_ms = statistics.mean(anneal_launches)
-    per_launch_moves = moves / max(1, len(anneal_launches)) / world
-    per_launch_evals = evals / max(1, len(anneal_launches)) / world
-    alg_bytes = algorithmic_smem_bytes(per_launch_moves, per_launch_evals)
+    nl = max(1, len(anneal_launches)) * world
+    alg_bytes = algorithmic_smem_bytes(evals / nl, evals2 / nl, acc_rows / nl)
     sm_mhz = clocks.get("sm_mhz") or 1965.0
     smem_peak = 148 * 128 * sm_mhz * 1e6 / 1e9   # GB/s, nominal: 128 B/clk/SM
     achieved = alg_bytes / (avg_launch_ms / 1e3) / 1e9
     prof = load_profile_figure("traffic_bytes_per_launch")
     issue = load_profile_figure("issue_active_pct")
+    # instruction issue: the profiled warp instructions per replica iteration
+    # times the iterations per second, against one warp instruction per
+    # scheduler per cycle (148 SMs x 4 schedulers x median SM clock)
+    inst_per_iter = load_profile_figure("warp_instructions_per_iteration")
+    iters_per_launch = args.steps * INSTANCES * RUNGS * iters / max(1, len(anneal_launches))
+    issue_rate = inst_per_iter * iters_per_launch / (avg_launch_ms / 1e3) if inst_per_iter else None
+    issue_peak = 148 * 4 * sm_mhz * 1e6
     line = {
         "metric": METRIC, "value": value, "unit": "moves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -338,6 +347,11 @@ def ours(args):
         "roofline": {"bound": "smem", "achieved": achieved, "peak": smem_peak, "unit": "GB/s",
                      "frac": achieved / smem_peak, "traffic": int(prof) if prof else None,
                      "issue_active_pct_ncu": issue,
+                     "issue_frac": issue_rate / issue_peak if issue_rate else None,
+                     "warp_instructions_per_iteration_ncu": inst_per_iter,
+                     "move_statistics": {"candidate_evaluations": evals, "two_row_evaluations": evals2,
+                                         "accepted_moves": acc, "accepted_rows": acc_rows, "moves": moves,
+                                         "acceptance": acc / moves if moves else None},
                      "kernel": "anneal_kernel", "avg_launch_ms": avg_launch_ms,
                      "peak_source": "nominal 128 B/clk/SM x 148 SMs x median SM clock (no measured shared-memory peak)"},
         "clocks": clocks,

@@ -99,7 +99,7 @@ def test_a_chunk_wait_that_runs_out_flags_the_replica_and_skips_its_later_chunks
     chunk runs to its end, so the replica holds exactly its iterations, and
     the next batch (default bound) runs normally."""
     jobs = [{"n": 26, "w": 25, "seed": 17, "replicas": 1}]
-    p = X.Params(stop_on_solve=0, t_init=4.0, moves_per_launch=300000,
+    p = X.Params(stop_on_solve=0, t_init=4.0, moves_per_launch=300000, warps_per_replica=1,
                  squared_objective_fraction=0.0, parity_objective_fraction=0.0)
     monkeypatch.setenv("XW_CHUNKS", "3")
     monkeypatch.setenv("XW_CHUNK_WAIT_NS", "2000000")

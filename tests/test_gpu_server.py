@@ -268,9 +268,10 @@ def test_retired_requests_are_verified_on_the_device_as_on_the_host():
             req(36, 4, 34, 8, 200000), req(40, 39, 35, 4, 2000), req(70, 4, 36, 4, 200000),
             req(100, 99, 37, 2, 300), req(26, 25, 38, 16, 4000), req(150, 149, 39, 2, 100)]
     out, _ = serve(reqs)
+    states = [(r["n"], r["w"], res.state, res.status, res.error.decode()) for (res, _), r in zip(out, reqs)]
     for (res, W), r in zip(out, reqs):
         n, w = r["n"], r["w"]
-        assert res.state == X.REQ_DONE and res.status == X.XW_OK, (n, w)
+        assert res.state == X.REQ_DONE and res.status == X.XW_OK, states
         host = X.score(n, w, W)
         assert (res.score, res.conflicts) == (host[0], host[1]), (n, w)
         assert bool(res.verified) == (bool(res.solved) and X.verify(n, w, W) == 3), (n, w)

@@ -24,8 +24,10 @@ def test_autotune_records_and_applies_the_fastest_shape(tmp_path, monkeypatch):
     monkeypatch.delenv("XW_WARPS_PER_BLOCK", raising=False)
     wpb, ms = X.autotune(JOBS, params(), iters=500)
     assert wpb in (1, 2, 4, 8, 16) and ms > 0
+    # cache lines: kind (rows per lane), slot-byte class, warps per CTA,
+    # replicas per warp
     rows = [tuple(int(v) for v in line.split()) for line in (tmp_path / "tune.txt").read_text().splitlines()]
-    assert any(opl == 1 and w == wpb for opl, _, _, w in rows)
+    assert any(kind == 1 and w == wpb and rpw == 1 for kind, _, _, w, rpw in rows)
     b = X.Batch(JOBS, params(warps_per_block=0))
     assert b.shape()[0] == wpb
     b.close()

@@ -58,6 +58,14 @@ __device__ __forceinline__ unsigned group_mask() {
     else return 0xffffu << (threadIdx.x & 16);
 }
 
+// Move statistics in the replica header (accepted moves, the rows they
+// changed, two-row candidate evaluations); a build with XW_MOVE_STATS=0
+// leaves them at zero and drops their counting from the hot loop.
+#ifndef XW_MOVE_STATS
+#define XW_MOVE_STATS 1
+#endif
+constexpr bool kMoveStats = XW_MOVE_STATS != 0;
+
 // Metropolis thresholds kept per replica for objective increases 1..kThrTable.
 constexpr uint32_t kThrTable = 64;
 
@@ -544,6 +552,56 @@ __device__ __forceinline__ uint64_t globaltimer() {
     return t;
 }
 
+// Phase C: the hot-row tournaments of candidates 0..3 (hot_row,
+// xweigh_cuda.cu:291-300), 8 lanes (samples) per candidate with a segmented
+// maximum: one pass of a warp, two of a half-warp.  Returns the row of the
+// lane's candidate for lanes 0..3.
+template <int GW>
+__device__ __forceinline__ int coop_hot_row(const uint32_t* sDw, const int32_t* sRes, int bpc, int count, int ts,
+                                            bool coop, int n, uint64_t it, uint32_t stream, uint32_t k0,
+                                            uint32_t k1, int lane) {
+    const unsigned gm = group_mask<GW>();
+    if constexpr (GW == 32) {
+        int hot_key = 0;
+        if (coop) {
+            const int c = lane >> 3, s = lane & 7;
+            if (c < count && s < ts) {
+                const uint32_t wd = sDw[(1 + c * bpc + 4 + (s >> 2)) * 4 + (s & 3)];
+                const uint32_t row =
+                    draw_index(wd, (uint32_t)n, cand_slot(c, 4 + (s >> 2)), it, stream, k0, k1, s & 3);
+                hot_key = (sRes[row] << 13) | ((31 - s) << 8) | (int)row;
+            }
+            hot_key = max(hot_key, __shfl_xor_sync(FULL, hot_key, 1));
+            hot_key = max(hot_key, __shfl_xor_sync(FULL, hot_key, 2));
+            hot_key = max(hot_key, __shfl_xor_sync(FULL, hot_key, 4));
+        }
+        return __shfl_sync(FULL, hot_key, (lane & 3) << 3) & 0xff;
+    } else {
+        int keys[2] = {0, 0};
+        if (coop) {
+#pragma unroll
+            for (int pass = 0; pass < 2; ++pass) {
+                const int c = 2 * pass + (lane >> 3), s = lane & 7;
+                int hot_key = 0;
+                if (c < count && s < ts) {
+                    const uint32_t wd = sDw[(1 + c * bpc + 4 + (s >> 2)) * 4 + (s & 3)];
+                    const uint32_t row =
+                        draw_index(wd, (uint32_t)n, cand_slot(c, 4 + (s >> 2)), it, stream, k0, k1, s & 3);
+                    hot_key = (sRes[row] << 13) | ((31 - s) << 8) | (int)row;
+                }
+                hot_key = max(hot_key, __shfl_xor_sync(gm, hot_key, 1, 16));
+                hot_key = max(hot_key, __shfl_xor_sync(gm, hot_key, 2, 16));
+                hot_key = max(hot_key, __shfl_xor_sync(gm, hot_key, 4, 16));
+                keys[pass] = hot_key;
+            }
+        }
+        // candidate c's winner sits in pass c/2 at lane (c%2)*8
+        const int k0v = __shfl_sync(gm, keys[0], (lane & 1) << 3, 16);
+        const int k1v = __shfl_sync(gm, keys[1], (lane & 1) << 3, 16);
+        return ((lane >> 1) & 1 ? k1v : k0v) & 0xff;
+    }
+}
+
 // A loaded replica: its shared-memory structures, the job's constants the
 // iteration reads, and the scalar state the loop carries.
 template <int OPL, int GW>
@@ -865,48 +923,8 @@ __device__ __forceinline__ Choice choose_move(const Replica<OPL, GW>& R, Propose
     const uint4 mblk = P.sDraw[0];
     const int count = (uint64_t)mblk.x < P.thr_greedy ? P.cs : 1;
 
-    // C: cooperative hot-row tournaments for candidates 0..3, 8 lanes
-    // (samples) per candidate: one pass of the warp, two of a half-warp
-    int coop_row = 0;
-    if constexpr (GW == 32) {
-        int hot_key = 0;
-        if (P.coop) {
-            const int c = lane >> 3, s = lane & 7;
-            if (c < count && s < ts) {
-                const uint32_t wd = sDw[(1 + c * bpc + 4 + (s >> 2)) * 4 + (s & 3)];
-                const uint32_t row =
-                    draw_index(wd, (uint32_t)n, cand_slot(c, 4 + (s >> 2)), it, stream, k0, k1, s & 3);
-                hot_key = (sRes[row] << 13) | ((31 - s) << 8) | (int)row;
-            }
-            hot_key = max(hot_key, __shfl_xor_sync(FULL, hot_key, 1));
-            hot_key = max(hot_key, __shfl_xor_sync(FULL, hot_key, 2));
-            hot_key = max(hot_key, __shfl_xor_sync(FULL, hot_key, 4));
-        }
-        coop_row = __shfl_sync(FULL, hot_key, (lane & 3) << 3) & 0xff;
-    } else {
-        int keys[2] = {0, 0};
-        if (P.coop) {
-#pragma unroll
-            for (int pass = 0; pass < 2; ++pass) {
-                const int c = 2 * pass + (lane >> 3), s = lane & 7;
-                int hot_key = 0;
-                if (c < count && s < ts) {
-                    const uint32_t wd = sDw[(1 + c * bpc + 4 + (s >> 2)) * 4 + (s & 3)];
-                    const uint32_t row =
-                        draw_index(wd, (uint32_t)n, cand_slot(c, 4 + (s >> 2)), it, stream, k0, k1, s & 3);
-                    hot_key = (sRes[row] << 13) | ((31 - s) << 8) | (int)row;
-                }
-                hot_key = max(hot_key, __shfl_xor_sync(gm, hot_key, 1, 16));
-                hot_key = max(hot_key, __shfl_xor_sync(gm, hot_key, 2, 16));
-                hot_key = max(hot_key, __shfl_xor_sync(gm, hot_key, 4, 16));
-                keys[pass] = hot_key;
-            }
-        }
-        // candidate c's winner sits in pass c/2 at lane (c%2)*8
-        const int k0v = __shfl_sync(gm, keys[0], (lane & 1) << 3, 16);
-        const int k1v = __shfl_sync(gm, keys[1], (lane & 1) << 3, 16);
-        coop_row = ((lane >> 1) & 1 ? k1v : k0v) & 0xff;
-    }
+    // C: cooperative hot-row tournaments
+    const int coop_row = coop_hot_row<GW>(sDw, sRes, bpc, count, ts, P.coop, n, it, stream, k0, k1, lane);
 
     // D: proposals, lane c proposes candidate c
     uint2 desc = make_uint2(0u, 0u);
@@ -936,7 +954,7 @@ __device__ __forceinline__ Choice choose_move(const Replica<OPL, GW>& R, Propose
             else if (R.obj_kind == 2) prim = __reduce_add_sync(gm, d.dpar);
         }
         ++ch.evals;
-        ch.evals2 += u.R2 >= 0;
+        if constexpr (kMoveStats) ch.evals2 += u.R2 >= 0;
         bool better = ch.b0 == 0;
         if (!better) {
             if (prim != ch.bprim) better = prim < ch.bprim;
@@ -975,8 +993,10 @@ __device__ __forceinline__ bool apply_move(Replica<OPL, GW>& R, const Choice& ch
         R.score += ch.bds;
         R.conflicts += ch.bdc;
         R.obj_total += ch.bprim;
-        ++R.accepted;
-        R.accepted_rows += u.R2 >= 0 ? 2u : 1u;
+        if constexpr (kMoveStats) {
+            ++R.accepted;
+            R.accepted_rows += u.R2 >= 0 ? 2u : 1u;
+        }
     }
 
     // H: best tracking, cooling, reheat
@@ -1016,37 +1036,341 @@ __device__ __forceinline__ bool apply_move(Replica<OPL, GW>& R, const Choice& ch
     return accept;
 }
 
+// The one-warp (or half-warp) replica loop.  Its phases A-H are those of
+// choose_move and apply_move above, written out in one body: as separate
+// functions, even inlined, they hold more values live across the loop and
+// spill more under the lean kernel's 96-register budget (measured 6%
+// slower on W(26,25) populations).
 template <int OPL, bool GEN, int GW = 32>
 __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int lane, uint64_t chunk_iters) {
-    Replica<OPL, GW> R;
-    if (!load_replica<OPL, GEN, GW>(a, rid, slot, lane, chunk_iters, R)) return;
-    const SlotLayout L = slot_layout(R.n, R.m, OPL > 4);
-    Proposer<GW> P;
-    setup_proposer<OPL, GW>(R, reinterpret_cast<uint4*>(slot + L.off_draws),
-                            reinterpret_cast<View*>(slot + L.off_view), lane, P);
-    build_thresholds<GW>(R.sThr, R.T, lane);
-    const XwJob* J = R.J;
+    const unsigned gm = group_mask<GW>();
+    uint8_t* rec = a.arena + a.rec_off[rid];
+    RepHeader* H = reinterpret_cast<RepHeader*>(rec);
+    const uint32_t jid = H->job;
+    XwJob* J = a.jobs + jid;
+    if (*(volatile int32_t*)&J->done) return;
+    if (a.stop_on_solve == 1 && *(volatile int32_t*)&J->solved) return;
+
+    // eight rows per lane: int16 Gram and 256-bit row masks (slot_layout)
+    constexpr int MW = OPL > 4 ? 4 : 2;
+    using GT = typename std::conditional<(OPL > 4), int16_t, int32_t>::type;
+    const int n = J->n, w = J->w, m = J->m, sparse = J->sparse;
+    const SlotLayout L = slot_layout(n, m, OPL > 4);
+    const int ld = L.ld;
+    int8_t* sW = reinterpret_cast<int8_t*>(slot);
+    GT* sG = reinterpret_cast<GT*>(slot + L.off_g);
+    int32_t* sRes = reinterpret_cast<int32_t*>(slot + L.off_res);
+    uint8_t* sMino = slot + L.off_mino;
+    uint64_t* sMask = reinterpret_cast<uint64_t*>(slot + L.off_mask);
+    uint4* sDraw = reinterpret_cast<uint4*>(slot + L.off_draws);
+    const uint32_t* sDw = reinterpret_cast<const uint32_t*>(sDraw);
+    View* sView = reinterpret_cast<View*>(slot + L.off_view);
+    uint64_t* sThr = reinterpret_cast<uint64_t*>(slot + L.off_thr);
+
+    uint64_t it = H->it;
+    uint64_t iters = chunk_iters;
+    if (J->budget_iters) {
+        if (it >= J->budget_iters) return;
+        if (iters > J->budget_iters - it) iters = J->budget_iters - it;
+    }
+
+    // ---- load W and the minority lists; rebuild masks, Gram, residuals ----
+    const uint32_t nn = (uint32_t)(n * n);
+    copy16<GW>(sW, rec + J->off_w, nn, lane);
+    const uint32_t status0 = H->status;
+    if (m > 0 && (status0 & XW_STATUS_INIT)) copy16<GW>(sMino, rec + J->off_mino, (uint32_t)(n * m), lane);
+    __syncwarp(gm);
+    int bad_rows = 0;
+#pragma unroll
+    for (int k = 0; k < OPL; ++k) {
+        const int o = lane + GW * k;
+        if (o < n) {
+            int pos = 0, weight = 0;
+#pragma unroll
+            for (int q = 0; q < MW; ++q) {
+                uint64_t word = 0;
+#pragma unroll 1
+                for (int c = 64 * q; c < n && c < 64 * q + 64; ++c) {
+                    const bool nz = sW[c * n + o] != 0;
+                    if (nz) word |= 1ull << (c & 63);
+                    if (m > 0 && !(status0 & XW_STATUS_INIT) && nz == (sparse != 0)) {
+                        if (pos < m) sMino[o * m + pos] = (uint8_t)c;
+                        ++pos;
+                    }
+                }
+                sMask[MW * o + q] = word;
+                weight += __popcll(word);
+            }
+            if (weight != w) bad_rows = 1;
+            if (m > 0 && !(status0 & XW_STATUS_INIT) && pos != m) bad_rows = 1;
+        }
+    }
+    if (__any_sync(gm, bad_rows)) {
+        if (lane == 0) H->err |= XW_ERR_MINORITY;
+        return;
+    }
+    __syncwarp(gm);
+    int p_score = 0, p_conf = 0, p_par = 0;
+    long long p_sq = 0;
+#pragma unroll
+    for (int k = 0; k < OPL; ++k) {
+        const int o = lane + GW * k;
+        if (o < n) {
+            int r_sum = 0;
+#pragma unroll 1
+            for (int r = 0; r < n; ++r) {
+                int dot = 0;
+#pragma unroll 1
+                for (int c = 0; c < n; ++c) dot += sW[c * n + r] * sW[c * n + o];
+                sG[r * ld + o] = (GT)dot;
+                if (r != o) {
+                    const int ad = iabs(dot);
+                    r_sum += ad;
+                    p_conf += dot != 0;
+                    p_sq += (long long)(dot * dot);
+                    p_par += ad & 1;
+                }
+            }
+            sRes[o] = r_sum;
+            p_score += r_sum;
+        }
+    }
+    const int score0 = __reduce_add_sync(gm, p_score) / 2;
+    const int conf0 = __reduce_add_sync(gm, p_conf) / 2;
+#pragma unroll
+    for (int off = GW / 2; off > 0; off >>= 1) p_sq += __shfl_xor_sync(gm, p_sq, off, GW);
+    const long long sq0 = p_sq / 2;
+    const int par0 = __reduce_add_sync(gm, p_par) / 2;
+    __syncwarp(gm);
+
+    const int obj_kind = GEN ? H->obj_kind : 0;
+    if (!GEN && (H->obj_kind != 0 || J->move_set != 0)) {
+        // the lean kernel was launched for a replica that needs the general one
+        if (lane == 0) H->err |= XW_ERR_KERNEL;
+        return;
+    }
+    const int64_t obj0 = obj_kind == 1 ? sq0 : obj_kind == 2 ? par0 : score0;
+    int score, conflicts, best_s, best_c, msi, cool;
+    int64_t obj_total;
+    uint64_t moves, cand_evals;
+    uint32_t accepted = H->accepted, accepted_rows = H->accepted_rows, two_row_evals = H->two_row_evals;
+    double T = H->temperature;
+    const double reheat_T = H->reheat_temperature;
+    if (status0 & XW_STATUS_INIT) {
+        if (H->score != score0 || H->conflicts != conf0 || H->obj_total != obj0) {
+            if (lane == 0) H->err |= XW_ERR_SCORE;
+            return;
+        }
+        best_s = H->best_score;
+        best_c = H->best_conflicts;
+        msi = H->msi;
+        cool = H->cool_ctr;
+        moves = H->moves;
+        cand_evals = H->cand_evals;
+    } else {
+        best_s = score0;
+        best_c = conf0;
+        msi = 0;
+        cool = 0;
+        moves = 0;
+        cand_evals = 0;
+        accepted = accepted_rows = two_row_evals = 0;
+        copy16<GW>(rec + J->off_best, sW, nn, lane);
+    }
+    score = score0;
+    conflicts = conf0;
+    obj_total = obj0;
+
+    // ---- job constants ----
     const int tempering = J->tempering;
+    const int cs = J->candidate_samples, ts = J->target_samples;
     const int mpc = J->moves_per_cool, stuck = J->stuck_threshold;
+    const uint32_t k0 = J->key0, k1 = J->key1, stream = H->stream;
+    const uint64_t thr_greedy = J->thr_greedy;
     const double t_min = J->t_min, cooling = J->cooling, reheat = J->reheat;
+    const int bpc = 4 + (ts <= 4 ? 1 : 2);          // cached blocks per candidate
+    const bool coop = ts <= 8;                      // cooperative hot-row tournament
+    if (lane == 0) {
+        View v;
+        v.W = sW; v.mino = sMino; v.res = sRes; v.mask = sMask; v.dw = sDw;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int lo = 64 * q;
+            v.valid[q] = n >= lo + 64 ? ~0ull : n <= lo ? 0ull : ((1ull << (n - lo)) - 1ull);
+        }
+        v.thr_target = J->thr_target; v.thr_dbl = J->thr_double; v.thr_sign = J->thr_sign;
+        v.thr_swsign = J->thr_swsign;
+        v.n = n; v.w = w; v.m = m; v.sparse = sparse; v.ts = ts; v.bpc = bpc; v.cc = 31 / bpc;
+        v.move_set = J->move_set;
+        v.stream = stream; v.k0 = k0; v.k1 = k1; v.pad = 0;
+        *sView = v;
+    }
+    __syncwarp(gm);
+
+    build_thresholds<GW>(sThr, T, lane);
+
+    // lane -> cached Philox blocks of this iteration (block 0 is the
+    // move-level block, 1 + c*bpc + b block b of candidate c); a half-warp
+    // group computes two blocks per lane
+    uint32_t my_slot = 0, my_slot2 = 0;
+    if (lane > 0) {
+        const int q = lane - 1, c = q / bpc, b = q - c * bpc;
+        my_slot = cand_slot(c, b);
+    }
+    if constexpr (GW == 16) {
+        const int q = lane + 15, c = q / bpc, b = q - c * bpc;
+        my_slot2 = cand_slot(c, b);
+    }
+    // register context of candidate `lane` for the inlined proposal path
+    Reg rg;
+    rg.W = sW; rg.mino = sMino; rg.mask = sMask;
+    rg.cw = sDw + (1 + lane * bpc) * 4;
+    rg.cached = lane < 31 / bpc;
+    rg.thr_target = J->thr_target; rg.thr_dbl = J->thr_double; rg.thr_sign = J->thr_sign;
+    rg.thr_swsign = J->thr_swsign;
+    rg.n = n; rg.w = w; rg.m = m; rg.sparse = sparse; rg.move_set = J->move_set;
+    rg.stream = stream; rg.k0 = k0; rg.k1 = k1;
 
     uint64_t done = 0;
 #pragma unroll 1
-    for (; done < R.iters; ++done) {
+    for (; done < iters; ++done) {
         // 1: every replica of the job stops soon after any solve;
         // 2: a replica stops at its own solve only, so that each replica's
         //    trajectory is independent of how the launches are scheduled
         if (a.stop_on_solve) {
-            if (R.best_s == 0) break;
+            if (best_s == 0) break;
             if (a.stop_on_solve == 1 && (done & 63) == 63 && *(volatile int32_t*)&J->solved) break;
         }
-        const Choice ch = choose_move<OPL, GEN, GW>(R, P, R.it, lane);
-        R.cand_evals += ch.evals;
-        R.two_row_evals += ch.evals2;
-        if (ch.b0) apply_move<OPL, GEN, GW>(R, ch, tempering, mpc, stuck, t_min, cooling, reheat, lane);
-        ++R.it;
+        // A: draws
+        sDraw[lane] = draw_block(my_slot, it, stream, k0, k1);
+        if constexpr (GW == 16) sDraw[lane + 16] = draw_block(my_slot2, it, stream, k0, k1);
+        __syncwarp(gm);
+        const uint4 mblk = sDraw[0];
+        const int count = (uint64_t)mblk.x < thr_greedy ? cs : 1;
+
+        // C: cooperative hot-row tournaments for candidates 0..3, 8 lanes
+        // (samples) per candidate: one pass of the warp, two of a half-warp
+        const int coop_row = coop_hot_row<GW>(sDw, sRes, bpc, count, ts, coop, n, it, stream, k0, k1, lane);
+
+        // D: proposals, lane c proposes candidate c
+        uint2 desc = make_uint2(0u, 0u);
+        rg.it = it;
+        if (lane < count) desc = d_propose<MW, GEN>(rg, sView, lane, coop && lane < 4, coop_row);
+        __syncwarp(gm);
+
+        // E: evaluate in candidate order, keep the first best
+        bool have = false;
+        uint32_t b0 = 0, b1 = 0;
+        int bds = 0, bdc = 0, bprim = 0;
+#pragma unroll 1
+        for (int c = 0; c < count; ++c) {
+            const uint32_t e0 = __shfl_sync(gm, desc.x, c, GW);
+            const uint32_t e1 = __shfl_sync(gm, desc.y, c, GW);
+            if (!(e0 & 1u)) continue;
+            const Update u = decode(e0, e1, sW, n);
+            const Deltas d = eval_lane<OPL, GT, GEN, GW>(u, sW, sG, n, ld, lane);
+            const int packed = __reduce_add_sync(gm, d.ds * 4096 + d.dc);
+            const int dc = ((packed + 2048) & 4095) - 2048;
+            const int ds = (packed - dc) >> 12;
+            int prim = ds;
+            if (GEN) {
+                if (obj_kind == 1) prim = __reduce_add_sync(gm, d.dsq);
+                else if (obj_kind == 2) prim = __reduce_add_sync(gm, d.dpar);
+            }
+            ++cand_evals;
+            if constexpr (kMoveStats) two_row_evals += u.R2 >= 0;
+            bool better = !have;
+            if (!better) {
+                if (prim != bprim) better = prim < bprim;
+                else if (ds != bds) better = ds < bds;
+                else better = dc < bdc;
+            }
+            if (better) {
+                have = true; b0 = e0; b1 = e1; bds = ds; bdc = dc; bprim = prim;
+            }
+        }
+        if (!have) {
+            ++it;
+            continue;
+        }
+        ++moves;
+
+        // F: Metropolis
+        bool accept = bprim <= 0;
+        if (!accept)
+            accept = bprim <= (int64_t)kThrTable ? (uint64_t)mblk.y < sThr[bprim - 1]
+                                                 : metropolis_accept(bprim, T, mblk.y);
+
+        // G: commit
+        if (accept) {
+            const Update u = decode(b0, b1, sW, n);
+            commit<OPL, MW, GT, GEN, GW>(b0, b1, u, bds, sW, sG, sRes, sMino, sMask, n, ld, m, sparse, lane);
+            score += bds;
+            conflicts += bdc;
+            obj_total += bprim;
+            if constexpr (kMoveStats) {
+                ++accepted;
+                accepted_rows += u.R2 >= 0 ? 2u : 1u;
+            }
+        }
+
+        // H: best tracking, cooling, reheat
+        if (score < best_s || (score == best_s && conflicts < best_c)) {
+            best_s = score;
+            best_c = conflicts;
+            msi = 0;
+            copy16<GW>(rec + J->off_best, sW, nn, lane);
+            if (best_s == 0 && lane == 0) {
+                H->solve_it = it;
+                H->solve_ns = globaltimer();
+                if (atomicCAS(&J->solved, 0, 1) == 0) {
+                    J->solved_replica = (int32_t)H->stream;
+                    J->solved_it = it;
+                    J->solve_ns = H->solve_ns;
+                }
+            }
+        } else {
+            ++msi;
+        }
+        if (!tempering) {
+            const double T0 = T;
+            if (++cool >= mpc) {
+                cool = 0;
+                T = __dmul_rn(T, cooling);
+                if (T < t_min) T = t_min;
+            }
+            if (msi >= stuck) {
+                msi = 0;
+                T = __dmul_rn(reheat_T, reheat);
+                if (T < t_min) T = t_min;
+            }
+            if (T != T0) build_thresholds<GW>(sThr, T, lane);
+        }
+        ++it;
     }
-    store_replica<OPL, GW>(R, lane);
+
+    // ---- write back ----
+    __syncwarp(gm);
+    copy16<GW>(rec + J->off_w, sW, nn, lane);
+    if (m > 0) copy16<GW>(rec + J->off_mino, sMino, (uint32_t)(n * m), lane);
+    if (lane == 0) {
+        H->it = it;
+        H->moves = moves;
+        H->cand_evals = cand_evals;
+        H->accepted = accepted;
+        H->accepted_rows = accepted_rows;
+        H->two_row_evals = two_row_evals;
+        H->score = score;
+        H->conflicts = conflicts;
+        H->best_score = best_s;
+        H->best_conflicts = best_c;
+        H->obj_total = obj_total;
+        H->temperature = T;
+        H->msi = msi;
+        H->cool_ctr = cool;
+        H->status = status0 | XW_STATUS_INIT | (best_s == 0 ? XW_STATUS_SOLVED : 0u);
+    }
+    __syncwarp(gm);
 }
 
 // ---------------------------------------------------------------------------

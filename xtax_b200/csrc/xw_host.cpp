@@ -437,7 +437,15 @@ void Batch::derive_layout() {
     classes.clear();
     for (uint32_t i = n_large; i < total_replicas; ++i) {
         const XwJob& J = jobs[job_of[items[i]]];
-        const int kind = tune_kind(J.n, J.candidate_samples);
+        int kind = tune_kind(J.n, J.candidate_samples);
+        if (kind == kTunePairKind && !split_pair_class) {
+            // orders up to 16 at one replica per warp run the one-row-per-lane
+            // kernel: they join that class's launch instead of a launch of
+            // their own
+            int rpw = params.replicas_per_warp;
+            if (rpw == 0) rpw = tuned_shape(kTunePairKind, anneal_slot_bytes(J.n, J.m, 1), params.device).rpw;
+            if (rpw == 1) kind = anneal_opl(J.n);
+        }
         if (classes.empty() || classes.back().kind != kind) {
             LaunchClass c;
             c.kind = kind;
@@ -721,6 +729,21 @@ void Batch::configure_shape() {
     for (const LaunchClass& c : classes) most_chunks = std::max(most_chunks, c.chunks);
     if (most_chunks > 1 && !d_chunk_done)
         dalloc(&d_chunk_done, sizeof(uint32_t) * std::max<uint32_t>(total_replicas, 1), "cudaMalloc chunk counters");
+    // launches of a round go out smallest estimated work first (replicas x
+    // order, the large-order kernel's iterations counted four times): each
+    // is a persistent kernel sized for the whole device, so the one issued
+    // last takes the SMs the others leave and absorbs their tails
+    std::vector<std::pair<double, int>> work;
+    if (n_large) {
+        int nmax = 0;
+        for (const XwJob& J : jobs)
+            if (J.large) nmax = std::max(nmax, J.n);
+        work.push_back({4.0 * n_large * nmax, -1});
+    }
+    for (size_t k = 0; k < classes.size(); ++k) work.push_back({(double)classes[k].item_count * classes[k].max_n, (int)k});
+    std::stable_sort(work.begin(), work.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+    launch_order.clear();
+    for (const auto& wv : work) launch_order.push_back(wv.second);
 }
 
 bool Batch::configure_latency(size_t k, int wpr) {
@@ -855,22 +878,24 @@ void Batch::enqueue_rounds(uint64_t iters, bool timed) {
             if (launches == 1 || idx == 0) return;
             check(cudaEventRecord(side_events[idx], st), "cudaEventRecord");
         };
-        if (n_large) {
-            AnnealArgs la = a;
-            la.items = static_cast<const uint32_t*>(d_items);
-            la.n_items = n_large;
-            la.slot_bytes = large_slot_bytes;
-            la.counter = counters + l;
-            la.gram = static_cast<uint8_t*>(d_gram);
-            la.gram_off = static_cast<const uint64_t*>(d_gram_off);
-            la.chunks = la.iters >= large_chunks ? large_chunks : 1;
-            if (la.chunks > 1) la.chunk_done = static_cast<uint32_t*>(d_chunk_done);
-            cudaStream_t st = on(l);
-            check(launch_anneal_large(la, general_large, large_wpb, large_blocks, st), "launch anneal_large_kernel");
-            join(l, st);
-            ++l;
-        }
-        for (const LaunchClass& c : classes) {
+        for (const int which : launch_order) {
+            if (which < 0) {
+                AnnealArgs la = a;
+                la.items = static_cast<const uint32_t*>(d_items);
+                la.n_items = n_large;
+                la.slot_bytes = large_slot_bytes;
+                la.counter = counters + l;
+                la.gram = static_cast<uint8_t*>(d_gram);
+                la.gram_off = static_cast<const uint64_t*>(d_gram_off);
+                la.chunks = la.iters >= large_chunks ? large_chunks : 1;
+                if (la.chunks > 1) la.chunk_done = static_cast<uint32_t*>(d_chunk_done);
+                cudaStream_t st = on(l);
+                check(launch_anneal_large(la, general_large, large_wpb, large_blocks, st), "launch anneal_large_kernel");
+                join(l, st);
+                ++l;
+                continue;
+            }
+            const LaunchClass& c = classes[(size_t)which];
             AnnealArgs ca = a;
             ca.items = static_cast<const uint32_t*>(d_items) + c.item_begin;
             ca.n_items = c.item_count;
@@ -1508,6 +1533,7 @@ int32_t xw_autotune(const xw_job_spec* jobs, int32_t njobs, const xw_params* pin
             if (!err.empty()) return fail(XW_ERR_INVALID, err);
         }
         Batch b;
+        b.split_pair_class = true;   // the orders up to 16 are tuned apart
         b.build(jobs, njobs, *pin, nullptr);
         if (b.classes.empty())
             return fail(XW_ERR_INVALID, "autotune covers the shared-memory kernel; every job here is of larger order");

@@ -147,6 +147,12 @@ struct Batch {
         uint32_t chunks = 1;
     };
     std::vector<LaunchClass> classes;
+    // launches of a round in issue order: class index, or -1 for the
+    // large-order kernel
+    std::vector<int> launch_order;
+    // keep the orders up to 16 in a class of their own even at one replica
+    // per warp (the autotuner times them apart)
+    bool split_pair_class = false;
     void* d_chunk_done = nullptr;
     std::vector<cudaStream_t> side_streams;
     std::vector<cudaEvent_t> side_events;    // fork, then one join per launch

@@ -146,6 +146,7 @@ using ReqPtr = std::shared_ptr<Request>;
 struct Server {
     xw_server_config cfg{};
     int sms = 0;
+    int optin_smem = 0;   // opt-in shared memory per CTA
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
 
     std::mutex mu;
@@ -460,7 +461,9 @@ void Server::round(bool& any_tempering) {
         if (cfg.warps_per_block > 0) t.wpb = cfg.warps_per_block;
         if (cfg.replicas_per_warp > 0) t.rpw = cfg.replicas_per_warp;
         if (c != 0) t.rpw = 1;
-        const int wpb = std::max(1, std::min(16, t.wpb));
+        // a CTA's slots must fit the opt-in shared memory (large orders)
+        const int fit = std::max(1, optin_smem / (int)std::max<uint32_t>(1, class_slot[c] * (uint32_t)t.rpw));
+        const int wpb = std::max(1, std::min({16, t.wpb, fit}));
         cls_wpb[c] = wpb;
         cls_rpw[c] = t.rpw;
         cls_blocks[c] = blocks_for(c, class_general[c], class_slot[c], wpb, t.rpw, items_host[c].size());
@@ -765,6 +768,8 @@ void Server::start() {
     cudaDeviceProp props{};
     check_cuda(cudaGetDeviceProperties(&props, cfg.device), "cudaGetDeviceProperties");
     sms = props.multiProcessorCount;
+    check_cuda(cudaDeviceGetAttribute(&optin_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, cfg.device),
+               "cudaDeviceGetAttribute max opt-in shared memory");
     for (int c = 0; c < kClasses; ++c)
         for (bool general : {false, true})
             for (int rpw = 1; rpw <= (c == 0 ? 2 : 1); ++rpw)
