@@ -433,18 +433,30 @@ void Batch::derive_layout() {
         if (A.large != B.large) return A.large > B.large;
         return A.n > B.n;
     });
-    // launch classes over the shared-memory items
+    // launch classes over the shared-memory items.  The orders up to 16 get
+    // a launch of their own (two replicas per warp) only when it pays: at
+    // one replica per warp they run the one-row-per-lane kernel and join
+    // that class's launch, and so they do when the batch holds other orders
+    // of that class and too few of them to fill the device alone -- a small
+    // second launch would run its replicas beside the first at low
+    // occupancy instead of sharing its chunked work list.
+    uint32_t pair_count = 0, one_row_count = 0;
+    for (uint32_t i = n_large; i < total_replicas; ++i) {
+        const XwJob& J = jobs[job_of[items[i]]];
+        const int kind = tune_kind(J.n, J.candidate_samples);
+        pair_count += kind == kTunePairKind;
+        one_row_count += kind == 1;
+    }
+    const uint32_t fill = 2u * 20u * (uint32_t)std::max(1, props.multiProcessorCount);
+    const bool merge_pairs = one_row_count > 0 && pair_count < fill;
     classes.clear();
     for (uint32_t i = n_large; i < total_replicas; ++i) {
         const XwJob& J = jobs[job_of[items[i]]];
         int kind = tune_kind(J.n, J.candidate_samples);
         if (kind == kTunePairKind && !split_pair_class) {
-            // orders up to 16 at one replica per warp run the one-row-per-lane
-            // kernel: they join that class's launch instead of a launch of
-            // their own
             int rpw = params.replicas_per_warp;
             if (rpw == 0) rpw = tuned_shape(kTunePairKind, anneal_slot_bytes(J.n, J.m, 1), params.device).rpw;
-            if (rpw == 1) kind = anneal_opl(J.n);
+            if (rpw == 1 || (merge_pairs && params.replicas_per_warp != 2)) kind = anneal_opl(J.n);
         }
         if (classes.empty() || classes.back().kind != kind) {
             LaunchClass c;
@@ -988,7 +1000,12 @@ void Batch::collect(std::vector<JobOut>& out, int8_t* best_host, bool want_best)
             of.push_back(j);
         }
         std::vector<VerifyStats> vs;
-        verifier.run(items, stream, vs);
+        std::mutex* mu = nullptr;
+        DeviceVerifier& verifier = shared_verifier(params.device, mu);
+        {
+            std::lock_guard<std::mutex> lock(*mu);
+            verifier.run(items, stream, vs);
+        }
         for (size_t k = 0; k < of.size(); ++k) {
             vstats[of[k]] = vs[k];
             vstats_valid[of[k]] = 1;

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -73,6 +74,10 @@ struct DeviceVerifier {
     // enqueues on `stream`, waits, and returns the stats in item order
     void run(const std::vector<VerifyItem>& items, cudaStream_t stream, std::vector<VerifyStats>& out);
 };
+// The verifier batches share on a device (its scratch is allocated once and
+// kept: a batch's own would pay pinned-memory allocations and a cudaFree
+// per batch), with the mutex that serialises its users.
+DeviceVerifier& shared_verifier(int device, std::mutex*& mu);
 
 // Launch-shape classes of the autotuner (xw_tune.cpp): the rows-per-lane
 // class of the order (1, 2, 4, 8), or kTunePairKind for orders up to 16
@@ -188,7 +193,6 @@ struct Batch {
 
     // collect() with the best states checks every job's best W of order
     // <= 256 on the device (score, conflicts, exact flag per job)
-    DeviceVerifier verifier;
     std::vector<VerifyStats> vstats;
     std::vector<char> vstats_valid;
 

@@ -484,6 +484,17 @@ __global__ void verify_gather_kernel(const VerifyItem* items, const int32_t* ind
     if (threadIdx.x == 0) dims[blockIdx.x] = make_int2(it.n, it.w);
 }
 
+DeviceVerifier& shared_verifier(int device, std::mutex*& mu) {
+    static std::mutex table_mu;
+    static std::mutex use_mu[64];
+    static DeviceVerifier* table[64] = {};   // kept until exit
+    if (device < 0 || device >= 64) throw std::invalid_argument("device ordinal out of range");
+    std::lock_guard<std::mutex> lock(table_mu);
+    if (!table[device]) table[device] = new DeviceVerifier();
+    mu = &use_mu[device];
+    return *table[device];
+}
+
 DeviceVerifier::~DeviceVerifier() {
     for (void* ptr : {(void*)d_items, (void*)d_index, (void*)d_stage, (void*)d_dims, (void*)d_stats})
         if (ptr) cudaFree(ptr);
