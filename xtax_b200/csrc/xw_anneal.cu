@@ -1567,9 +1567,9 @@ __global__ void __maxnreg__(anneal_maxnreg(OPL, GEN, GW)) anneal_kernel(AnnealAr
         const uint32_t rid = a.items[item - c * a.n_items];
         const uint64_t lo = a.iters * c / a.chunks, hi = a.iters * (c + 1) / a.chunks;
         RepHeader* H = reinterpret_cast<RepHeader*>(a.arena + a.rec_off[rid]);
-        run_chunk(
-            a.chunk_done + rid, c, a.chunk_wait_ns, &H->err, lane,
-            [&]() { run_replica<OPL, GEN, GW>(a, rid, slot, lane, hi - lo); }, gm);
+        const bool ok = chunk_begin(a.chunk_done + rid, c, a.chunk_wait_ns, &H->err, lane, gm);
+        if (ok) run_replica<OPL, GEN, GW>(a, rid, slot, lane, hi - lo);
+        chunk_end(a.chunk_done + rid, c, ok, lane, gm);
     }
 }
 

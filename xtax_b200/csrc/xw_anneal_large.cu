@@ -875,8 +875,9 @@ __global__ void __launch_bounds__(128, XW_LARGE_MIN_BLOCKS) anneal_large_kernel(
         const uint32_t rid = a.items[item - c * a.n_items];
         const uint64_t lo = a.iters * c / a.chunks, hi = a.iters * (c + 1) / a.chunks;
         RepHeader* H = reinterpret_cast<RepHeader*>(a.arena + a.rec_off[rid]);
-        run_chunk(a.chunk_done + rid, c, a.chunk_wait_ns, &H->err, lane,
-                  [&]() { run_large<GEN>(a, rid, slot, lane, hi - lo); });
+        const bool ok = chunk_begin(a.chunk_done + rid, c, a.chunk_wait_ns, &H->err, lane, FULL);
+        if (ok) run_large<GEN>(a, rid, slot, lane, hi - lo);
+        chunk_end(a.chunk_done + rid, c, ok, lane, FULL);
     }
 }
 

@@ -157,25 +157,27 @@ __device__ __forceinline__ void release_chunk(uint32_t* flag, uint32_t value, in
     if (lane == 0) asm volatile("red.release.gpu.global.max.u32 [%0], %1;" ::"l"(flag), "r"(value) : "memory");
 }
 
-// One chunk of a chunked launch: wait for the replica's previous chunk, run
-// `body` when it finished normally, flag the replica and skip otherwise, and
-// publish this chunk's count.  Every lane of the replica's lane group `gm`
-// calls it.
-template <typename Body>
-__device__ __forceinline__ void run_chunk(uint32_t* done, uint32_t c, uint64_t limit_ns, uint32_t* err, int lane,
-                                          Body body, unsigned gm = 0xffffffffu) {
+// One chunk of a chunked launch: chunk_begin waits for the replica's
+// previous chunk and says whether this one runs (false: flag the replica,
+// skip); chunk_end publishes this chunk's count, poisoned when it did not
+// run.  Every lane of the replica's lane group `gm` calls both.  (The chunk
+// body is called between them by the kernel itself: wrapping it in a lambda
+// raised the lean kernel's spills from 40 to 412 bytes a thread and made the
+// W(26,25) tempering batch 9% slower on B200.)
+__device__ __forceinline__ bool chunk_begin(const uint32_t* done, uint32_t c, uint64_t limit_ns, uint32_t* err,
+                                            int lane, unsigned gm) {
     bool ok = true;
     if (c > 0) {
         const uint32_t seen = wait_chunk(done, c, limit_ns);
         ok = __all_sync(gm, seen != 0 && !(seen & kChunkPoison));
     }
     __syncwarp(gm);
-    if (ok) {
-        body();
-    } else if (lane == 0) {
-        atomicOr(err, XW_ERR_CHUNK);
-    }
-    release_chunk(done, ok ? c + 1 : (kChunkPoison | (c + 1)), lane, gm);
+    if (!ok && lane == 0) atomicOr(err, XW_ERR_CHUNK);
+    return ok;
+}
+
+__device__ __forceinline__ void chunk_end(uint32_t* done, uint32_t c, bool ran, int lane, unsigned gm) {
+    release_chunk(done, ran ? c + 1 : (kChunkPoison | (c + 1)), lane, gm);
 }
 
 // Metropolis test u*2^-32 < exp(-delta/T), delta > 0.
