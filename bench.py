@@ -374,7 +374,7 @@ def ours(args):
         except Exception as e:  # noqa: BLE001 - report, do not fail the bench
             line["plain_kernel"] = {"unavailable": str(e)[:200]}
     if args.rescore:
-        line["rescore"] = rescore_bench(torch, X)
+        line["rescore"] = rescore_bench(torch, X, [int(v) for v in args.rescore_orders.split(",")])
     if args.c1:
         line["single_replica"] = c1_bench(X, args.c1_ref_seconds)
     if args.uneven_iters > 0:
@@ -391,10 +391,10 @@ def ours(args):
 REF_HARNESS = os.path.join(REPO, "oracle", "_ref", "ref_harness")
 
 
-def rescore_bench(torch, X):
+def rescore_bench(torch, X, orders=(32, 64, 96, 128)):
     """Batched exact W W^T (tcgen05 kind::i8): 65536 fixed-degree ternary
-    matrices per order n in {32, 64, 96, 128}, w = n/2, resident in HBM.
-    HBM-bound: n^2 bytes in and 16 bytes out per matrix."""
+    matrices per order n (32, 64, 96, 128 by default), w = n/2, resident in
+    HBM.  HBM-bound: n^2 bytes in and 16 bytes out per matrix."""
     import ctypes as C
     peaks = {}
     try:
@@ -408,7 +408,7 @@ def rescore_bench(torch, X):
     count = 65536
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
-    for n in (32, 64, 96, 128):
+    for n in orders:
         w = n // 2
         gen = torch.Generator(device="cuda").manual_seed(n)
         W = torch.zeros((count, n, n), dtype=torch.int8, device="cuda")
@@ -809,6 +809,7 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--iters", type=int, default=ITERS, help="iterations per replica per step (profiling cases)")
     ap.add_argument("--rescore", type=int, default=1, help="also time the batched tensor-core rescoring")
+    ap.add_argument("--rescore-orders", default="32,64,96,128", help="orders of that section (multiples of 32)")
     ap.add_argument("--c1", type=int, default=1, help="also time single-replica W(12,11) searches")
     ap.add_argument("--c1-ref-seconds", type=float, default=8.0,
                     help="wall seconds of single-thread reference runs beside them")

@@ -16,11 +16,13 @@
 // columns past n are not multiplied) into a TMEM
 // accumulator; the diagonal n x n blocks of D are the tile's Gram matrices.
 // The epilogue warps read their TMEM lane quarter (one row per thread) and
-// reduce the row statistics per matrix.  The kernel is persistent over
-// tiles with a 3-stage TMA ring and four CTAs per SM, so loads of later tiles
-// and other CTAs' MMAs overlap the epilogue of the current one; at the
-// benchmark's sizes it is HBM-bound
-// (n^2 bytes read per matrix, 2n^3 MACs).
+// reduce the row statistics per matrix.  The kernel is persistent (two
+// CTAs per SM) and warp-specialised: per CTA a producer warp keeps a 6-tile
+// TMA ring full, an MMA warp fills two TMEM accumulators in turn, and two
+// groups of four epilogue warps drain them, each step waiting only on the
+// mbarrier of its stage or accumulator, so that loads, MMAs and epilogues of
+// successive tiles overlap.  The bound is HBM: n^2 bytes read per matrix against 2n^3
+// MACs.
 //
 // Every wait on an mbarrier has an iteration limit; on expiry the kernel
 // records an error code, waits (bounded) for its own loads still in flight,
@@ -44,10 +46,44 @@ namespace xw {
 
 namespace {
 
-constexpr int kStages = 3;
+// Pipeline shape: CTAs per SM, TMA ring depth (tiles), TMEM accumulators
+// (128 columns each) and epilogue groups (four warps each) per CTA.  The
+// shared-memory ring must admit no more CTAs per SM than the TMEM columns
+// do (kCtasPerSm x kAccs x 128 <= 512).  Measured on B200, 65536 matrices,
+// ms at n = 32 / 64 / 96 / 128 (CTAs x stages x accumulators x groups):
+//   2 x 6 x 2 x 2   0.047 / 0.121 / 0.234 / 0.278   (the default)
+//   4 x 3 x 1 x 1   0.049 / 0.133 / 0.256 / 0.307
+//   1 x 8 x 4 x 4   0.070 / 0.141 / 0.311 / 0.346
+//   1 x 8 x 4 x 2   0.070 / 0.168 / 0.305 / 0.412
+//   2 x 6 x 2 x 1   0.057 / 0.165 / 0.320 / 0.381
+// against 0.053 / 0.125 / 0.238 / 0.317 for one CTA-wide barrier per tile
+// step (4 CTAs per SM, 3 stages).
+#ifndef XW_RESCORE_CTAS
+#define XW_RESCORE_CTAS 2
+#endif
+#ifndef XW_RESCORE_STAGES
+#define XW_RESCORE_STAGES 6
+#endif
+#ifndef XW_RESCORE_ACCS
+#define XW_RESCORE_ACCS 2
+#endif
+#ifndef XW_RESCORE_GROUPS
+#define XW_RESCORE_GROUPS 2
+#endif
+constexpr int kCtasPerSm = XW_RESCORE_CTAS;
+constexpr int kStages = XW_RESCORE_STAGES;
 constexpr int kTileRows = 128;
 constexpr int kTileBytes = kTileRows * 128;   // 128 rows x 128 bytes (K padded to 128)
-constexpr uint32_t kTmemCols = 128;
+constexpr int kAccs = XW_RESCORE_ACCS;
+constexpr int kAccCols = 128;                 // columns of one accumulator (N <= 128)
+constexpr uint32_t kTmemCols = kAccs * kAccCols;
+constexpr int kGroups = XW_RESCORE_GROUPS;
+constexpr int kThreads = 64 + 128 * kGroups;
+constexpr int kCombineSlots = 8;
+static_assert(kAccs % kGroups == 0, "an accumulator belongs to one epilogue group");
+static_assert(kCombineSlots >= kAccs / kGroups + 1, "a combine slot outlives its tile");
+static_assert(kCtasPerSm * kAccs * kAccCols <= 512, "TMEM columns of the resident CTAs");
+static_assert(kTmemCols == 128 || kTmemCols == 256 || kTmemCols == 512, "TMEM allocation size");
 constexpr long long kSpinLimit = 1ll << 22;
 
 struct RescoreParams {
@@ -100,6 +136,8 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
 }
 
 // K-major operand with 128-byte swizzle: 8-row groups 1024 bytes apart.
+// (The 32- and 64-byte swizzles with boxes of n bytes per row, tried for
+// n = 32 and 64, were slower: 0.055 against 0.047 ms at n = 32.)
 __device__ __forceinline__ uint64_t smem_desc(const void* tile) {
     const uint64_t addr = smem_addr(tile);
     uint64_t d = 0;
@@ -143,29 +181,142 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, int (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-__global__ void __launch_bounds__(128, 4) rescore_tc_kernel(const __grid_constant__ CUtensorMap tmap,
-                                                             RescoreParams p) {
+// Warp roles.  Warp 0 (one thread): TMA producer over a kStages ring of
+// tiles.  Warp 1: allocates TMEM; one thread issues each tile's MMA chain
+// into the next of kAccs accumulators (128 columns each) and commits it to
+// the tile's stage (free again) and to the accumulator (ready).  Warps
+// 2..2+4*kGroups-1: epilogue groups of four warps, one per TMEM lane
+// quarter (warp w reads lanes 32*(w%4)..); group g takes the tiles
+// it = g, g + kGroups, ... of this CTA and frees the accumulator as soon as
+// its rows are read.  No CTA-wide barrier inside the tile loop: a tile's
+// load, MMA and epilogue each wait only on the mbarrier of the stage or
+// accumulator they use, so loads run kStages tiles ahead and the MMA of the
+// next tiles overlaps the epilogue of this one.
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void rescore_fail(const RescoreParams& p, volatile int* abort_flag, int code) {
+    atomicExch(p.error, code);
+    *abort_flag = 1;
+}
+
+// Per-row statistics of one tile's accumulator rows 32q..32q+31 (this
+// warp's lane quarter); see the epilogue comment below.  Returns the warp's
+// sums and whether every row's diagonal entry is right.
+__device__ __forceinline__ void tile_rows(const RescoreParams& p, uint32_t tacc, int t, int q, int lane, int4& part,
+                                          int& diag_ok, int& mat) {
+    const int row0 = 32 * q;
+    const int b = row0 / p.n;       // matrix of this warp within the tile
+    const int i0 = row0 - b * p.n;  // first row of the warp within the matrix
+    const int i = i0 + lane;
+    mat = t * p.mpt + b;
+    const int col0 = b * p.n;
+    const int nb = p.n / 32, rb = i0 / 32;
+    int s_abs = 0, s_nz = 0, s_sq = 0, dg = 0;
+    int o_abs = 0, o_nz = 0, o_sq = 0;
+    auto block = [&](int c, int& a_abs, int& a_nz, int& a_sq) {
+        int v[32];
+        tmem_ld32(tacc + ((uint32_t)row0 << 16) + (uint32_t)(col0 + c), v);
+#pragma unroll
+        for (int j = 0; j < 32; j += 2) {
+            const int a0 = abs(v[j]), a1 = abs(v[j + 1]);
+            a_abs += a0 + a1;
+            a_nz += min(a0, 1) + min(a1, 1);
+            a_sq += v[j] * v[j] + v[j + 1] * v[j + 1];
+        }
+        if (c == i0) {
+            int d = v[0];
+#pragma unroll
+            for (int j = 1; j < 32; ++j) d = lane == j ? v[j] : d;
+            dg = d;
+        }
+        if (p.gram && mat < p.count) {
+            int32_t* dst = p.gram + (size_t)mat * p.n * p.n + (size_t)i * p.n + c;
+            if (((uintptr_t)p.gram & 15u) == 0) {   // 16-byte stores need a 16-byte aligned base
+                int4* d4 = reinterpret_cast<int4*>(dst);
+#pragma unroll
+                for (int j = 0; j < 32; j += 4) d4[j / 4] = make_int4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) dst[j] = v[j];
+            }
+        }
+    };
+    // G is symmetric: without a Gram output each unordered pair of
+    // off-diagonal 32x32 blocks is read once, by the warp of one of its two
+    // row blocks (offsets d = 1..nb/2 cyclically), and counted twice; the
+    // diagonal entry (lane j of the warp's diagonal block) is taken out after
+    if (p.gram) {
+        for (int c = 0; c < p.n; c += 32) block(c, s_abs, s_nz, s_sq);
+    } else {
+        block(i0, s_abs, s_nz, s_sq);
+        for (int d = 1; 2 * d <= nb; ++d) {
+            if (2 * d == nb && rb >= d) continue;
+            block(((rb + d) % nb) * 32, o_abs, o_nz, o_sq);
+        }
+    }
+    s_abs += 2 * o_abs - abs(dg);
+    s_nz += 2 * o_nz - min(abs(dg), 1);
+    s_sq += 2 * o_sq - dg * dg;
+    // a zero-padded matrix: its own rows carry w on the diagonal, the
+    // padding rows 0 (their off-diagonal entries are 0 anyway)
+    int nv = p.n, wv = p.w;
+    if (p.dims && mat < p.count) {
+        const int2 d = p.dims[mat];
+        nv = d.x;
+        wv = d.y;
+    }
+    diag_ok = i < nv ? dg == wv : dg == 0;
+    part.x = __reduce_add_sync(0xffffffffu, s_abs);
+    part.y = __reduce_add_sync(0xffffffffu, s_nz);
+    part.z = __reduce_add_sync(0xffffffffu, s_sq);
+    diag_ok = (int)__reduce_and_sync(0xffffffffu, (unsigned)diag_ok);
+}
+
+// symmetric G: the off-diagonal sums count each pair twice
+__device__ __forceinline__ int4 matrix_stats(int abs_sum, int nz_sum, int sq_sum, int diag_ok) {
+    return make_int4(abs_sum / 2, nz_sum / 2, sq_sum / 2, (nz_sum == 0 && diag_ok) ? 1 : 0);
+}
+
+__global__ void __launch_bounds__(kThreads, kCtasPerSm) rescore_tc_kernel(const __grid_constant__ CUtensorMap tmap,
+                                                                 RescoreParams p) {
     extern __shared__ uint8_t smem_raw[];
     // tiles on a 1024-byte boundary (the 128-byte swizzle pattern repeats every 1024 bytes)
     uint8_t* tiles = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     __shared__ __align__(8) uint64_t full_bar[kStages];
-    __shared__ __align__(8) uint64_t mma_bar;
+    __shared__ __align__(8) uint64_t empty_bar[kStages];
+    __shared__ __align__(8) uint64_t accf_bar[kAccs];
+    __shared__ __align__(8) uint64_t acce_bar[kAccs];
     __shared__ uint32_t tmem_base_sh;
-    __shared__ int abort_sh;
-    __shared__ int4 warp_part[4];
-    __shared__ int warp_diag_ok[4];
+    __shared__ volatile int abort_sh;
+    // cross-warp sums of matrices that span several lane quarters (n >= 64):
+    // per group, kCombineSlots tiles in flight, two matrices per tile at
+    // most; fields abs, nonzero, squared, diagonal-ok, arrivals
+    __shared__ int comb_sh[kGroups][kCombineSlots][2][5];
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    if (warp == 0) {
+    if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_base_sh)),
                      "r"(kTmemCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        for (int s = 0; s < kStages; ++s) mbar_init(&full_bar[s], 1);
-        mbar_init(&mma_bar, 1);
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], 1);
+        }
+        for (int a = 0; a < kAccs; ++a) {
+            mbar_init(&accf_bar[a], 1);
+            mbar_init(&acce_bar[a], 4);   // the four warps of the group that owns the accumulator
+        }
         abort_sh = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int k = tid; k < kGroups * kCombineSlots * 2; k += blockDim.x) {
+        int* f = &comb_sh[0][0][0][0] + 5 * k;
+        f[0] = f[1] = f[2] = f[4] = 0;
+        f[3] = 1;
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
@@ -173,172 +324,106 @@ __global__ void __launch_bounds__(128, 4) rescore_tc_kernel(const __grid_constan
     const uint32_t tmem = tmem_base_sh;
 
     const int grid = gridDim.x;
+    // this CTA's tiles: blockIdx.x, blockIdx.x + grid, ...
+    const int ntl = (int)blockIdx.x < p.ntiles ? (p.ntiles - 1 - (int)blockIdx.x) / grid + 1 : 0;
     // a TMA box delivers rows_per_tile rows of 128 bytes (zero fill included)
     const uint32_t box_bytes = 128u * (uint32_t)p.rows_per_tile;
-    int issued = 0;  // loads issued by this CTA (thread 0's count)
-    if (tid == 0) {
-        for (int s = 0; s < kStages; ++s) {
-            const int t = blockIdx.x + s * grid;
-            if (t >= p.ntiles) break;
-            mbar_expect_tx(&full_bar[s], box_bytes);
-            tma_load_2d(tiles + s * kTileBytes, &tmap, 0, t * p.rows_per_tile, &full_bar[s]);
-            ++issued;
+    constexpr int S = kStages;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int it = 0;
+            for (; it < ntl && !abort_sh; ++it) {
+                const int s = it % S;
+                if (it >= S && !mbar_wait(&empty_bar[s], (uint32_t)(it / S - 1) & 1u)) {
+                    rescore_fail(p, &abort_sh, 3);
+                    break;
+                }
+                mbar_expect_tx(&full_bar[s], box_bytes);
+                tma_load_2d(tiles + s * kTileBytes, &tmap, 0, ((int)blockIdx.x + it * grid) * p.rows_per_tile,
+                            &full_bar[s]);
+            }
+            // drain: the loads still in flight are among the last S
+            // issued (earlier ones were consumed before their stage came back)
+            for (int k = it > S ? it - S : 0; k < it; ++k)
+                mbar_wait(&full_bar[k % S], (uint32_t)(k / S) & 1u);
         }
-    }
-    const uint32_t idesc = instr_desc(p.rows_per_tile);
-    // K steps of 32 columns that hold matrix entries; the box's columns past
-    // n are zero-filled by the TMA load and add nothing to the product
-    const int ksteps = (p.n + 31) / 32;
-    int iter = 0;
-    for (int t = blockIdx.x; t < p.ntiles; t += grid, ++iter) {
-        const int s = iter % kStages;
-        const uint32_t phase = (uint32_t)(iter / kStages) & 1u;
-        if (tid == 0 && !abort_sh) {
-            if (!mbar_wait(&full_bar[s], phase)) {
-                atomicExch(p.error, 1);
-                abort_sh = 1;
-            } else {
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = instr_desc(p.rows_per_tile);
+            // K steps of 32 columns that hold matrix entries; the box's
+            // columns past n are zero-filled by the TMA load and add nothing
+            const int ksteps = (p.n + 31) / 32;
+            int it = 0;
+            for (; it < ntl && !abort_sh; ++it) {
+                const int s = it % S, a = it % kAccs;
+                if (!mbar_wait(&full_bar[s], (uint32_t)(it / S) & 1u)) {
+                    rescore_fail(p, &abort_sh, 1);
+                    break;
+                }
+                if (it >= kAccs && !mbar_wait(&acce_bar[a], (uint32_t)(it / kAccs - 1) & 1u)) {
+                    rescore_fail(p, &abort_sh, 4);
+                    break;
+                }
                 asm volatile("tcgen05.fence::after_thread_sync;");
                 const uint64_t d = smem_desc(tiles + s * kTileBytes);
+                const uint32_t tacc = tmem + (uint32_t)(a * kAccCols);
 #pragma unroll 1
                 for (int k = 0; k < ksteps; ++k)
-                    mma_i8(tmem, d + (uint64_t)(2 * k), d + (uint64_t)(2 * k), idesc, k > 0);
-                mma_commit(&mma_bar);
+                    mma_i8(tacc, d + (uint64_t)(2 * k), d + (uint64_t)(2 * k), idesc, k > 0);
+                mma_commit(&empty_bar[s]);
+                mma_commit(&accf_bar[a]);
+            }
+            // every MMA issued has completed once the last commit arrived
+            if (it > 0) mbar_wait(&accf_bar[(it - 1) % kAccs], (uint32_t)((it - 1) / kAccs) & 1u);
+        }
+    } else {
+        const int e = warp - 2, g = e >> 2, q = warp & 3;
+        const bool active = 32 * q < p.rows_per_tile;
+        const int wpm = (p.n + 31) / 32;   // warps (lane quarters) per matrix
+        for (int it = g; it < ntl; it += kGroups) {
+            if (abort_sh) break;
+            const int a = it % kAccs;
+            if (!mbar_wait(&accf_bar[a], (uint32_t)(it / kAccs) & 1u)) {
+                rescore_fail(p, &abort_sh, 2);
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const int t = (int)blockIdx.x + it * grid;
+            int4 part = make_int4(0, 0, 0, 0);
+            int diag_ok = 1, mat = 0;
+            if (active) tile_rows(p, tmem + (uint32_t)(a * kAccCols), t, q, lane, part, diag_ok, mat);
+            // the accumulator is free for the MMA of a later tile
+            asm volatile("tcgen05.fence::before_thread_sync;");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acce_bar[a]);
+            if (!active || lane != 0 || mat >= p.count) continue;
+            if (wpm == 1) {
+                p.stats[mat] = matrix_stats(part.x, part.y, part.z, diag_ok);
+                continue;
+            }
+            // the last of the matrix's warps to arrive writes its stats and
+            // resets the slot; a slot is reused kCombineSlots tiles later,
+            // when every warp of the group has long finished this tile
+            int* f = comb_sh[g][(it / kGroups) % kCombineSlots][(32 * q) / p.n];
+            atomicAdd(&f[0], part.x);
+            atomicAdd(&f[1], part.y);
+            atomicAdd(&f[2], part.z);
+            atomicAnd(&f[3], diag_ok);
+            __threadfence_block();
+            if (atomicAdd(&f[4], 1) == wpm - 1) {
+                __threadfence_block();
+                const int sa = atomicExch(&f[0], 0), sn = atomicExch(&f[1], 0), sq = atomicExch(&f[2], 0),
+                          ok = atomicExch(&f[3], 1);
+                atomicExch(&f[4], 0);
+                p.stats[mat] = matrix_stats(sa, sn, sq, ok);
             }
         }
-        __syncthreads();
-        if (abort_sh) break;
-        if (!mbar_wait(&mma_bar, (uint32_t)iter & 1u)) {
-            atomicExch(p.error, 2);
-            abort_sh = 1;
-        }
-        __syncthreads();
-        if (abort_sh) {
-            // the MMA may still be running: give it one more bounded wait
-            // before the accumulator is released
-            if (tid == 0) mbar_wait(&mma_bar, (uint32_t)iter & 1u);
-            break;
-        }
-        asm volatile("tcgen05.fence::after_thread_sync;");
-        // stage s is free again: fetch the tile kStages iterations ahead
-        if (tid == 0) {
-            const int tn = t + kStages * grid;
-            if (tn < p.ntiles) {
-                mbar_expect_tx(&full_bar[s], box_bytes);
-                tma_load_2d(tiles + s * kTileBytes, &tmap, 0, tn * p.rows_per_tile, &full_bar[s]);
-                ++issued;
-            }
-        }
-        // epilogue: warp w reads D rows 32w..32w+31 (its TMEM lane quarter)
-        // and sums |G|, [G != 0] and G^2 per row; the diagonal entry (lane j
-        // of the warp's diagonal 32x32 block) is taken out after.  G is
-        // symmetric, so without a Gram output each unordered pair of
-        // off-diagonal 32x32 blocks is read once, by the warp of one of its
-        // two row blocks (offsets d = 1..nb/2 cyclically), and counted twice.
-        const int row0 = 32 * warp;
-        const bool active = row0 < p.rows_per_tile;
-        int4 part = make_int4(0, 0, 0, 0);
-        int diag_ok = 1;
-        if (active) {
-            const int b = row0 / p.n;       // matrix of this warp within the tile
-            const int i0 = row0 - b * p.n;  // first row of the warp within the matrix
-            const int i = i0 + lane;
-            const int mat = t * p.mpt + b;
-            const int col0 = b * p.n;
-            const int nb = p.n / 32, rb = i0 / 32;
-            int s_abs = 0, s_nz = 0, s_sq = 0, dg = 0;
-            int o_abs = 0, o_nz = 0, o_sq = 0;
-            auto block = [&](int c, int& a_abs, int& a_nz, int& a_sq) {
-                int v[32];
-                tmem_ld32(tmem + ((uint32_t)row0 << 16) + (uint32_t)(col0 + c), v);
-#pragma unroll
-                for (int j = 0; j < 32; j += 2) {
-                    const int a0 = abs(v[j]), a1 = abs(v[j + 1]);
-                    a_abs += a0 + a1;
-                    a_nz += min(a0, 1) + min(a1, 1);
-                    a_sq += v[j] * v[j] + v[j + 1] * v[j + 1];
-                }
-                if (c == i0) {
-                    int d = v[0];
-#pragma unroll
-                    for (int j = 1; j < 32; ++j) d = lane == j ? v[j] : d;
-                    dg = d;
-                }
-                if (p.gram && mat < p.count) {
-                    int32_t* dst = p.gram + (size_t)mat * p.n * p.n + (size_t)i * p.n + c;
-                    if (((uintptr_t)p.gram & 15u) == 0) {   // 16-byte stores need a 16-byte aligned base
-                        int4* d4 = reinterpret_cast<int4*>(dst);
-#pragma unroll
-                        for (int j = 0; j < 32; j += 4) d4[j / 4] = make_int4(v[j], v[j + 1], v[j + 2], v[j + 3]);
-                    } else {
-#pragma unroll
-                        for (int j = 0; j < 32; ++j) dst[j] = v[j];
-                    }
-                }
-            };
-            if (p.gram) {
-                for (int c = 0; c < p.n; c += 32) block(c, s_abs, s_nz, s_sq);
-            } else {
-                block(i0, s_abs, s_nz, s_sq);
-                for (int d = 1; 2 * d <= nb; ++d) {
-                    if (2 * d == nb && rb >= d) continue;
-                    block(((rb + d) % nb) * 32, o_abs, o_nz, o_sq);
-                }
-            }
-            s_abs += 2 * o_abs - abs(dg);
-            s_nz += 2 * o_nz - min(abs(dg), 1);
-            s_sq += 2 * o_sq - dg * dg;
-            // a zero-padded matrix: its own rows carry w on the diagonal,
-            // the padding rows 0 (their off-diagonal entries are 0 anyway)
-            int nv = p.n, wv = p.w;
-            if (p.dims && mat < p.count) {
-                const int2 d = p.dims[mat];
-                nv = d.x;
-                wv = d.y;
-            }
-            diag_ok = i < nv ? dg == wv : dg == 0;
-            part.x = __reduce_add_sync(0xffffffffu, s_abs);
-            part.y = __reduce_add_sync(0xffffffffu, s_nz);
-            part.z = __reduce_add_sync(0xffffffffu, s_sq);
-            diag_ok = (int)__reduce_and_sync(0xffffffffu, (unsigned)diag_ok);
-        }
-        if (lane == 0) {
-            warp_part[warp] = part;
-            warp_diag_ok[warp] = diag_ok;
-        }
-        asm volatile("tcgen05.fence::before_thread_sync;");
-        __syncthreads();
-        // one thread per matrix of the tile combines its warps
-        if (tid < p.mpt) {
-            const int mat = t * p.mpt + tid;
-            if (mat < p.count) {
-                const int wpm = (p.n + 31) / 32;   // warps per matrix
-                int4 tot = make_int4(0, 0, 0, 1);
-                for (int q = tid * wpm; q < tid * wpm + wpm && q < 4; ++q) {
-                    tot.x += warp_part[q].x;
-                    tot.y += warp_part[q].y;
-                    tot.z += warp_part[q].z;
-                    tot.w &= warp_diag_ok[q];
-                }
-                // symmetric G: the off-diagonal sums count each pair twice
-                int4 o;
-                o.x = tot.x / 2;
-                o.y = tot.y / 2;
-                o.z = tot.z / 2;
-                o.w = (tot.y == 0 && tot.w) ? 1 : 0;
-                p.stats[mat] = o;
-            }
-        }
-        __syncthreads();
-    }
-    // drain: wait (bounded) for this CTA's loads that are still in flight
-    if (tid == 0) {
-        for (int k = iter; k < issued; ++k) mbar_wait(&full_bar[k % kStages], (uint32_t)(k / kStages) & 1u);
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
-    if (warp == 0)
+    if (warp == 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
 }
 
@@ -459,14 +544,10 @@ int32_t rescore_device(const int8_t* W, int64_t count, int n, int w, int32_t* st
     const size_t smem = (size_t)kStages * kTileBytes + 1024;
     e = cudaFuncSetAttribute(rescore_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return rfail(XW_ERR_CUDA, std::string("rescore attribute: ") + cudaGetErrorString(e));
-    cudaFuncSetAttribute(rescore_tc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    // four CTAs per SM (shared memory: 4 x 50 KB; TMEM: 4 x 128 of 512
-    // columns) so that one CTA's epilogue overlaps the others' loads and
-    // MMAs (measured: 3 CTAs x 4 stages 0.349 ms, 4 x 3 0.303 ms at n=128);
-    // the tile loop is grid-strided, so fewer resident CTAs only serialise,
-    // never skip, tiles
-    const int blocks = (int)std::min<int64_t>(p.ntiles, (int64_t)4 * sms);
-    rescore_tc_kernel<<<blocks, 128, smem, stream>>>(map, p);
+    // kCtasPerSm persistent CTAs per SM; the tile loop is grid-strided, so
+    // fewer resident CTAs only serialise, never skip, tiles
+    const int blocks = (int)std::min<int64_t>(p.ntiles, (int64_t)kCtasPerSm * sms);
+    rescore_tc_kernel<<<blocks, kThreads, smem, stream>>>(map, p);
     e = cudaGetLastError();
     return e == cudaSuccess ? XW_OK : rfail(XW_ERR_CUDA, std::string("rescore launch: ") + cudaGetErrorString(e));
 }
