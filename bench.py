@@ -536,28 +536,48 @@ LARGE_N, LARGE_W, LARGE_R = 276, 275, 2368
 
 
 def large_bench(X, iters, ref_seconds):
-    """W(276,275) with 2368 replicas (16 warps on each of 148 SMs) and the
-    reference's defaults otherwise (t_init 6, t_min 0.1, cooling and reheat,
-    no restarts).  276 is about the largest order whose state the reference's
-    kernel holds in one CTA's shared memory; here it runs on the HBM-resident
-    kernel.  Beside it the reference's xweigh_cuda on the same order and
-    replica count."""
+    """W(276,275) with 2368 replicas and the reference's defaults otherwise
+    (t_init 6, t_min 0.1, cooling and reheat, no restarts).  276 is about the
+    largest order whose state the reference's kernel holds in one CTA's
+    shared memory; here it runs on the large-order kernel, in both its forms
+    (the Gram matrix in HBM, 16 warps per SM; bit planes in shared memory,
+    8 warps per SM).  Beside it the reference's xweigh_cuda on the same order
+    and replica count."""
     p = X.Params(stop_on_solve=0, t_init=6.0, t_min=0.1, moves_per_launch=1000,
                  squared_objective_fraction=0.0, parity_objective_fraction=0.0)
-    b = X.Batch([{"n": LARGE_N, "w": LARGE_W, "seed": 1, "replicas": LARGE_R}], p)
-    b.run(1000)          # the first launch builds each replica's Gram arena
-    b.synchronize()
-    m0 = b.results()[0][0].moves
-    b.run_timed(iters)
-    b.synchronize()
-    ms = sum(b.launch_times())
-    r = b.results()[0][0]
-    b.close()
-    moves = r.moves - m0
+
+    def form(planes):
+        # XW_LARGE_PLANES selects the kernel's form when the batch is built
+        old = os.environ.get("XW_LARGE_PLANES")
+        os.environ["XW_LARGE_PLANES"] = "1" if planes else "0"
+        try:
+            b = X.Batch([{"n": LARGE_N, "w": LARGE_W, "seed": 1, "replicas": LARGE_R}], p)
+        finally:
+            if old is None:
+                del os.environ["XW_LARGE_PLANES"]
+            else:
+                os.environ["XW_LARGE_PLANES"] = old
+        (cls,) = b.classes()
+        b.run(1000)          # the first launch builds each replica's arena (Gram matrix, or planes and residuals)
+        b.synchronize()
+        r0 = b.results()[0][0]
+        b.run_timed(iters)
+        b.synchronize()
+        ms = sum(b.launch_times())
+        r = b.results()[0][0]
+        b.close()
+        moves = r.moves - r0.moves
+        return {"moves": moves, "ms": ms, "moves_per_sec": moves / (ms / 1e3), "error": r.error,
+                "candidate_evaluations": r.candidate_evaluations - r0.candidate_evaluations,
+                "two_row_evaluations": r.two_row_evaluations - r0.two_row_evaluations,
+                "accepted_moves": r.accepted_moves - r0.accepted_moves,
+                "launch_class": cls,
+                "kernel": "anneal_large_kernel, " + ("bit planes in shared memory, Gram entries recomputed"
+                                                     if cls["large"] == 2 else "Gram matrix in HBM")}
+
     out = {"workload": f"W({LARGE_N},{LARGE_W}) x {LARGE_R} replicas, cooling from T 6 (t_min 0.1), L1 objective, "
                        f"the reference's moves, {iters} iterations per replica",
-           "device": {"moves": moves, "ms": ms, "moves_per_sec": moves / (ms / 1e3), "error": r.error,
-                      "kernel": "anneal_large_kernel (replica state in HBM)"}}
+           "device": form(False), "device_bit_planes": form(True)}
     if ref_seconds > 0 and os.path.exists(REF_XWEIGH_CUDA):
         try:
             mv, secs = run_reference_cuda(ref_seconds, n=LARGE_N, w=LARGE_W, replicas=LARGE_R)

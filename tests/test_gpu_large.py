@@ -1,4 +1,6 @@
-"""The HBM-resident kernel for orders above the shared-memory classes.
+"""The kernel for orders above the shared-memory classes, in both its forms:
+the Gram matrix stored in HBM (the default), and bit planes in shared memory
+with the Gram entries recomputed (orders up to 448, XW_LARGE_PLANES=1).
 
 Its replicas follow the same draw layout and move rules as the shared-memory
 kernel, so the CPU oracle replays them bit for bit: W, best W, minority
@@ -21,6 +23,13 @@ def large_from(monkeypatch):
     def set_order(n):
         monkeypatch.setenv("XW_LARGE_MIN_ORDER", str(n))
     return set_order
+
+
+@pytest.fixture(params=["planes", "gram"])
+def form(request, monkeypatch):
+    """Both forms of the large-order kernel."""
+    monkeypatch.setenv("XW_LARGE_PLANES", "1" if request.param == "planes" else "0")
+    return request.param
 
 
 def run_and_replay(n, w, R, iters, kw, seed):
@@ -52,7 +61,7 @@ SMALL_CASES = [
 
 
 @pytest.mark.parametrize("n,w,R,iters,kw", SMALL_CASES, ids=lambda v: str(v) if not isinstance(v, dict) else "")
-def test_small_orders_through_the_large_kernel_match_oracle(large_from, n, w, R, iters, kw):
+def test_small_orders_through_the_large_kernel_match_oracle(large_from, form, n, w, R, iters, kw):
     large_from(1)
     run_and_replay(n, w, R, iters, kw, 3000 + n * 7 + w).close()
 
@@ -70,8 +79,20 @@ LARGE_CASES = [
 
 
 @pytest.mark.parametrize("n,w,R,iters,kw", LARGE_CASES, ids=lambda v: str(v) if not isinstance(v, dict) else "")
-def test_large_orders_match_oracle(n, w, R, iters, kw):
+def test_large_orders_match_oracle(form, n, w, R, iters, kw):
     run_and_replay(n, w, R, iters, kw, 5000 + n * 7 + w).close()
+
+
+@pytest.mark.parametrize("n,w,planes", [(276, 275, True), (448, 447, True), (449, 448, False), (1024, 1000, False)])
+def test_large_class_reports_its_form(monkeypatch, n, w, planes):
+    """Bit planes up to order 448, the stored Gram matrix above it and
+    whenever XW_LARGE_PLANES=0."""
+    for allowed in ("1", "0"):
+        monkeypatch.setenv("XW_LARGE_PLANES", allowed)
+        b = X.Batch([{"n": n, "w": w, "seed": 1, "replicas": 2}], X.Params(stop_on_solve=0))
+        (c,) = b.classes()
+        assert c["large"] == (2 if planes and allowed == "1" else 1)
+        b.close()
 
 
 def test_both_kernels_agree_on_a_mixed_batch(large_from):

@@ -18,6 +18,12 @@
 // it is built once from W with popcounts over the sign and support masks,
 // and rebuilt whenever the host replaces W (restarts, snapshots).
 //
+// A second form, the bit-plane form (orders up to 448, selected by the
+// host), stores no G: W sits in the warp's slot as support and sign bit
+// planes and each Gram entry an evaluation or commit needs is recomputed by
+// popcounts, so a move makes no HBM traffic; its arena keeps residuals,
+// planes and the best state's planes between launches.
+//
 // The iteration is the one of xw_anneal.cu with the same draw layout, the
 // same proposal order and the same tie rules, so a replica's trajectory is
 // identical in both kernels and the CPU replay checks either.  Two
@@ -38,6 +44,10 @@ constexpr unsigned FULL = 0xffffffffu;
 constexpr uint32_t kThrTable = 64;
 
 // Replica-constant fields the proposal code reads, in the warp's slot.
+// Support mask word k of row r is mask[r * mrs + k * mks] (in u64 words):
+// the Gram arena's row-major masks (mrs = nw, mks = 1), or the bit planes
+// in shared memory (mrs = 2, mks = 2n; the sign word follows each support
+// word), from which `planes` replicas also read W's entries.
 struct LView {
     const int8_t* W;
     const uint16_t* mino;
@@ -46,25 +56,75 @@ struct LView {
     const uint32_t* dw;
     uint64_t thr_target, thr_dbl, thr_sign, thr_swsign;
     int n, w, m, sparse, ts, bpc, cc, move_set, nw;
-    uint32_t stream, k0, k1, pad;
+    int mrs, mks, planes;
+    uint32_t stream, k0, k1;
 };
 
+// Shared memory per warp.  Every replica: residuals (int32 x n), the
+// iteration's draw blocks, the view, the Metropolis thresholds.  A replica
+// in bit-plane mode adds W as support and sign planes, planes[q * n + o] =
+// {support word q of row o, sign word q of row o} (16 bytes; consecutive
+// rows consecutive, so a warp reading word q of its 32 rows reads 512
+// contiguous bytes), and its minority lists when they take at most
+// kMinoSmemBytes (off_mino 0: they stay in the record).
 struct LSlot {
-    uint32_t off_draws, off_view, off_thr, bytes;
+    uint32_t off_draws, off_view, off_thr, off_planes, off_mino, bytes;
 };
 
-__host__ __device__ inline LSlot large_slot(int n) {
+constexpr uint32_t kMinoSmemBytes = 8192;
+
+__host__ __device__ inline LSlot large_slot(int n, int m, bool planes) {
     LSlot L;
     L.off_draws = xw_pad16((uint32_t)n * 4u);
     L.off_view = L.off_draws + 32u * 16u;
     L.off_thr = L.off_view + xw_pad16((uint32_t)sizeof(LView));
     L.bytes = L.off_thr + kThrTable * 8u;
+    L.off_planes = L.off_mino = 0;
+    if (planes) {
+        const uint32_t nw = (uint32_t)(n + 63) / 64u;
+        L.off_planes = xw_pad16(L.bytes);
+        L.bytes = L.off_planes + nw * (uint32_t)n * 16u;
+        const uint32_t mb = (uint32_t)n * (uint32_t)m * 2u;
+        if (mb <= kMinoSmemBytes) {
+            L.off_mino = L.bytes;
+            L.bytes += xw_pad16(mb);
+        }
+    }
     return L;
 }
 
+// Bit-plane mode: orders whose warp slot fits kPlanesSlotMax (four warps
+// per CTA within the 227 KiB a CTA may hold), which bounds the plane words
+// per row by kPlanesNw (n <= 448).
+constexpr uint32_t kPlanesSlotMax = 56u * 1024u;
+constexpr int kPlanesNw = 7;
+
+__host__ __device__ inline bool large_planes_fit(int n, int m) {
+    return n <= 64 * kPlanesNw && large_slot(n, m, true).bytes <= kPlanesSlotMax;
+}
+
+// Arena per replica.  Stored-Gram form: G (int16, row-major), support and
+// sign masks.  Bit-plane form: the residuals, the planes and the best
+// state's planes, so that a launch resumes without rebuilding them and a
+// best state is saved with 16-byte copies (expanded to the record's int8
+// layout once, at the end of the launch).  XW_STATUS_GRAM: the arena holds
+// the record's W in that form.
 struct LGram {
     uint64_t off_mask, off_sign, bytes;
 };
+
+struct LPArena {
+    uint64_t off_planes, off_best, bytes;
+};
+
+__host__ __device__ inline LPArena planes_arena(int n) {
+    const uint64_t nw = (uint64_t)(n + 63) / 64;
+    LPArena A;
+    A.off_planes = ((uint64_t)n * 4u + 15u) & ~uint64_t(15);
+    A.off_best = A.off_planes + nw * (uint64_t)n * 16u;
+    A.bytes = A.off_best + nw * (uint64_t)n * 16u;
+    return A;
+}
 
 __host__ __device__ inline LGram large_gram(int n) {
     const uint64_t nw = (uint64_t)(n + 63) / 64;
@@ -93,11 +153,21 @@ __device__ __forceinline__ uint32_t l_index(const LView* v, uint64_t it, int c, 
     return draw_index(l_word(v, it, c, b, j), count, cand_slot(c, b), it, v->stream, v->k0, v->k1, j);
 }
 
-__device__ __forceinline__ int l_at(const LView* v, int r, int c) { return v->W[(size_t)c * v->n + r]; }
+// entry (r, c) of a bit-plane pair: 0, +1 or -1
+__device__ __forceinline__ int plane_entry(const uint64_t* e, int c) {
+    const int s = (int)((e[0] >> (c & 63)) & 1ull), g = (int)((e[1] >> (c & 63)) & 1ull);
+    return s - 2 * (s & g);
+}
+
+__device__ __forceinline__ int l_at(const LView* v, int r, int c) {
+    if (v->planes) return plane_entry(v->mask + (size_t)r * v->mrs + (size_t)(c >> 6) * v->mks, c);
+    return v->W[(size_t)c * v->n + r];
+}
 
 // word k of a row's support mask, or of its zero set (columns < n)
-__device__ __forceinline__ uint64_t mask_word(const uint64_t* row, int k, int nw, int n, bool zeros) {
-    uint64_t x = row[k];
+__device__ __forceinline__ uint64_t mask_word(const LView* v, int row, int k, bool zeros) {
+    const int nw = v->nw, n = v->n;
+    uint64_t x = v->mask[(size_t)row * v->mrs + (size_t)k * v->mks];
     if (zeros) {
         x = ~x;
         if (k == nw - 1 && (n & 63)) x &= (1ull << (n & 63)) - 1ull;
@@ -106,17 +176,18 @@ __device__ __forceinline__ uint64_t mask_word(const uint64_t* row, int k, int nw
 }
 
 // first set bit at or after `start`, cyclically
-__device__ __noinline__ int l_cyclic_first(const uint64_t* row, int nw, int n, int start, bool zeros) {
+__device__ __noinline__ int l_cyclic_first(const LView* v, int row, int start, bool zeros) {
+    const int nw = v->nw;
     const int ws = start >> 6;
 #pragma unroll 1
     for (int k = ws; k < nw; ++k) {
-        uint64_t x = mask_word(row, k, nw, n, zeros);
+        uint64_t x = mask_word(v, row, k, zeros);
         if (k == ws) x &= ~0ull << (start & 63);
         if (x) return 64 * k + __ffsll((long long)x) - 1;
     }
 #pragma unroll 1
     for (int k = 0; k <= ws && k < nw; ++k) {
-        const uint64_t x = mask_word(row, k, nw, n, zeros);
+        const uint64_t x = mask_word(v, row, k, zeros);
         if (x) return 64 * k + __ffsll((long long)x) - 1;
     }
     return -1;
@@ -150,7 +221,7 @@ __device__ __forceinline__ LMove lpack(int kind, int r1, int r2, int c1, int c2,
 __device__ __noinline__ int l_flip_col(const LView* v, uint64_t it, int c, int b, int j, int row) {
     if (v->sparse && v->m > 0) return v->mino[(size_t)row * v->m + (int)l_index(v, it, c, b, j, (uint32_t)v->m)];
     const int start = (int)l_index(v, it, c, b, j, (uint32_t)v->n);
-    return l_cyclic_first(v->mask + (size_t)row * v->nw, v->nw, v->n, start, false);
+    return l_cyclic_first(v, row, start, false);
 }
 
 // hot_row (xweigh_cuda.cu:291-300), serial form
@@ -205,16 +276,15 @@ __device__ __noinline__ LMove l_switch(const LView* v, uint64_t it, int c, int r
 // within-row swap: a nonzero of the row moves to one of its zeros
 __device__ __noinline__ LMove l_row_swap(const LView* v, uint64_t it, int c, int row) {
     if (v->m == 0) return none();
-    const uint64_t* nz = v->mask + (size_t)row * v->nw;
     int c1, c2, pos;
     if (v->sparse) {
         pos = (int)l_index(v, it, c, 1, 1, (uint32_t)v->m);
         c1 = v->mino[(size_t)row * v->m + pos];
-        c2 = l_cyclic_first(nz, v->nw, v->n, (int)l_index(v, it, c, 1, 2, (uint32_t)v->n), true);
+        c2 = l_cyclic_first(v, row, (int)l_index(v, it, c, 1, 2, (uint32_t)v->n), true);
     } else {
         pos = (int)l_index(v, it, c, 1, 2, (uint32_t)v->m);
         c2 = v->mino[(size_t)row * v->m + pos];
-        c1 = l_cyclic_first(nz, v->nw, v->n, (int)l_index(v, it, c, 1, 1, (uint32_t)v->n), false);
+        c1 = l_cyclic_first(v, row, (int)l_index(v, it, c, 1, 1, (uint32_t)v->n), false);
     }
     if (c1 < 0 || c2 < 0) return none();
     return lpack(3, row, 0, c1, c2, l_word(v, it, c, 1, 3) < 0x80000000u ? 1 : -1, 0, pos, 0, l_at(v, row, c1), 0);
@@ -473,6 +543,209 @@ __device__ void l_commit(const LMove& mv, const LUpdate& u, int ds, int8_t* W, i
     __syncwarp();
 }
 
+// ---------------------------------------------------------------------------
+// Bit-plane mode.  No Gram matrix is stored: the entries an evaluation or a
+// commit needs are recomputed from the planes in shared memory,
+// G[r][o] = |S_r & S_o| - 2 |S_r & S_o & (N_r ^ N_o)| (S: support, N: sign
+// bits), and a commit changes only the planes, the residuals and the
+// minority lists.  A move costs no HBM traffic and no scattered stores; the
+// price is the popcount arithmetic, about 12 instructions per 64 columns of
+// each Gram entry read.  The deltas, ties and trajectory are those of the
+// stored-Gram form.
+
+__device__ __forceinline__ int p_at(const ulonglong2* P, int n, int r, int c) {
+    return plane_entry(reinterpret_cast<const uint64_t*>(&P[(size_t)(c >> 6) * n + r]), c);
+}
+
+__device__ __forceinline__ void p_set(ulonglong2* P, int n, int r, int c, int v) {
+    ulonglong2& e = P[(size_t)(c >> 6) * n + r];
+    const uint64_t bit = 1ull << (c & 63);
+    e.x = v != 0 ? (e.x | bit) : (e.x & ~bit);
+    e.y = v < 0 ? (e.y | bit) : (e.y & ~bit);
+}
+
+__device__ __forceinline__ int p_dot(const ulonglong2* P, int n, int nw, int r, int o) {
+    int d = 0;
+#pragma unroll 1
+    for (int q = 0; q < nw; ++q) {
+        const ulonglong2 a = P[(size_t)q * n + r], b = P[(size_t)q * n + o];
+        const uint64_t both = a.x & b.x;
+        d += __popcll(both) - 2 * __popcll(both & (a.y ^ b.y));
+    }
+    return d;
+}
+
+__device__ __forceinline__ int p_pair_new(const LUpdate& u, int op, const ulonglong2* P, int n) {
+    return op + u.A1 * p_at(P, n, u.R2, u.X1) + u.A2 * p_at(P, n, u.R1, u.X2) + (u.X1 == u.X2 ? u.A1 * u.A2 : 0);
+}
+
+// One pass over the lane's rows o = lane, lane + 32, ... for a move's
+// updated rows R1 (and R2 when two): G[R1][o] (and G[R2][o]) by popcounts
+// over the plane words (row o's words read once for both rows; the updated
+// rows' words are broadcast reads), the new entries G + A W[o][X] + B W[o][Y],
+// and then either the objective deltas (evaluation) or the residual
+// updates (commit: res[o] changes, and the returned S1 sums R1's changes).
+// One small loop serves both, so that it stays in the instruction cache
+// and in registers.
+struct PRows {
+    LDeltas d;   // evaluation: the lane's objective deltas
+    int s1;      // commit: the lane's sum of R1's residual changes
+};
+
+template <bool GEN, bool TWO>
+__device__ __forceinline__ PRows p_rows(const LUpdate& u, const ulonglong2* P, int32_t* res, int n, int nw, int lane,
+                                     bool commit) {
+    PRows out = {{0, 0, 0, 0}, 0};
+    const ulonglong2* pa = P + u.R1;
+    const ulonglong2* pb = P + (TWO ? u.R2 : u.R1);
+#pragma unroll 1
+    for (int o = lane; o < n; o += 32) {
+        int g1 = 0, g2 = 0;
+#pragma unroll 1
+        for (int q = 0; q < nw; ++q) {
+            const size_t off = (size_t)q * n;
+            const ulonglong2 e = P[off + o], a = pa[off];
+            const uint64_t b1 = a.x & e.x;
+            g1 += __popcll(b1) - 2 * __popcll(b1 & (a.y ^ e.y));
+            if constexpr (TWO) {
+                const ulonglong2 b = pb[off];
+                const uint64_t b2 = b.x & e.x;
+                g2 += __popcll(b2) - 2 * __popcll(b2 & (b.y ^ e.y));
+            }
+        }
+        if (o == u.R1 || (TWO && o == u.R2)) continue;
+        int n1 = g1 + u.A1 * p_at(P, n, o, u.X1);
+        if (u.B1) n1 += u.B1 * p_at(P, n, o, u.Y1);
+        int n2 = g2;
+        if constexpr (TWO) {
+            n2 += u.A2 * p_at(P, n, o, u.X2);
+            if (u.B2) n2 += u.B2 * p_at(P, n, o, u.Y2);
+        }
+        if (commit) {
+            const int e1 = iabs(n1) - iabs(g1);
+            res[o] += TWO ? e1 + iabs(n2) - iabs(g2) : e1;
+            out.s1 += e1;
+        } else {
+            lacc<GEN>(out.d, g1, n1);
+            if constexpr (TWO) lacc<GEN>(out.d, g2, n2);
+        }
+    }
+    return out;
+}
+
+template <bool GEN>
+__device__ __forceinline__ PRows p_rows_any(const LUpdate& u, const ulonglong2* P, int32_t* res, int n, int nw,
+                                            int lane, bool commit) {
+    return u.R2 >= 0 ? p_rows<GEN, true>(u, P, res, n, nw, lane, commit)
+                     : p_rows<GEN, false>(u, P, res, n, nw, lane, commit);
+}
+
+// l_eval on the planes
+template <bool GEN>
+__device__ __forceinline__ LDeltas p_eval(const LUpdate& u, const ulonglong2* P, int n, int nw, int lane) {
+    LDeltas d = p_rows_any<GEN>(u, P, nullptr, n, nw, lane, false).d;
+    if (u.pair && lane == 0) {
+        const int op = p_dot(P, n, nw, u.R1, u.R2);
+        lacc<GEN>(d, op, p_pair_new(u, op, P, n));
+    }
+    return d;
+}
+
+// l_commit on the planes: residuals from the recomputed rows, then the
+// changed entries (lane 0, after every lane has read the old planes)
+template <bool GEN>
+__device__ void p_commit(const LMove& mv, const LUpdate& u, int ds, ulonglong2* P, int32_t* res, uint16_t* mino,
+                         int n, int m, int nw, int sparse, int lane) {
+    const int s1 = p_rows_any<GEN>(u, P, res, n, nw, lane, true).s1;
+    const int S1 = __reduce_add_sync(FULL, s1);
+    __syncwarp();
+    if (lane == 0) {
+        const int kind = (mv.x >> 1) & 3, r1 = (mv.x >> 3) & 1023, r2 = (mv.x >> 13) & 1023;
+        const int c1 = mv.y & 1023, c2 = (mv.y >> 10) & 1023;
+        const int nv1 = (int)((mv.y >> 20) & 3) - 1, nv2 = (int)((mv.y >> 22) & 3) - 1;
+        const int p1 = mv.z & 1023, p2 = (mv.z >> 10) & 1023;
+        const int o11 = (int)((mv.x >> 23) & 3) - 1, o22 = (int)((mv.x >> 25) & 3) - 1;
+        if (u.pair) {
+            const int op = p_dot(P, n, nw, r1, r2);
+            const int pd = iabs(p_pair_new(u, op, P, n)) - iabs(op);
+            res[r1] += S1 + pd;
+            res[r2] += ds - S1;
+        } else if (u.R2 >= 0) {
+            res[r1] += S1;
+            res[r2] += ds - S1;
+        } else {
+            res[r1] += ds;
+        }
+        if (kind == 0) {
+            p_set(P, n, r1, c1, -o11);
+        } else if (kind == 2) {
+            p_set(P, n, r1, c1, -o11);
+            p_set(P, n, r2, c2, -o22);
+        } else if (kind == 1) {
+            p_set(P, n, r1, c1, 0);
+            p_set(P, n, r2, c2, 0);
+            p_set(P, n, r1, c2, nv1);
+            p_set(P, n, r2, c1, nv2);
+            mino[(size_t)r1 * m + p1] = (uint16_t)(sparse ? c2 : c1);
+            mino[(size_t)r2 * m + p2] = (uint16_t)(sparse ? c1 : c2);
+        } else if (GEN) {
+            p_set(P, n, r1, c1, 0);
+            p_set(P, n, r1, c2, nv1);
+            mino[(size_t)r1 * m + p1] = (uint16_t)(sparse ? c2 : c1);
+        }
+    }
+    __syncwarp();
+}
+
+// Residuals and the totals of the lane's rows from the planes (a replica
+// whose planes were just built): every G[r][o], r != o
+__device__ __noinline__ void p_totals(const ulonglong2* P, int32_t* res, int n, int nw, int lane, int& score,
+                                      int& conf, long long& sq, int& par) {
+#pragma unroll 1
+    for (int o = lane; o < n; o += 32) {
+        int r_sum = 0;
+#pragma unroll 1
+        for (int r = 0; r < n; ++r) {
+            int g = 0;
+#pragma unroll 1
+            for (int q = 0; q < nw; ++q) {
+                const ulonglong2 x = P[(size_t)q * n + r], e = P[(size_t)q * n + o];
+                const uint64_t both = x.x & e.x;
+                g += __popcll(both) - 2 * __popcll(both & (x.y ^ e.y));
+            }
+            if (r != o) {
+                const int ag = iabs(g);
+                r_sum += ag;
+                conf += g != 0;
+                sq += (long long)(g * g);
+                par += ag & 1;
+            }
+        }
+        res[o] = r_sum;
+        score += r_sum;
+    }
+}
+
+// W (column-major int8, as in the record) from the planes (in shared
+// memory or in the arena): each lane expands its rows' words, the warp's
+// stores for one column are 32 consecutive bytes
+__device__ void p_store_w(int8_t* dst, const ulonglong2* P, int n, int lane) {
+    const int nw = (n + 63) / 64;
+#pragma unroll 1
+    for (int q = 0; q < nw; ++q) {
+        const int c1 = min(n, 64 * q + 64);
+#pragma unroll 1
+        for (int o = lane; o < n; o += 32) {
+            const ulonglong2 e = P[(size_t)q * n + o];
+#pragma unroll 4
+            for (int c = 64 * q; c < c1; ++c) {
+                const int s = (int)((e.x >> (c & 63)) & 1ull), g = (int)((e.y >> (c & 63)) & 1ull);
+                dst[(size_t)c * n + o] = (int8_t)(s - 2 * (s & g));
+            }
+        }
+    }
+}
+
 // tab[d-1] = ceil(exp(-d/T) * 2^32) (see build_thresholds, xw_anneal.cu)
 __device__ __noinline__ void l_thresholds(uint64_t* tab, double T, int lane) {
     const double t = T > 1.0e-12 ? T : 1.0e-12;
@@ -542,7 +815,7 @@ __device__ bool build_gram(const int8_t* W, int16_t* G, uint64_t* mask, uint64_t
     return ok;
 }
 
-template <bool GEN>
+template <bool GEN, bool PM>
 __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int lane, uint64_t chunk_iters) {
     uint8_t* rec = a.arena + a.rec_off[rid];
     RepHeader* H = reinterpret_cast<RepHeader*>(rec);
@@ -553,14 +826,25 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
 
     const int n = J->n, w = J->w, m = J->m, sparse = J->sparse;
     const int nw = (n + 63) / 64;
-    const LSlot L = large_slot(n);
-    const LGram LG = large_gram(n);
+    const LSlot L = large_slot(n, m, PM);
     int8_t* W = reinterpret_cast<int8_t*>(rec + J->off_w);
-    uint16_t* mino = reinterpret_cast<uint16_t*>(rec + J->off_mino);
-    uint8_t* gbase = a.gram + a.gram_off[rid];
-    int16_t* G = reinterpret_cast<int16_t*>(gbase);
-    uint64_t* mask = reinterpret_cast<uint64_t*>(gbase + LG.off_mask);
-    uint64_t* sign = reinterpret_cast<uint64_t*>(gbase + LG.off_sign);
+    uint16_t* const mino_rec = reinterpret_cast<uint16_t*>(rec + J->off_mino);
+    // bit-plane mode: W as planes in the slot; the arena keeps residuals,
+    // planes and the best state's planes between launches
+    ulonglong2* const P = PM ? reinterpret_cast<ulonglong2*>(slot + L.off_planes) : nullptr;
+    uint16_t* const mino = PM && L.off_mino ? reinterpret_cast<uint16_t*>(slot + L.off_mino) : mino_rec;
+    uint8_t* const parena = PM ? a.gram + a.gram_off[rid] : nullptr;
+    const LPArena PA = planes_arena(n);
+    const uint32_t plane_bytes = (uint32_t)nw * (uint32_t)n * 16u;
+    int16_t* G = nullptr;
+    uint64_t *mask = nullptr, *sign = nullptr;
+    if constexpr (!PM) {
+        const LGram LG = large_gram(n);
+        uint8_t* gbase = a.gram + a.gram_off[rid];
+        G = reinterpret_cast<int16_t*>(gbase);
+        mask = reinterpret_cast<uint64_t*>(gbase + LG.off_mask);
+        sign = reinterpret_cast<uint64_t*>(gbase + LG.off_sign);
+    }
     int32_t* sRes = reinterpret_cast<int32_t*>(slot);
     uint4* sDraw = reinterpret_cast<uint4*>(slot + L.off_draws);
     const uint32_t* sDw = reinterpret_cast<const uint32_t*>(sDraw);
@@ -574,9 +858,48 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
         if (iters > J->budget_iters - it) iters = J->budget_iters - it;
     }
 
-    // ---- Gram and masks (once per W the host wrote), minority lists ----
+    // ---- Gram and masks (once per W the host wrote), or the planes (every
+    // load); minority lists ----
     const uint32_t status0 = H->status;
-    if (!(status0 & XW_STATUS_GRAM)) {
+    const bool cached = PM && (status0 & XW_STATUS_GRAM);
+    if constexpr (PM) {
+        if (!large_planes_fit(n, m)) {
+            if (lane == 0) H->err |= XW_ERR_KERNEL;
+            return;
+        }
+    }
+    if (cached) {
+        l_copy16(P, parena + PA.off_planes, plane_bytes, lane);
+        l_copy16(sRes, parena, (uint32_t)n * 4u, lane);
+        if (m > 0 && mino != mino_rec) l_copy16(mino, mino_rec, (uint32_t)(n * m) * 2u, lane);
+        __syncwarp();
+    } else if constexpr (PM) {
+        bool ok = true;
+#pragma unroll 1
+        for (int o = lane; o < n; o += 32) {
+            int weight = 0;
+#pragma unroll 1
+            for (int q = 0; q < nw; ++q) {
+                uint64_t nz = 0, ng = 0;
+#pragma unroll 1
+                for (int c = 64 * q; c < n && c < 64 * q + 64; ++c) {
+                    const int v = W[(size_t)c * n + o];
+                    if (v != 0) nz |= 1ull << (c & 63);
+                    if (v < 0) ng |= 1ull << (c & 63);
+                }
+                P[(size_t)q * n + o] = make_ulonglong2(nz, ng);
+                weight += __popcll(nz);
+            }
+            if (weight != w) ok = false;
+        }
+        if (__any_sync(FULL, !ok)) {
+            if (lane == 0) H->err |= XW_ERR_MINORITY;
+            return;
+        }
+        if (m > 0 && (status0 & XW_STATUS_INIT) && mino != mino_rec)
+            l_copy16(mino, mino_rec, (uint32_t)(n * m) * 2u, lane);
+        __syncwarp();
+    } else if (!(status0 & XW_STATUS_GRAM)) {
         const bool ok = build_gram(W, G, mask, sign, n, w, nw, lane);
         if (__any_sync(FULL, !ok)) {
             if (lane == 0) H->err |= XW_ERR_MINORITY;
@@ -604,28 +927,36 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
         __syncwarp();
     }
 
-    // ---- residuals and totals from G ----
+    // ---- residuals and totals from G (a cached bit-plane replica: the
+    // score from its saved residuals, the other totals from its header) ----
     int p_score = 0, p_conf = 0, p_par = 0;
     long long p_sq = 0;
+    if (cached) {
 #pragma unroll 1
-    for (int o = lane; o < n; o += 32) {
-        int r_sum = 0;
+        for (int o = lane; o < n; o += 32) p_score += sRes[o];
+    } else if constexpr (PM) {
+        p_totals(P, sRes, n, nw, lane, p_score, p_conf, p_sq, p_par);
+    } else {
+#pragma unroll 1
+        for (int o = lane; o < n; o += 32) {
+            int r_sum = 0;
 #pragma unroll 4
-        for (int r = 0; r < n; ++r) {
-            const int g = G[(size_t)r * n + o];
-            if (r != o) {
-                const int ag = iabs(g);
-                r_sum += ag;
-                p_conf += g != 0;
-                p_sq += (long long)(g * g);
-                p_par += ag & 1;
+            for (int r = 0; r < n; ++r) {
+                const int g = G[(size_t)r * n + o];
+                if (r != o) {
+                    const int ag = iabs(g);
+                    r_sum += ag;
+                    p_conf += g != 0;
+                    p_sq += (long long)(g * g);
+                    p_par += ag & 1;
+                }
             }
+            sRes[o] = r_sum;
+            p_score += r_sum;
         }
-        sRes[o] = r_sum;
-        p_score += r_sum;
     }
     const int score0 = __reduce_add_sync(FULL, p_score) / 2;
-    const int conf0 = __reduce_add_sync(FULL, p_conf) / 2;
+    const int conf0 = cached ? H->conflicts : __reduce_add_sync(FULL, p_conf) / 2;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) p_sq += __shfl_xor_sync(FULL, p_sq, off);
     const long long sq0 = p_sq / 2;
@@ -637,7 +968,10 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
         if (lane == 0) H->err |= XW_ERR_KERNEL;
         return;
     }
-    const int64_t obj0 = obj_kind == 1 ? sq0 : obj_kind == 2 ? par0 : score0;
+    const int64_t obj0 = cached && obj_kind != 0 ? H->obj_total
+                         : obj_kind == 1         ? sq0
+                         : obj_kind == 2         ? par0
+                                                 : score0;
     int score, conflicts, best_s, best_c, msi, cool;
     int64_t obj_total;
     uint64_t moves, cand_evals;
@@ -681,12 +1015,23 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
     const bool coop = ts <= 8;
     if (lane == 0) {
         LView v;
-        v.W = W; v.mino = mino; v.res = sRes; v.mask = mask; v.dw = sDw;
+        v.W = W; v.mino = mino; v.res = sRes; v.dw = sDw;
+        if constexpr (PM) {
+            v.mask = reinterpret_cast<const uint64_t*>(P);
+            v.mrs = 2;
+            v.mks = 2 * n;
+            v.planes = 1;
+        } else {
+            v.mask = mask;
+            v.mrs = nw;
+            v.mks = 1;
+            v.planes = 0;
+        }
         v.thr_target = J->thr_target; v.thr_dbl = J->thr_double; v.thr_sign = J->thr_sign;
         v.thr_swsign = J->thr_swsign;
         v.n = n; v.w = w; v.m = m; v.sparse = sparse; v.ts = ts; v.bpc = bpc; v.cc = 31 / bpc;
         v.move_set = J->move_set; v.nw = nw;
-        v.stream = stream; v.k0 = k0; v.k1 = k1; v.pad = 0;
+        v.stream = stream; v.k0 = k0; v.k1 = k1;
         *sView = v;
     }
     __syncwarp();
@@ -699,6 +1044,7 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
     }
     uint8_t* best_dst = rec + J->off_best;
     const uint32_t nn = (uint32_t)(n * n);
+    bool best_saved = false;   // bit-plane form: a best state saved in the arena this run
 
     uint64_t done = 0;
 #pragma unroll 1
@@ -746,7 +1092,9 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
             e.y = __shfl_sync(FULL, desc.y, c);
             e.z = __shfl_sync(FULL, desc.z, c);
             const LUpdate u = l_decode(e);
-            const LDeltas d = l_eval<GEN>(u, W, G, n, lane);
+            LDeltas d;
+            if constexpr (PM) d = p_eval<GEN>(u, P, n, nw, lane);
+            else d = l_eval<GEN>(u, W, G, n, lane);
             const int ds = __reduce_add_sync(FULL, d.ds);
             const int dc = __reduce_add_sync(FULL, d.dc);
             int prim = ds;
@@ -780,12 +1128,18 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
         if (accept) {
             // leaving a best state without improving on it: its copy is due
             if (at_best && !(bds < 0 || (bds == 0 && bdc < 0))) {
-                l_copy16(best_dst, W, nn, lane);
+                if constexpr (PM) {
+                    l_copy16(parena + PA.off_best, P, plane_bytes, lane);
+                    best_saved = true;
+                } else {
+                    l_copy16(best_dst, W, nn, lane);
+                }
                 __syncwarp();
                 at_best = false;
             }
             const LUpdate u = l_decode(best_mv);
-            l_commit<GEN>(best_mv, u, bds, W, G, sRes, mino, mask, n, m, nw, sparse, lane);
+            if constexpr (PM) p_commit<GEN>(best_mv, u, bds, P, sRes, mino, n, m, nw, sparse, lane);
+            else l_commit<GEN>(best_mv, u, bds, W, G, sRes, mino, mask, n, m, nw, sparse, lane);
             score += bds;
             conflicts += bdc;
             obj_total += bprim;
@@ -828,7 +1182,24 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
     }
 
     __syncwarp();
-    if (at_best) l_copy16(best_dst, W, nn, lane);
+    if constexpr (PM) {
+        // the arena's planes and residuals, the record's W, best W and
+        // minority lists from the slot
+        l_copy16(parena + PA.off_planes, P, plane_bytes, lane);
+        l_copy16(parena, sRes, (uint32_t)n * 4u, lane);
+        if (at_best) {
+            p_store_w(reinterpret_cast<int8_t*>(best_dst), P, n, lane);
+        } else if (best_saved) {
+            __syncwarp();
+            p_store_w(reinterpret_cast<int8_t*>(best_dst),
+                      reinterpret_cast<const ulonglong2*>(parena + PA.off_best), n, lane);
+        }
+        p_store_w(W, P, n, lane);
+        if (m > 0 && mino != mino_rec) l_copy16(mino_rec, mino, (uint32_t)(n * m) * 2u, lane);
+        __syncwarp();
+    } else {
+        if (at_best) l_copy16(best_dst, W, nn, lane);
+    }
     if (lane == 0) {
         H->it = it;
         H->moves = moves;
@@ -849,12 +1220,15 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
     __syncwarp();
 }
 
-// CTAs of four warps per SM the register budget is sized for
+// CTAs of four warps per SM the register budget is sized for: the
+// stored-Gram form hides HBM latency with warps; the bit-plane form holds
+// two CTAs (its slots fill shared memory) and spends the registers on its
+// per-lane Gram rows
 #ifndef XW_LARGE_MIN_BLOCKS
 #define XW_LARGE_MIN_BLOCKS 4
 #endif
-template <bool GEN>
-__global__ void __launch_bounds__(128, XW_LARGE_MIN_BLOCKS) anneal_large_kernel(AnnealArgs a) {
+template <bool GEN, bool PM>
+__global__ void __launch_bounds__(128, PM ? 2 : XW_LARGE_MIN_BLOCKS) anneal_large_kernel(AnnealArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -868,7 +1242,7 @@ __global__ void __launch_bounds__(128, XW_LARGE_MIN_BLOCKS) anneal_large_kernel(
         item = __shfl_sync(FULL, item, 0);
         if (item >= total) break;
         if (a.chunks == 1) {
-            run_large<GEN>(a, a.items[item], slot, lane, a.iters);
+            run_large<GEN, PM>(a, a.items[item], slot, lane, a.iters);
             continue;
         }
         const uint32_t c = item / a.n_items;
@@ -876,28 +1250,35 @@ __global__ void __launch_bounds__(128, XW_LARGE_MIN_BLOCKS) anneal_large_kernel(
         const uint64_t lo = a.iters * c / a.chunks, hi = a.iters * (c + 1) / a.chunks;
         RepHeader* H = reinterpret_cast<RepHeader*>(a.arena + a.rec_off[rid]);
         const bool ok = chunk_begin(a.chunk_done + rid, c, a.chunk_wait_ns, &H->err, lane, FULL);
-        if (ok) run_large<GEN>(a, rid, slot, lane, hi - lo);
+        if (ok) run_large<GEN, PM>(a, rid, slot, lane, hi - lo);
         chunk_end(a.chunk_done + rid, c, ok, lane, FULL);
     }
 }
 
 }  // namespace
 
-uint32_t anneal_large_slot_bytes(int n) { return large_slot(n).bytes; }
+bool anneal_large_planes_fit(int n, int m) { return large_planes_fit(n, m); }
 
-uint64_t anneal_large_gram_bytes(int n) { return (large_gram(n).bytes + 255u) & ~uint64_t(255); }
+uint32_t anneal_large_slot_bytes(int n, int m, bool planes) { return large_slot(n, m, planes).bytes; }
 
-const void* anneal_large_kernel_fn(bool general) {
-    return general ? reinterpret_cast<const void*>(&anneal_large_kernel<true>)
-                   : reinterpret_cast<const void*>(&anneal_large_kernel<false>);
+uint64_t anneal_large_arena_bytes(int n, bool planes) {
+    return ((planes ? planes_arena(n).bytes : large_gram(n).bytes) + 255u) & ~uint64_t(255);
 }
 
-cudaError_t launch_anneal_large(const AnnealArgs& args, bool general, int warps_per_block, int blocks,
+const void* anneal_large_kernel_fn(bool general, bool planes) {
+    if (planes)
+        return general ? reinterpret_cast<const void*>(&anneal_large_kernel<true, true>)
+                       : reinterpret_cast<const void*>(&anneal_large_kernel<false, true>);
+    return general ? reinterpret_cast<const void*>(&anneal_large_kernel<true, false>)
+                   : reinterpret_cast<const void*>(&anneal_large_kernel<false, false>);
+}
+
+cudaError_t launch_anneal_large(const AnnealArgs& args, bool general, bool planes, int warps_per_block, int blocks,
                                 cudaStream_t stream) {
     const size_t smem = (size_t)warps_per_block * args.slot_bytes;
     const dim3 grid(blocks), block(32 * warps_per_block);
     void* kargs[] = {const_cast<AnnealArgs*>(&args)};
-    return cudaLaunchKernel(anneal_large_kernel_fn(general), grid, block, kargs, smem, stream);
+    return cudaLaunchKernel(anneal_large_kernel_fn(general, planes), grid, block, kargs, smem, stream);
 }
 
 }  // namespace xw

@@ -141,6 +141,16 @@ int large_min_order() {
     return std::clamp(std::atoi(e), 1, XW_MAX_N + 1);
 }
 
+// XW_LARGE_PLANES=1 runs large-order launches in bit-plane form where the
+// orders fit it (no Gram arena: a quarter of the device memory per replica
+// at n = 276 and no HBM traffic per move); the stored-Gram form is the
+// default, being faster where both were measured (W(276,275) on B200: 69
+// against 60 M moves/s)
+static bool large_planes_allowed() {
+    const char* e = std::getenv("XW_LARGE_PLANES");
+    return e && std::atoi(e) != 0;
+}
+
 std::string validate(int n, int w, const xw_params& p) {
     if (n < 1 || n > 32767) return "CUDA xweigh order is out of range";
     if (w < 1 || w > n) return "CUDA xweigh weight must be in [1, n]";
@@ -408,6 +418,11 @@ void Batch::derive_layout() {
     n_large = 0;
     general_large = false;
     large_slot_bytes = 0;
+    // the large-order launch runs in bit-plane mode when every large job's
+    // W fits a warp's shared memory as bit planes
+    planes_large = large_planes_allowed();
+    for (const XwJob& J : jobs)
+        if (J.large && !anneal_large_planes_fit(J.n, J.m)) planes_large = false;
     for (int j = 0; j < njobs; ++j) {
         const XwJob& J = jobs[j];
         total_replicas += (uint32_t)J.replicas;
@@ -416,7 +431,7 @@ void Batch::derive_layout() {
         if (J.large) {
             n_large += (uint32_t)J.replicas;
             general_large = general_large || J.general != 0;
-            large_slot_bytes = std::max(large_slot_bytes, anneal_large_slot_bytes(J.n));
+            large_slot_bytes = std::max(large_slot_bytes, anneal_large_slot_bytes(J.n, J.m, planes_large));
         }
     }
     best_bytes = best_off;
@@ -472,14 +487,15 @@ void Batch::derive_layout() {
         c.general = c.general || J.general != 0;
         c.slot_bytes = std::max(c.slot_bytes, anneal_slot_bytes(J.n, J.m, c.opl));
     }
-    // Gram arena offsets of the HBM-resident replicas
+    // arena offsets of the large-order replicas (Gram matrices, or planes
+    // and residuals in bit-plane mode)
     gram_off.assign(total_replicas, 0);
     gram_bytes = 0;
     for (uint32_t i = 0; i < total_replicas; ++i) {
         const XwJob& J = jobs[job_of[i]];
         if (!J.large) continue;
         gram_off[i] = gram_bytes;
-        gram_bytes += anneal_large_gram_bytes(J.n);
+        gram_bytes += anneal_large_arena_bytes(J.n, planes_large);
     }
 }
 
@@ -700,7 +716,7 @@ void Batch::configure_shape() {
     }
     if (n_large) {
         // four warps per CTA, as many CTAs as the SMs hold
-        const void* lfn = anneal_large_kernel_fn(general_large);
+        const void* lfn = anneal_large_kernel_fn(general_large, planes_large);
         const size_t lsmem = (size_t)large_wpb * large_slot_bytes;
         raise_smem_limit(lfn, params.device);
         int per_sm = 0;
@@ -902,7 +918,8 @@ void Batch::enqueue_rounds(uint64_t iters, bool timed) {
                 la.chunks = la.iters >= large_chunks ? large_chunks : 1;
                 if (la.chunks > 1) la.chunk_done = static_cast<uint32_t*>(d_chunk_done);
                 cudaStream_t st = on(l);
-                check(launch_anneal_large(la, general_large, large_wpb, large_blocks, st), "launch anneal_large_kernel");
+                check(launch_anneal_large(la, general_large, planes_large, large_wpb, large_blocks, st),
+                      "launch anneal_large_kernel");
                 join(l, st);
                 ++l;
                 continue;
@@ -1750,7 +1767,7 @@ int32_t xw_batch_classes(xw_batch* h, xw_launch_class* out, int32_t cap, int32_t
     std::vector<xw_launch_class> all;
     if (b.n_large) {
         xw_launch_class c{};
-        c.large = 1;
+        c.large = b.planes_large ? 2 : 1;
         c.min_order = 0x7fffffff;
         for (const XwJob& J : b.jobs)
             if (J.large) {
@@ -1857,12 +1874,13 @@ int32_t xw_run(int32_t n, int32_t w, const xw_params* pin, const int8_t* start, 
         int replicas = p.replicas;
         const int m = std::min(w, n - w);
         const bool large = n >= large_min_order();
-        const uint32_t slot = large ? anneal_large_slot_bytes(n) : anneal_slot_bytes(n, m, anneal_opl(n));
+        const bool planes = large && large_planes_allowed() && anneal_large_planes_fit(n, m);
+        const uint32_t slot = large ? anneal_large_slot_bytes(n, m, planes) : anneal_slot_bytes(n, m, anneal_opl(n));
         if (replicas == 0) {
             // one resident wave: warp slots per SM times SMs
             const int wpb = large ? 4 : p.warps_per_block > 0 ? p.warps_per_block : 4;
             int per_sm = 0;
-            const void* fn = large ? anneal_large_kernel_fn(needs_general_kernel(p))
+            const void* fn = large ? anneal_large_kernel_fn(needs_general_kernel(p), planes)
                                    : anneal_kernel_fn(anneal_opl(n), needs_general_kernel(p));
             raise_smem_limit(fn, p.device);
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * wpb, (size_t)wpb * slot);

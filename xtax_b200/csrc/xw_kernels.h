@@ -56,13 +56,16 @@ cudaError_t launch_anneal(const AnnealArgs& args, int opl, bool general, int war
 uint32_t anneal_spec_cta_bytes(uint32_t slot_bytes, int K);
 const void* anneal_spec_kernel_fn(bool general);
 cudaError_t launch_anneal_spec(const AnnealArgs& args, bool general, int K, int blocks, cudaStream_t stream);
-// Orders above XW_MAX_N: the kernel whose replica state lives in HBM
-// (xw_anneal_large.cu).  Shared memory per warp, Gram-arena bytes per
-// replica (a multiple of 256), the kernel, and its launch.
-uint32_t anneal_large_slot_bytes(int n);
-uint64_t anneal_large_gram_bytes(int n);
-const void* anneal_large_kernel_fn(bool general);
-cudaError_t launch_anneal_large(const AnnealArgs& args, bool general, int warps_per_block, int blocks,
+// Orders above XW_MAX_N (xw_anneal_large.cu): in bit-plane mode (orders
+// whose W fits a warp's shared memory as bit planes: no Gram matrix stored,
+// its entries recomputed by popcounts) or with the Gram matrix in an HBM
+// arena.  Whether (n, m) fits the bit-plane mode, shared memory per warp,
+// arena bytes per replica (a multiple of 256), the kernel, and its launch.
+bool anneal_large_planes_fit(int n, int m);
+uint32_t anneal_large_slot_bytes(int n, int m, bool planes);
+uint64_t anneal_large_arena_bytes(int n, bool planes);
+const void* anneal_large_kernel_fn(bool general, bool planes);
+cudaError_t launch_anneal_large(const AnnealArgs& args, bool general, bool planes, int warps_per_block, int blocks,
                                 cudaStream_t stream);
 cudaError_t launch_exchange(XwJob* jobs, int njobs, uint8_t* arena, const uint64_t* rec_off,
                             const double* ladder, int stop_on_solve, cudaStream_t stream);

@@ -28,7 +28,8 @@
 
 #define XW_STATUS_INIT 1u      // record holds incremental state (score etc.)
 #define XW_STATUS_SOLVED 2u    // best score reached 0
-#define XW_STATUS_GRAM 4u      // large orders: the Gram arena holds this W's Gram and masks
+#define XW_STATUS_GRAM 4u      // large orders: the arena holds this W's Gram and masks (or, in
+                               // bit-plane mode, its planes and residuals)
 #define XW_ERR_SCORE 1u        // rebuilt score differs from the tracked one
 #define XW_ERR_MINORITY 2u     // W row weights disagree with the minority lists
 #define XW_ERR_KERNEL 4u       // a lean launch met a replica that needs the general kernel
