@@ -539,17 +539,18 @@ def large_bench(X, iters, ref_seconds):
     """W(276,275) with 2368 replicas and the reference's defaults otherwise
     (t_init 6, t_min 0.1, cooling and reheat, no restarts).  276 is about the
     largest order whose state the reference's kernel holds in one CTA's
-    shared memory; here it runs on the large-order kernel, in both its forms
-    (the Gram matrix in HBM, 16 warps per SM; bit planes in shared memory,
-    8 warps per SM).  Beside it the reference's xweigh_cuda on the same order
-    and replica count."""
+    shared memory; here it runs on the large-order kernel in its default
+    form (bit planes in shared memory, the Gram matrix in HBM, 8 warps per
+    SM) and in its two others (the Gram matrix and masks in HBM, 16 warps
+    per SM; bit planes with every Gram entry recomputed).  Beside it the
+    reference's xweigh_cuda on the same order and replica count."""
     p = X.Params(stop_on_solve=0, t_init=6.0, t_min=0.1, moves_per_launch=1000,
                  squared_objective_fraction=0.0, parity_objective_fraction=0.0)
 
-    def form(planes):
+    def form(which):
         # XW_LARGE_PLANES selects the kernel's form when the batch is built
         old = os.environ.get("XW_LARGE_PLANES")
-        os.environ["XW_LARGE_PLANES"] = "1" if planes else "0"
+        os.environ["XW_LARGE_PLANES"] = str(which)
         try:
             b = X.Batch([{"n": LARGE_N, "w": LARGE_W, "seed": 1, "replicas": LARGE_R}], p)
         finally:
@@ -572,12 +573,13 @@ def large_bench(X, iters, ref_seconds):
                 "two_row_evaluations": r.two_row_evaluations - r0.two_row_evaluations,
                 "accepted_moves": r.accepted_moves - r0.accepted_moves,
                 "launch_class": cls,
-                "kernel": "anneal_large_kernel, " + ("bit planes in shared memory, Gram entries recomputed"
-                                                     if cls["large"] == 2 else "Gram matrix in HBM")}
+                "kernel": "anneal_large_kernel, " + {1: "Gram matrix in HBM",
+                                                     2: "bit planes in shared memory, Gram entries recomputed",
+                                                     3: "bit planes in shared memory, Gram matrix in HBM"}[cls["large"]]}
 
     out = {"workload": f"W({LARGE_N},{LARGE_W}) x {LARGE_R} replicas, cooling from T 6 (t_min 0.1), L1 objective, "
                        f"the reference's moves, {iters} iterations per replica",
-           "device": form(False), "device_bit_planes": form(True)}
+           "device": form(2), "device_stored_gram": form(0), "device_bit_planes": form(1)}
     if ref_seconds > 0 and os.path.exists(REF_XWEIGH_CUDA):
         try:
             mv, secs = run_reference_cuda(ref_seconds, n=LARGE_N, w=LARGE_W, replicas=LARGE_R)

@@ -291,8 +291,9 @@ int32_t xw_batch_shape(xw_batch* b, int32_t* warps_per_block, int32_t* blocks, i
  * counterpart in the reference, which launches one search at a time. */
 typedef struct xw_launch_class {
     int32_t min_order, max_order;
-    int32_t large;                 /* orders above 256: 2 bit-plane mode (W as bit planes in shared
-                                      memory, Gram entries recomputed), 1 Gram matrix in HBM; 0 below */
+    int32_t large;                 /* orders above 256: 1 Gram matrix in HBM; 2 W as bit planes in
+                                      shared memory, Gram entries recomputed; 3 bit planes and the
+                                      Gram matrix in HBM; 0 below */
     int32_t rows_per_lane;         /* 1, 2, 4 or 8 (shared-memory kernel) */
     int32_t replicas_per_warp;     /* 1, or 2 (half-warp replicas, orders up to 16) */
     int32_t warps_per_block;

@@ -1,6 +1,8 @@
-"""The kernel for orders above the shared-memory classes, in both its forms:
-the Gram matrix stored in HBM (the default), and bit planes in shared memory
-with the Gram entries recomputed (orders up to 448, XW_LARGE_PLANES=1).
+"""The kernel for orders above the shared-memory classes, in its three
+forms: bit planes in shared memory with the Gram matrix in HBM (the default
+for orders up to 448, XW_LARGE_PLANES=2); the Gram matrix and masks in HBM
+(larger orders, XW_LARGE_PLANES=0); bit planes with every Gram entry
+recomputed (XW_LARGE_PLANES=1).
 
 Its replicas follow the same draw layout and move rules as the shared-memory
 kernel, so the CPU oracle replays them bit for bit: W, best W, minority
@@ -25,10 +27,13 @@ def large_from(monkeypatch):
     return set_order
 
 
-@pytest.fixture(params=["planes", "gram"])
+FORMS = {"gram": "0", "planes": "1", "hybrid": "2"}
+
+
+@pytest.fixture(params=list(FORMS))
 def form(request, monkeypatch):
-    """Both forms of the large-order kernel."""
-    monkeypatch.setenv("XW_LARGE_PLANES", "1" if request.param == "planes" else "0")
+    """Every form of the large-order kernel."""
+    monkeypatch.setenv("XW_LARGE_PLANES", FORMS[request.param])
     return request.param
 
 
@@ -85,13 +90,13 @@ def test_large_orders_match_oracle(form, n, w, R, iters, kw):
 
 @pytest.mark.parametrize("n,w,planes", [(276, 275, True), (448, 447, True), (449, 448, False), (1024, 1000, False)])
 def test_large_class_reports_its_form(monkeypatch, n, w, planes):
-    """Bit planes up to order 448, the stored Gram matrix above it and
-    whenever XW_LARGE_PLANES=0."""
-    for allowed in ("1", "0"):
-        monkeypatch.setenv("XW_LARGE_PLANES", allowed)
+    """The bit-plane forms up to order 448 (the hybrid by default), the
+    stored Gram matrix above it."""
+    for wanted in ("", "0", "1", "2"):
+        monkeypatch.setenv("XW_LARGE_PLANES", wanted)
         b = X.Batch([{"n": n, "w": w, "seed": 1, "replicas": 2}], X.Params(stop_on_solve=0))
         (c,) = b.classes()
-        assert c["large"] == (2 if planes and allowed == "1" else 1)
+        assert c["large"] == (1 + int(wanted or "2") if planes else 1)
         b.close()
 
 

@@ -18,11 +18,14 @@
 // it is built once from W with popcounts over the sign and support masks,
 // and rebuilt whenever the host replaces W (restarts, snapshots).
 //
-// A second form, the bit-plane form (orders up to 448, selected by the
-// host), stores no G: W sits in the warp's slot as support and sign bit
-// planes and each Gram entry an evaluation or commit needs is recomputed by
-// popcounts, so a move makes no HBM traffic; its arena keeps residuals,
-// planes and the best state's planes between launches.
+// For orders up to 448 W can instead sit in the warp's slot as support and
+// sign bit planes, which the proposals read without touching global
+// memory.  Two forms do that: the hybrid (the default there) keeps G in
+// HBM and stages each candidate's Gram rows in shared memory with all their
+// loads in flight at once; the bit-plane form stores no G and recomputes
+// each Gram entry it needs by popcounts, so a move makes no HBM traffic.
+// Their arena keeps residuals, planes and the best state's planes between
+// launches.
 //
 // The iteration is the one of xw_anneal.cu with the same draw layout, the
 // same proposal order and the same tie rules, so a replica's trajectory is
@@ -60,27 +63,38 @@ struct LView {
     uint32_t stream, k0, k1;
 };
 
+// The large-order kernel's forms: the Gram matrix and masks in HBM; bit
+// planes in shared memory with every Gram entry recomputed; and the hybrid
+// of the two, bit planes in shared memory (proposals and W's entries) with
+// the Gram matrix in HBM (evaluation and commit), each candidate's Gram
+// rows staged in shared memory with all their loads in flight at once.
+enum LargeForm : int { kFormGram = 0, kFormPlanes = 1, kFormHybrid = 2 };
+
+// Row stride of the hybrid form's Gram matrix: rows start on 16 bytes.
+__host__ __device__ inline int gram_ld(int n) { return (n + 7) & ~7; }
+
 // Shared memory per warp.  Every replica: residuals (int32 x n), the
 // iteration's draw blocks, the view, the Metropolis thresholds.  A replica
 // in bit-plane mode adds W as support and sign planes, planes[q * n + o] =
 // {support word q of row o, sign word q of row o} (16 bytes; consecutive
 // rows consecutive, so a warp reading word q of its 32 rows reads 512
 // contiguous bytes), and its minority lists when they take at most
-// kMinoSmemBytes (off_mino 0: they stay in the record).
+// kMinoSmemBytes (off_mino 0: they stay in the record); the hybrid form
+// adds a staging buffer of two Gram rows.
 struct LSlot {
-    uint32_t off_draws, off_view, off_thr, off_planes, off_mino, bytes;
+    uint32_t off_draws, off_view, off_thr, off_planes, off_mino, off_stage, bytes;
 };
 
 constexpr uint32_t kMinoSmemBytes = 8192;
 
-__host__ __device__ inline LSlot large_slot(int n, int m, bool planes) {
+__host__ __device__ inline LSlot large_slot(int n, int m, int form) {
     LSlot L;
     L.off_draws = xw_pad16((uint32_t)n * 4u);
     L.off_view = L.off_draws + 32u * 16u;
     L.off_thr = L.off_view + xw_pad16((uint32_t)sizeof(LView));
     L.bytes = L.off_thr + kThrTable * 8u;
-    L.off_planes = L.off_mino = 0;
-    if (planes) {
+    L.off_planes = L.off_mino = L.off_stage = 0;
+    if (form != kFormGram) {
         const uint32_t nw = (uint32_t)(n + 63) / 64u;
         L.off_planes = xw_pad16(L.bytes);
         L.bytes = L.off_planes + nw * (uint32_t)n * 16u;
@@ -89,6 +103,10 @@ __host__ __device__ inline LSlot large_slot(int n, int m, bool planes) {
             L.off_mino = L.bytes;
             L.bytes += xw_pad16(mb);
         }
+    }
+    if (form == kFormHybrid) {
+        L.off_stage = L.bytes;
+        L.bytes += 2u * (uint32_t)gram_ld(n) * 2u;
     }
     return L;
 }
@@ -100,7 +118,7 @@ constexpr uint32_t kPlanesSlotMax = 56u * 1024u;
 constexpr int kPlanesNw = 7;
 
 __host__ __device__ inline bool large_planes_fit(int n, int m) {
-    return n <= 64 * kPlanesNw && large_slot(n, m, true).bytes <= kPlanesSlotMax;
+    return n <= 64 * kPlanesNw && large_slot(n, m, kFormHybrid).bytes <= kPlanesSlotMax;
 }
 
 // Arena per replica.  Stored-Gram form: G (int16, row-major), support and
@@ -114,15 +132,18 @@ struct LGram {
 };
 
 struct LPArena {
-    uint64_t off_planes, off_best, bytes;
+    uint64_t off_planes, off_best, off_g, bytes;
 };
 
-__host__ __device__ inline LPArena planes_arena(int n) {
+// residuals, planes and the best state's planes (and, in the hybrid form,
+// G: int16 row-major, rows gram_ld(n) entries apart)
+__host__ __device__ inline LPArena planes_arena(int n, bool stored_gram) {
     const uint64_t nw = (uint64_t)(n + 63) / 64;
     LPArena A;
     A.off_planes = ((uint64_t)n * 4u + 15u) & ~uint64_t(15);
     A.off_best = A.off_planes + nw * (uint64_t)n * 16u;
-    A.bytes = A.off_best + nw * (uint64_t)n * 16u;
+    A.off_g = A.off_best + nw * (uint64_t)n * 16u;
+    A.bytes = A.off_g + (stored_gram ? (uint64_t)n * gram_ld(n) * 2u : 0u);
     return A;
 }
 
@@ -592,15 +613,47 @@ struct PRows {
     int s1;      // commit: the lane's sum of R1's residual changes
 };
 
-template <bool GEN, bool TWO>
-__device__ __forceinline__ PRows p_rows(const LUpdate& u, const ulonglong2* P, int32_t* res, int n, int nw, int lane,
-                                     bool commit) {
+// Hybrid form: copy the stored Gram rows r1 (and r2) into the warp's
+// staging buffer S (rows gram_ld(n) entries apart, 16-byte chunks, at most
+// two per lane and row), every load issued before the first store, so that
+// staging costs one round trip to L2/HBM
+__device__ __forceinline__ void p_stage(const int16_t* G, int n, int r1, int r2, bool two, int16_t* S, int lane) {
+    const int ldg = gram_ld(n), chunks = ldg / 8;
+    const uint4* a = reinterpret_cast<const uint4*>(G + (size_t)r1 * ldg);
+    const uint4* b = reinterpret_cast<const uint4*>(G + (size_t)r2 * ldg);
+    const int k0 = lane, k1 = lane + 32;
+    uint4 x0 = make_uint4(0, 0, 0, 0), x1 = x0, y0 = x0, y1 = x0;
+    if (k0 < chunks) x0 = a[k0];
+    if (k1 < chunks) x1 = a[k1];
+    if (two) {
+        if (k0 < chunks) y0 = b[k0];
+        if (k1 < chunks) y1 = b[k1];
+    }
+    uint4* sa = reinterpret_cast<uint4*>(S);
+    uint4* sb = reinterpret_cast<uint4*>(S + ldg);
+    if (k0 < chunks) sa[k0] = x0;
+    if (k1 < chunks) sa[k1] = x1;
+    if (two) {
+        if (k0 < chunks) sb[k0] = y0;
+        if (k1 < chunks) sb[k1] = y1;
+    }
+    __syncwarp();
+}
+
+template <bool GEN, bool TWO, bool SG>
+__device__ __forceinline__ PRows p_rows(const LUpdate& u, const ulonglong2* P, int16_t* G, const int16_t* S,
+                                        int32_t* res, int n, int nw, int lane, bool commit) {
     PRows out = {{0, 0, 0, 0}, 0};
+    const int ldg = gram_ld(n);
     const ulonglong2* pa = P + u.R1;
     const ulonglong2* pb = P + (TWO ? u.R2 : u.R1);
 #pragma unroll 1
     for (int o = lane; o < n; o += 32) {
         int g1 = 0, g2 = 0;
+        if constexpr (SG) {
+            g1 = S[o];
+            if constexpr (TWO) g2 = S[ldg + o];
+        } else {
 #pragma unroll 1
         for (int q = 0; q < nw; ++q) {
             const size_t off = (size_t)q * n;
@@ -612,6 +665,7 @@ __device__ __forceinline__ PRows p_rows(const LUpdate& u, const ulonglong2* P, i
                 const uint64_t b2 = b.x & e.x;
                 g2 += __popcll(b2) - 2 * __popcll(b2 & (b.y ^ e.y));
             }
+        }
         }
         if (o == u.R1 || (TWO && o == u.R2)) continue;
         int n1 = g1 + u.A1 * p_at(P, n, o, u.X1);
@@ -625,6 +679,14 @@ __device__ __forceinline__ PRows p_rows(const LUpdate& u, const ulonglong2* P, i
             const int e1 = iabs(n1) - iabs(g1);
             res[o] += TWO ? e1 + iabs(n2) - iabs(g2) : e1;
             out.s1 += e1;
+            if constexpr (SG) {
+                G[(size_t)u.R1 * ldg + o] = (int16_t)n1;
+                G[(size_t)o * ldg + u.R1] = (int16_t)n1;
+                if constexpr (TWO) {
+                    G[(size_t)u.R2 * ldg + o] = (int16_t)n2;
+                    G[(size_t)o * ldg + u.R2] = (int16_t)n2;
+                }
+            }
         } else {
             lacc<GEN>(out.d, g1, n1);
             if constexpr (TWO) lacc<GEN>(out.d, g2, n2);
@@ -633,19 +695,20 @@ __device__ __forceinline__ PRows p_rows(const LUpdate& u, const ulonglong2* P, i
     return out;
 }
 
-template <bool GEN>
-__device__ __forceinline__ PRows p_rows_any(const LUpdate& u, const ulonglong2* P, int32_t* res, int n, int nw,
-                                            int lane, bool commit) {
-    return u.R2 >= 0 ? p_rows<GEN, true>(u, P, res, n, nw, lane, commit)
-                     : p_rows<GEN, false>(u, P, res, n, nw, lane, commit);
+template <bool GEN, bool SG>
+__device__ __forceinline__ PRows p_rows_any(const LUpdate& u, const ulonglong2* P, int16_t* G, const int16_t* S,
+                                            int32_t* res, int n, int nw, int lane, bool commit) {
+    return u.R2 >= 0 ? p_rows<GEN, true, SG>(u, P, G, S, res, n, nw, lane, commit)
+                     : p_rows<GEN, false, SG>(u, P, G, S, res, n, nw, lane, commit);
 }
 
-// l_eval on the planes
-template <bool GEN>
-__device__ __forceinline__ LDeltas p_eval(const LUpdate& u, const ulonglong2* P, int n, int nw, int lane) {
-    LDeltas d = p_rows_any<GEN>(u, P, nullptr, n, nw, lane, false).d;
+// l_eval on the planes (and, SG, the move's stored Gram rows staged in S)
+template <bool GEN, bool SG>
+__device__ __forceinline__ LDeltas p_eval(const LUpdate& u, const ulonglong2* P, int16_t* G, const int16_t* S, int n,
+                                          int nw, int lane) {
+    LDeltas d = p_rows_any<GEN, SG>(u, P, G, S, nullptr, n, nw, lane, false).d;
     if (u.pair && lane == 0) {
-        const int op = p_dot(P, n, nw, u.R1, u.R2);
+        const int op = SG ? (int)S[u.R2] : p_dot(P, n, nw, u.R1, u.R2);
         lacc<GEN>(d, op, p_pair_new(u, op, P, n));
     }
     return d;
@@ -653,10 +716,10 @@ __device__ __forceinline__ LDeltas p_eval(const LUpdate& u, const ulonglong2* P,
 
 // l_commit on the planes: residuals from the recomputed rows, then the
 // changed entries (lane 0, after every lane has read the old planes)
-template <bool GEN>
-__device__ void p_commit(const LMove& mv, const LUpdate& u, int ds, ulonglong2* P, int32_t* res, uint16_t* mino,
-                         int n, int m, int nw, int sparse, int lane) {
-    const int s1 = p_rows_any<GEN>(u, P, res, n, nw, lane, true).s1;
+template <bool GEN, bool SG>
+__device__ void p_commit(const LMove& mv, const LUpdate& u, int ds, ulonglong2* P, int16_t* G, const int16_t* S,
+                         int32_t* res, uint16_t* mino, int n, int m, int nw, int sparse, int lane) {
+    const int s1 = p_rows_any<GEN, SG>(u, P, G, S, res, n, nw, lane, true).s1;
     const int S1 = __reduce_add_sync(FULL, s1);
     __syncwarp();
     if (lane == 0) {
@@ -666,8 +729,14 @@ __device__ void p_commit(const LMove& mv, const LUpdate& u, int ds, ulonglong2* 
         const int p1 = mv.z & 1023, p2 = (mv.z >> 10) & 1023;
         const int o11 = (int)((mv.x >> 23) & 3) - 1, o22 = (int)((mv.x >> 25) & 3) - 1;
         if (u.pair) {
-            const int op = p_dot(P, n, nw, r1, r2);
-            const int pd = iabs(p_pair_new(u, op, P, n)) - iabs(op);
+            const int op = SG ? (int)S[r2] : p_dot(P, n, nw, r1, r2);
+            const int np = p_pair_new(u, op, P, n);
+            const int pd = iabs(np) - iabs(op);
+            if constexpr (SG) {
+                const int ldg = gram_ld(n);
+                G[(size_t)r1 * ldg + r2] = (int16_t)np;
+                G[(size_t)r2 * ldg + r1] = (int16_t)np;
+            }
             res[r1] += S1 + pd;
             res[r2] += ds - S1;
         } else if (u.R2 >= 0) {
@@ -698,9 +767,10 @@ __device__ void p_commit(const LMove& mv, const LUpdate& u, int ds, ulonglong2* 
 }
 
 // Residuals and the totals of the lane's rows from the planes (a replica
-// whose planes were just built): every G[r][o], r != o
-__device__ __noinline__ void p_totals(const ulonglong2* P, int32_t* res, int n, int nw, int lane, int& score,
-                                      int& conf, long long& sq, int& par) {
+// whose planes were just built): every G[r][o], r != o; G, when given,
+// receives the Gram matrix
+__device__ __noinline__ void p_totals(const ulonglong2* P, int16_t* G, int32_t* res, int n, int nw, int lane,
+                                      int& score, int& conf, long long& sq, int& par) {
 #pragma unroll 1
     for (int o = lane; o < n; o += 32) {
         int r_sum = 0;
@@ -713,6 +783,7 @@ __device__ __noinline__ void p_totals(const ulonglong2* P, int32_t* res, int n, 
                 const uint64_t both = x.x & e.x;
                 g += __popcll(both) - 2 * __popcll(both & (x.y ^ e.y));
             }
+            if (G) G[(size_t)r * gram_ld(n) + o] = (int16_t)g;
             if (r != o) {
                 const int ag = iabs(g);
                 r_sum += ag;
@@ -815,8 +886,10 @@ __device__ bool build_gram(const int8_t* W, int16_t* G, uint64_t* mask, uint64_t
     return ok;
 }
 
-template <bool GEN, bool PM>
+template <bool GEN, int FORM>
 __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int lane, uint64_t chunk_iters) {
+    constexpr bool PM = FORM != kFormGram;     // W as bit planes in the slot
+    constexpr bool SG = FORM != kFormPlanes;   // the Gram matrix stored in HBM
     uint8_t* rec = a.arena + a.rec_off[rid];
     RepHeader* H = reinterpret_cast<RepHeader*>(rec);
     const uint32_t jid = H->job;
@@ -826,7 +899,7 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
 
     const int n = J->n, w = J->w, m = J->m, sparse = J->sparse;
     const int nw = (n + 63) / 64;
-    const LSlot L = large_slot(n, m, PM);
+    const LSlot L = large_slot(n, m, FORM);
     int8_t* W = reinterpret_cast<int8_t*>(rec + J->off_w);
     uint16_t* const mino_rec = reinterpret_cast<uint16_t*>(rec + J->off_mino);
     // bit-plane mode: W as planes in the slot; the arena keeps residuals,
@@ -834,9 +907,10 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
     ulonglong2* const P = PM ? reinterpret_cast<ulonglong2*>(slot + L.off_planes) : nullptr;
     uint16_t* const mino = PM && L.off_mino ? reinterpret_cast<uint16_t*>(slot + L.off_mino) : mino_rec;
     uint8_t* const parena = PM ? a.gram + a.gram_off[rid] : nullptr;
-    const LPArena PA = planes_arena(n);
+    const LPArena PA = planes_arena(n, SG);
     const uint32_t plane_bytes = (uint32_t)nw * (uint32_t)n * 16u;
-    int16_t* G = nullptr;
+    int16_t* G = PM && SG ? reinterpret_cast<int16_t*>(parena + PA.off_g) : nullptr;
+    int16_t* const S = PM && SG ? reinterpret_cast<int16_t*>(slot + L.off_stage) : nullptr;
     uint64_t *mask = nullptr, *sign = nullptr;
     if constexpr (!PM) {
         const LGram LG = large_gram(n);
@@ -935,7 +1009,7 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
 #pragma unroll 1
         for (int o = lane; o < n; o += 32) p_score += sRes[o];
     } else if constexpr (PM) {
-        p_totals(P, sRes, n, nw, lane, p_score, p_conf, p_sq, p_par);
+        p_totals(P, G, sRes, n, nw, lane, p_score, p_conf, p_sq, p_par);
     } else {
 #pragma unroll 1
         for (int o = lane; o < n; o += 32) {
@@ -1080,10 +1154,10 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
         LMove desc = none();
         if (lane < count) desc = l_propose<GEN>(sView, it, lane, coop && lane < 4, coop_row);
         __syncwarp();
-
         bool have = false;
         LMove best_mv = none();
         int bds = 0, bdc = 0, bprim = 0;
+        int best_cand = -1, staged = -1;   // hybrid form: the candidates whose rows are in S
 #pragma unroll 1
         for (int c = 0; c < count; ++c) {
             LMove e;
@@ -1093,7 +1167,11 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
             e.z = __shfl_sync(FULL, desc.z, c);
             const LUpdate u = l_decode(e);
             LDeltas d;
-            if constexpr (PM) d = p_eval<GEN>(u, P, n, nw, lane);
+            if constexpr (PM && SG) {
+                p_stage(G, n, u.R1, u.R2, u.R2 >= 0, S, lane);
+                staged = c;
+            }
+            if constexpr (PM) d = p_eval<GEN, SG>(u, P, G, S, n, nw, lane);
             else d = l_eval<GEN>(u, W, G, n, lane);
             const int ds = __reduce_add_sync(FULL, d.ds);
             const int dc = __reduce_add_sync(FULL, d.dc);
@@ -1111,7 +1189,7 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
                 else better = dc < bdc;
             }
             if (better) {
-                have = true; best_mv = e; bds = ds; bdc = dc; bprim = prim;
+                have = true; best_mv = e; bds = ds; bdc = dc; bprim = prim; best_cand = c;
             }
         }
         if (!have) {
@@ -1138,7 +1216,11 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
                 at_best = false;
             }
             const LUpdate u = l_decode(best_mv);
-            if constexpr (PM) p_commit<GEN>(best_mv, u, bds, P, sRes, mino, n, m, nw, sparse, lane);
+            if constexpr (PM && SG) {
+                // the staging buffer holds the last evaluated candidate's rows
+                if (staged != best_cand) p_stage(G, n, u.R1, u.R2, u.R2 >= 0, S, lane);
+            }
+            if constexpr (PM) p_commit<GEN, SG>(best_mv, u, bds, P, G, S, sRes, mino, n, m, nw, sparse, lane);
             else l_commit<GEN>(best_mv, u, bds, W, G, sRes, mino, mask, n, m, nw, sparse, lane);
             score += bds;
             conflicts += bdc;
@@ -1227,8 +1309,8 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
 #ifndef XW_LARGE_MIN_BLOCKS
 #define XW_LARGE_MIN_BLOCKS 4
 #endif
-template <bool GEN, bool PM>
-__global__ void __launch_bounds__(128, PM ? 2 : XW_LARGE_MIN_BLOCKS) anneal_large_kernel(AnnealArgs a) {
+template <bool GEN, int FORM>
+__global__ void __launch_bounds__(128, FORM != kFormGram ? 2 : XW_LARGE_MIN_BLOCKS) anneal_large_kernel(AnnealArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -1242,7 +1324,7 @@ __global__ void __launch_bounds__(128, PM ? 2 : XW_LARGE_MIN_BLOCKS) anneal_larg
         item = __shfl_sync(FULL, item, 0);
         if (item >= total) break;
         if (a.chunks == 1) {
-            run_large<GEN, PM>(a, a.items[item], slot, lane, a.iters);
+            run_large<GEN, FORM>(a, a.items[item], slot, lane, a.iters);
             continue;
         }
         const uint32_t c = item / a.n_items;
@@ -1250,7 +1332,7 @@ __global__ void __launch_bounds__(128, PM ? 2 : XW_LARGE_MIN_BLOCKS) anneal_larg
         const uint64_t lo = a.iters * c / a.chunks, hi = a.iters * (c + 1) / a.chunks;
         RepHeader* H = reinterpret_cast<RepHeader*>(a.arena + a.rec_off[rid]);
         const bool ok = chunk_begin(a.chunk_done + rid, c, a.chunk_wait_ns, &H->err, lane, FULL);
-        if (ok) run_large<GEN, PM>(a, rid, slot, lane, hi - lo);
+        if (ok) run_large<GEN, FORM>(a, rid, slot, lane, hi - lo);
         chunk_end(a.chunk_done + rid, c, ok, lane, FULL);
     }
 }
@@ -1259,26 +1341,30 @@ __global__ void __launch_bounds__(128, PM ? 2 : XW_LARGE_MIN_BLOCKS) anneal_larg
 
 bool anneal_large_planes_fit(int n, int m) { return large_planes_fit(n, m); }
 
-uint32_t anneal_large_slot_bytes(int n, int m, bool planes) { return large_slot(n, m, planes).bytes; }
+uint32_t anneal_large_slot_bytes(int n, int m, int form) { return large_slot(n, m, form).bytes; }
 
-uint64_t anneal_large_arena_bytes(int n, bool planes) {
-    return ((planes ? planes_arena(n).bytes : large_gram(n).bytes) + 255u) & ~uint64_t(255);
+uint64_t anneal_large_arena_bytes(int n, int form) {
+    const uint64_t b = form == kFormGram ? large_gram(n).bytes : planes_arena(n, form == kFormHybrid).bytes;
+    return (b + 255u) & ~uint64_t(255);
 }
 
-const void* anneal_large_kernel_fn(bool general, bool planes) {
-    if (planes)
-        return general ? reinterpret_cast<const void*>(&anneal_large_kernel<true, true>)
-                       : reinterpret_cast<const void*>(&anneal_large_kernel<false, true>);
-    return general ? reinterpret_cast<const void*>(&anneal_large_kernel<true, false>)
-                   : reinterpret_cast<const void*>(&anneal_large_kernel<false, false>);
+const void* anneal_large_kernel_fn(bool general, int form) {
+    if (form == kFormPlanes)
+        return general ? reinterpret_cast<const void*>(&anneal_large_kernel<true, kFormPlanes>)
+                       : reinterpret_cast<const void*>(&anneal_large_kernel<false, kFormPlanes>);
+    if (form == kFormHybrid)
+        return general ? reinterpret_cast<const void*>(&anneal_large_kernel<true, kFormHybrid>)
+                       : reinterpret_cast<const void*>(&anneal_large_kernel<false, kFormHybrid>);
+    return general ? reinterpret_cast<const void*>(&anneal_large_kernel<true, kFormGram>)
+                   : reinterpret_cast<const void*>(&anneal_large_kernel<false, kFormGram>);
 }
 
-cudaError_t launch_anneal_large(const AnnealArgs& args, bool general, bool planes, int warps_per_block, int blocks,
+cudaError_t launch_anneal_large(const AnnealArgs& args, bool general, int form, int warps_per_block, int blocks,
                                 cudaStream_t stream) {
     const size_t smem = (size_t)warps_per_block * args.slot_bytes;
     const dim3 grid(blocks), block(32 * warps_per_block);
     void* kargs[] = {const_cast<AnnealArgs*>(&args)};
-    return cudaLaunchKernel(anneal_large_kernel_fn(general, planes), grid, block, kargs, smem, stream);
+    return cudaLaunchKernel(anneal_large_kernel_fn(general, form), grid, block, kargs, smem, stream);
 }
 
 }  // namespace xw

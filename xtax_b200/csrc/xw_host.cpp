@@ -141,14 +141,18 @@ int large_min_order() {
     return std::clamp(std::atoi(e), 1, XW_MAX_N + 1);
 }
 
-// XW_LARGE_PLANES=1 runs large-order launches in bit-plane form where the
-// orders fit it (no Gram arena: a quarter of the device memory per replica
-// at n = 276 and no HBM traffic per move); the stored-Gram form is the
-// default, being faster where both were measured (W(276,275) on B200: 69
-// against 60 M moves/s)
-static bool large_planes_allowed() {
+// The large-order kernel's form for orders whose bit planes fit a warp's
+// slot (n <= 448): by default 2, bit planes in shared memory with the Gram
+// matrix in HBM (W(276,275) on B200: 104 M moves/s against 69 M for form 0
+// and 60 M for form 1); XW_LARGE_PLANES=0 the Gram matrix and masks in HBM
+// (the form of larger orders), 1 bit planes with every Gram entry
+// recomputed (no Gram matrix: a quarter of the device memory per replica
+// at n = 276, and no HBM traffic per move).
+static int large_form_wanted() {
     const char* e = std::getenv("XW_LARGE_PLANES");
-    return e && std::atoi(e) != 0;
+    if (!e || !*e) return 2;
+    const int v = std::atoi(e);
+    return v == 1 || v == 2 ? v : 0;
 }
 
 std::string validate(int n, int w, const xw_params& p) {
@@ -420,9 +424,9 @@ void Batch::derive_layout() {
     large_slot_bytes = 0;
     // the large-order launch runs in bit-plane mode when every large job's
     // W fits a warp's shared memory as bit planes
-    planes_large = large_planes_allowed();
+    large_form = large_form_wanted();
     for (const XwJob& J : jobs)
-        if (J.large && !anneal_large_planes_fit(J.n, J.m)) planes_large = false;
+        if (J.large && !anneal_large_planes_fit(J.n, J.m)) large_form = 0;
     for (int j = 0; j < njobs; ++j) {
         const XwJob& J = jobs[j];
         total_replicas += (uint32_t)J.replicas;
@@ -431,7 +435,7 @@ void Batch::derive_layout() {
         if (J.large) {
             n_large += (uint32_t)J.replicas;
             general_large = general_large || J.general != 0;
-            large_slot_bytes = std::max(large_slot_bytes, anneal_large_slot_bytes(J.n, J.m, planes_large));
+            large_slot_bytes = std::max(large_slot_bytes, anneal_large_slot_bytes(J.n, J.m, large_form));
         }
     }
     best_bytes = best_off;
@@ -495,7 +499,7 @@ void Batch::derive_layout() {
         const XwJob& J = jobs[job_of[i]];
         if (!J.large) continue;
         gram_off[i] = gram_bytes;
-        gram_bytes += anneal_large_arena_bytes(J.n, planes_large);
+        gram_bytes += anneal_large_arena_bytes(J.n, large_form);
     }
 }
 
@@ -716,7 +720,7 @@ void Batch::configure_shape() {
     }
     if (n_large) {
         // four warps per CTA, as many CTAs as the SMs hold
-        const void* lfn = anneal_large_kernel_fn(general_large, planes_large);
+        const void* lfn = anneal_large_kernel_fn(general_large, large_form);
         const size_t lsmem = (size_t)large_wpb * large_slot_bytes;
         raise_smem_limit(lfn, params.device);
         int per_sm = 0;
@@ -918,7 +922,7 @@ void Batch::enqueue_rounds(uint64_t iters, bool timed) {
                 la.chunks = la.iters >= large_chunks ? large_chunks : 1;
                 if (la.chunks > 1) la.chunk_done = static_cast<uint32_t*>(d_chunk_done);
                 cudaStream_t st = on(l);
-                check(launch_anneal_large(la, general_large, planes_large, large_wpb, large_blocks, st),
+                check(launch_anneal_large(la, general_large, large_form, large_wpb, large_blocks, st),
                       "launch anneal_large_kernel");
                 join(l, st);
                 ++l;
@@ -1767,7 +1771,7 @@ int32_t xw_batch_classes(xw_batch* h, xw_launch_class* out, int32_t cap, int32_t
     std::vector<xw_launch_class> all;
     if (b.n_large) {
         xw_launch_class c{};
-        c.large = b.planes_large ? 2 : 1;
+        c.large = 1 + b.large_form;
         c.min_order = 0x7fffffff;
         for (const XwJob& J : b.jobs)
             if (J.large) {
@@ -1874,13 +1878,13 @@ int32_t xw_run(int32_t n, int32_t w, const xw_params* pin, const int8_t* start, 
         int replicas = p.replicas;
         const int m = std::min(w, n - w);
         const bool large = n >= large_min_order();
-        const bool planes = large && large_planes_allowed() && anneal_large_planes_fit(n, m);
-        const uint32_t slot = large ? anneal_large_slot_bytes(n, m, planes) : anneal_slot_bytes(n, m, anneal_opl(n));
+        const int form = large && anneal_large_planes_fit(n, m) ? large_form_wanted() : 0;
+        const uint32_t slot = large ? anneal_large_slot_bytes(n, m, form) : anneal_slot_bytes(n, m, anneal_opl(n));
         if (replicas == 0) {
             // one resident wave: warp slots per SM times SMs
             const int wpb = large ? 4 : p.warps_per_block > 0 ? p.warps_per_block : 4;
             int per_sm = 0;
-            const void* fn = large ? anneal_large_kernel_fn(needs_general_kernel(p), planes)
+            const void* fn = large ? anneal_large_kernel_fn(needs_general_kernel(p), form)
                                    : anneal_kernel_fn(anneal_opl(n), needs_general_kernel(p));
             raise_smem_limit(fn, p.device);
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * wpb, (size_t)wpb * slot);

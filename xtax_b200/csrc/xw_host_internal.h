@@ -166,7 +166,7 @@ struct Batch {
     // are their replicas; the rest run on the shared-memory kernel
     uint32_t n_large = 0;
     bool general_large = false;
-    bool planes_large = false;   // the large-order class runs in bit-plane mode (no Gram arena)
+    int large_form = 0;          // the large-order class's kernel form (anneal_large_kernel_fn)
     uint32_t large_slot_bytes = 0;
     int large_wpb = 4;
     int large_blocks = 1;

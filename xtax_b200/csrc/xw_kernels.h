@@ -56,16 +56,18 @@ cudaError_t launch_anneal(const AnnealArgs& args, int opl, bool general, int war
 uint32_t anneal_spec_cta_bytes(uint32_t slot_bytes, int K);
 const void* anneal_spec_kernel_fn(bool general);
 cudaError_t launch_anneal_spec(const AnnealArgs& args, bool general, int K, int blocks, cudaStream_t stream);
-// Orders above XW_MAX_N (xw_anneal_large.cu): in bit-plane mode (orders
-// whose W fits a warp's shared memory as bit planes: no Gram matrix stored,
-// its entries recomputed by popcounts) or with the Gram matrix in an HBM
-// arena.  Whether (n, m) fits the bit-plane mode, shared memory per warp,
-// arena bytes per replica (a multiple of 256), the kernel, and its launch.
+// Orders above XW_MAX_N (xw_anneal_large.cu), in one of three forms:
+// 0 the Gram matrix and masks in an HBM arena; 1 bit planes in shared
+// memory, no Gram matrix stored (its entries recomputed by popcounts);
+// 2 bit planes in shared memory and the Gram matrix in HBM.  Forms 1 and 2
+// take orders whose W fits a warp's slot as bit planes.  Whether (n, m)
+// fits them, shared memory per warp, arena bytes per replica (a multiple of
+// 256), the kernel, and its launch.
 bool anneal_large_planes_fit(int n, int m);
-uint32_t anneal_large_slot_bytes(int n, int m, bool planes);
-uint64_t anneal_large_arena_bytes(int n, bool planes);
-const void* anneal_large_kernel_fn(bool general, bool planes);
-cudaError_t launch_anneal_large(const AnnealArgs& args, bool general, bool planes, int warps_per_block, int blocks,
+uint32_t anneal_large_slot_bytes(int n, int m, int form);
+uint64_t anneal_large_arena_bytes(int n, int form);
+const void* anneal_large_kernel_fn(bool general, int form);
+cudaError_t launch_anneal_large(const AnnealArgs& args, bool general, int form, int warps_per_block, int blocks,
                                 cudaStream_t stream);
 cudaError_t launch_exchange(XwJob* jobs, int njobs, uint8_t* arena, const uint64_t* rec_off,
                             const double* ladder, int stop_on_solve, cudaStream_t stream);
