@@ -80,7 +80,7 @@ __host__ __device__ inline int gram_ld(int n) { return (n + 7) & ~7; }
 // rows consecutive, so a warp reading word q of its 32 rows reads 512
 // contiguous bytes), and its minority lists when they take at most
 // kMinoSmemBytes (off_mino 0: they stay in the record); the hybrid form
-// adds a staging buffer of two Gram rows.
+// adds two staging buffers of two Gram rows each.
 struct LSlot {
     uint32_t off_draws, off_view, off_thr, off_planes, off_mino, off_stage, bytes;
 };
@@ -106,7 +106,7 @@ __host__ __device__ inline LSlot large_slot(int n, int m, int form) {
     }
     if (form == kFormHybrid) {
         L.off_stage = L.bytes;
-        L.bytes += 2u * (uint32_t)gram_ld(n) * 2u;
+        L.bytes += 4u * (uint32_t)gram_ld(n) * 2u;
     }
     return L;
 }
@@ -114,7 +114,7 @@ __host__ __device__ inline LSlot large_slot(int n, int m, int form) {
 // Bit-plane mode: orders whose warp slot fits kPlanesSlotMax (four warps
 // per CTA within the 227 KiB a CTA may hold), which bounds the plane words
 // per row by kPlanesNw (n <= 448).
-constexpr uint32_t kPlanesSlotMax = 56u * 1024u;
+constexpr uint32_t kPlanesSlotMax = 227u * 1024u / 4u;
 constexpr int kPlanesNw = 7;
 
 __host__ __device__ inline bool large_planes_fit(int n, int m) {
@@ -640,6 +640,38 @@ __device__ __forceinline__ void p_stage(const int16_t* G, int n, int r1, int r2,
     __syncwarp();
 }
 
+// The same copy issued as cp.async (global -> shared, bypassing L1, no
+// registers held) and committed as one group: the caller overlaps it with
+// the evaluation of the previous candidate and waits with cp.async.wait_group.
+__device__ __forceinline__ void p_stage_async(const int16_t* G, int n, int r1, int r2, bool two, int16_t* S,
+                                              int lane) {
+    const int ldg = gram_ld(n), chunks = ldg / 8;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int k = lane + 32 * h;
+        if (k < chunks) {
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                             (uint32_t)__cvta_generic_to_shared(S + 8 * k)),
+                         "l"(G + (size_t)r1 * ldg + 8 * k)
+                         : "memory");
+            if (two)
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                                 (uint32_t)__cvta_generic_to_shared(S + ldg + 8 * k)),
+                             "l"(G + (size_t)r2 * ldg + 8 * k)
+                             : "memory");
+        }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// the updated rows of candidate c's move (from its descriptor word x)
+__device__ __forceinline__ void move_rows(uint32_t x, int& r1, int& r2, bool& two) {
+    const int kind = (x >> 1) & 3;
+    r1 = (x >> 3) & 1023;
+    r2 = (x >> 13) & 1023;
+    two = kind == 1 || (kind == 2 && r1 != r2);
+}
+
 template <bool GEN, bool TWO, bool SG>
 __device__ __forceinline__ PRows p_rows(const LUpdate& u, const ulonglong2* P, int16_t* G, const int16_t* S,
                                         int32_t* res, int n, int nw, int lane, bool commit) {
@@ -1157,7 +1189,23 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
         bool have = false;
         LMove best_mv = none();
         int bds = 0, bdc = 0, bprim = 0;
-        int best_cand = -1, staged = -1;   // hybrid form: the candidates whose rows are in S
+        // hybrid form: candidate c's Gram rows are staged into one of two
+        // buffers while the candidate before it is evaluated; held[b] is
+        // the candidate whose rows buffer b holds
+        int best_cand = -1, held0 = -1, held1 = -1, cur = 0;
+        uint32_t vmask = 0;
+        const int ldg = gram_ld(n);
+        if constexpr (PM && SG) {
+            vmask = __ballot_sync(FULL, lane < count && (desc.x & 1u));
+            if (vmask) {
+                const int c0 = __ffs(vmask) - 1;
+                int r1, r2;
+                bool two;
+                move_rows(__shfl_sync(FULL, desc.x, c0), r1, r2, two);
+                p_stage_async(G, n, r1, r2, two, S, lane);
+                held0 = c0;
+            }
+        }
 #pragma unroll 1
         for (int c = 0; c < count; ++c) {
             LMove e;
@@ -1167,11 +1215,27 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
             e.z = __shfl_sync(FULL, desc.z, c);
             const LUpdate u = l_decode(e);
             LDeltas d;
+            int16_t* Sc = S;
             if constexpr (PM && SG) {
-                p_stage(G, n, u.R1, u.R2, u.R2 >= 0, S, lane);
-                staged = c;
+                // c is in buffer cur; the next valid candidate goes to the other
+                const uint32_t rest = vmask & ~((2u << c) - 1u);
+                if (rest) {
+                    const int cn = __ffs(rest) - 1;
+                    int r1, r2;
+                    bool two;
+                    move_rows(__shfl_sync(FULL, desc.x, cn), r1, r2, two);
+                    p_stage_async(G, n, r1, r2, two, S + (cur ^ 1) * 2 * ldg, lane);
+                    if (cur) held0 = cn;
+                    else held1 = cn;
+                    asm volatile("cp.async.wait_group 1;" ::: "memory");
+                } else {
+                    asm volatile("cp.async.wait_group 0;" ::: "memory");
+                }
+                __syncwarp();
+                Sc = S + cur * 2 * ldg;
+                cur ^= 1;
             }
-            if constexpr (PM) d = p_eval<GEN, SG>(u, P, G, S, n, nw, lane);
+            if constexpr (PM) d = p_eval<GEN, SG>(u, P, G, Sc, n, nw, lane);
             else d = l_eval<GEN>(u, W, G, n, lane);
             const int ds = __reduce_add_sync(FULL, d.ds);
             const int dc = __reduce_add_sync(FULL, d.dc);
@@ -1216,11 +1280,19 @@ __device__ void run_large(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int 
                 at_best = false;
             }
             const LUpdate u = l_decode(best_mv);
+            int16_t* Sb = S;
             if constexpr (PM && SG) {
-                // the staging buffer holds the last evaluated candidate's rows
-                if (staged != best_cand) p_stage(G, n, u.R1, u.R2, u.R2 >= 0, S, lane);
+                // the buffers hold the last two evaluated candidates' rows
+                if (held0 == best_cand) {
+                    Sb = S;
+                } else if (held1 == best_cand) {
+                    Sb = S + 2 * ldg;
+                } else {
+                    p_stage(G, n, u.R1, u.R2, u.R2 >= 0, S, lane);
+                    Sb = S;
+                }
             }
-            if constexpr (PM) p_commit<GEN, SG>(best_mv, u, bds, P, G, S, sRes, mino, n, m, nw, sparse, lane);
+            if constexpr (PM) p_commit<GEN, SG>(best_mv, u, bds, P, G, Sb, sRes, mino, n, m, nw, sparse, lane);
             else l_commit<GEN>(best_mv, u, bds, W, G, sRes, mino, mask, n, m, nw, sparse, lane);
             score += bds;
             conflicts += bdc;
