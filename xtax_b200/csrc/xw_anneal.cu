@@ -1391,11 +1391,14 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
 // (warp 0's) structures and the other warps' draw buffers and Views.
 struct SpecOut {
     Choice ch;
+    int32_t acc;        // the Metropolis outcome at the round's starting temperature
+    int32_t pad;
 };
 struct SpecCtl {
     uint64_t it;        // first iteration of the round
     int32_t count;      // iterations of the round (0: the replica stops)
     int32_t pad;
+    double T;           // the temperature at the round's start
 };
 
 struct SpecLayout {
@@ -1441,6 +1444,7 @@ __device__ void run_replica_spec(const AnnealArgs& a, uint32_t rid, uint8_t* slo
         if (ok) build_thresholds<32>(R.sThr, R.T, lane);
         if (lane == 0) {
             ctl->it = ok ? R.it : 0;
+            ctl->T = ok ? R.T : 0.0;
             const bool stop = !ok || R.iters == 0 || (a.stop_on_solve && R.best_s == 0);
             ctl->count = stop ? 0 : (int32_t)(R.iters < (uint64_t)K ? R.iters : (uint64_t)K);
         }
@@ -1480,39 +1484,97 @@ __device__ void run_replica_spec(const AnnealArgs& a, uint32_t rid, uint8_t* slo
         const int cnt = ctl->count;
         if (warp < cnt) {
             const Choice ch = choose_move<1, GEN, 32>(R, P, it0 + (uint64_t)warp, lane);
-            if (lane == 0) outs[warp].ch = ch;
+            // the Metropolis test at the round's starting temperature: the
+            // one warp 0 would make if no cooling or reheat step falls
+            // between the round's start and this iteration
+            bool acc = false;
+            if (ch.b0) {
+                acc = ch.bprim <= 0;
+                if (!acc)
+                    acc = ch.bprim <= (int64_t)kThrTable ? (uint64_t)ch.u < R.sThr[ch.bprim - 1]
+                                                         : metropolis_accept(ch.bprim, ctl->T, ch.u);
+            }
+            if (lane == 0) {
+                outs[warp].ch = ch;
+                outs[warp].acc = acc ? 1 : 0;
+            }
         }
         __syncthreads();
         if (warp == 0) {
-            // iterations in order until the first accepted move
+            // Iterations in order until the first accepted move.  Fast path:
+            // the rejected calls before it change only counters (moves, msi,
+            // cool) unless one of them reaches a cooling or reheat step, so
+            // when none can, they are counted in bulk and only the accepted
+            // move goes through apply_move.  Otherwise the ordered walk.
+            const bool in = lane < cnt;
+            Choice cl = {};
+            int al = 0;
+            if (in) {
+                cl = outs[lane].ch;
+                al = outs[lane].acc;
+            }
+            const unsigned have_m = __ballot_sync(FULL, in && cl.b0 != 0);
+            const unsigned acc_m = __ballot_sync(FULL, in && cl.b0 != 0 && al != 0);
+            // calls (iterations with a candidate) that leave the temperature
+            // unchanged: fewer than `room`
+            const int room = tempering ? 0x7fffffff : min(mpc - R.cool, stuck - R.msi);
+            const int ja = acc_m ? __ffs(acc_m) - 1 : -1;
+            const int jend = ja >= 0 ? ja + 1 : cnt;
+            const int calls = __popc(have_m & (jend >= 32 ? 0xffffffffu : ((1u << jend) - 1u)));
+            const int rejects = ja >= 0 ? calls - 1 : calls;
+            bool fast = rejects < room;
+            // a check of the job's solved flag (every 64th iteration) that
+            // falls in the span and finds it set: take the span in order
+            if (fast && a.stop_on_solve == 1 && (done | 63) < done + (uint64_t)jend &&
+                *(volatile int32_t*)&R.J->solved)
+                fast = false;
             int j = 0;
             bool stop = false;
-#pragma unroll 1
-            for (; j < cnt; ++j) {
-                if (a.stop_on_solve == 1 && ((done + (uint64_t)j) & 63) == 63 &&
-                    *(volatile int32_t*)&R.J->solved) {
-                    stop = true;
-                    break;
-                }
-                const Choice ch = outs[j].ch;
-                R.cand_evals += ch.evals;
-                R.two_row_evals += ch.evals2;
-                if (!ch.b0) {
-                    ++R.it;
-                    continue;
-                }
-                const bool accept =
+            if (fast) {
+                const unsigned span = jend >= 32 ? 0xffffffffu : ((1u << jend) - 1u);
+                R.cand_evals += __reduce_add_sync(FULL, (span >> lane) & 1u ? cl.evals : 0u);
+                R.two_row_evals += __reduce_add_sync(FULL, (span >> lane) & 1u ? cl.evals2 : 0u);
+                R.moves += (uint64_t)rejects;
+                R.msi += rejects;
+                if (!tempering) R.cool += rejects;
+                if (ja >= 0) {
+                    R.it += (uint64_t)ja;
+                    const Choice ch = outs[ja].ch;
                     apply_move<1, GEN, 32>(R, ch, tempering, mpc, stuck, t_min, cooling, reheat, lane);
-                ++R.it;
-                if (accept) {
-                    ++j;
-                    break;
+                    ++R.it;
+                } else {
+                    R.it += (uint64_t)cnt;
+                }
+                j = jend;
+            } else {
+#pragma unroll 1
+                for (; j < cnt; ++j) {
+                    if (a.stop_on_solve == 1 && ((done + (uint64_t)j) & 63) == 63 &&
+                        *(volatile int32_t*)&R.J->solved) {
+                        stop = true;
+                        break;
+                    }
+                    const Choice ch = outs[j].ch;
+                    R.cand_evals += ch.evals;
+                    R.two_row_evals += ch.evals2;
+                    if (!ch.b0) {
+                        ++R.it;
+                        continue;
+                    }
+                    const bool accept =
+                        apply_move<1, GEN, 32>(R, ch, tempering, mpc, stuck, t_min, cooling, reheat, lane);
+                    ++R.it;
+                    if (accept) {
+                        ++j;
+                        break;
+                    }
                 }
             }
             done += (uint64_t)j;
             if (a.stop_on_solve && R.best_s == 0) stop = true;
             if (lane == 0) {
                 ctl->it = R.it;
+                ctl->T = R.T;
                 const uint64_t left = R.iters - done;
                 ctl->count = stop || left == 0 ? 0 : (int32_t)(left < (uint64_t)K ? left : (uint64_t)K);
             }

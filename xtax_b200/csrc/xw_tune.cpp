@@ -116,7 +116,7 @@ TunedShape tuned_shape(int kind, uint32_t slot_bytes, int device) {
 int tuned_warps_per_replica(uint32_t slot_bytes, int device) {
     (void)device;
     // untuned default: 16 warps (W(12,11) single searches on B200, per
-    // search: 0.80 / 1.24 / 1.53 / 1.73 M moves/s at 4 / 8 / 12 / 16 warps)
+    // search: 0.97 / 1.81 / 2.56 / 3.19 M moves/s at 4 / 8 / 12 / 16 warps)
     int k = 16;
     {
         std::lock_guard<std::mutex> lock(g_mu);
