@@ -607,7 +607,7 @@ def uneven_bench(X, iters):
                  squared_objective_fraction=0.0, parity_objective_fraction=0.0, stop_on_solve=0)
     jobs = [{"n": n, "w": w, "seed": 7000 + 100 * i + k, "replicas": UNEVEN_RUNGS}
             for i, (n, w) in enumerate(UNEVEN) for k in range(UNEVEN_INSTANCES)]
-    wpb, tune_ms = X.autotune(jobs, p, iters=2000)
+    wpb, tune_ms = X.autotune(jobs, p, iters=5000)
 
     def timed(js, steps=3):
         b = X.Batch(js, p)

@@ -101,6 +101,17 @@ def test_request_alone_equals_request_in_mix(schedule):
             assert res.verified and X.verify(res.n, res.w, W) == 3
 
 
+def test_served_outcomes_do_not_depend_on_replicas_per_warp():
+    """Orders up to 16 served one and two replicas per warp (the untuned
+    server runs one) reach the same outcomes, move for move."""
+    reqs = [req(12, 11, 4242, 16, 200000), req(14, 13, 11, 24, 4000), req(16, 4, 15, 8, 5000),
+            req(13, 9, 21, 9, 3000, objective=1, move_set=1)]
+    one, _ = serve(reqs, replicas_per_warp=1)
+    two, _ = serve(reqs, replicas_per_warp=2)
+    assert [outcome(*o) for o in one] == [outcome(*o) for o in two]
+    assert one[0][0].solved and one[0][0].verified
+
+
 def test_round_length_does_not_change_the_first_solution():
     r = req(12, 11, 777, 12, 200000)
     (a,), _ = serve([r], quantum_iters=250)
