@@ -135,6 +135,19 @@ void raise_smem_limit(const void* fn, int device) {
           "cudaFuncSetAttribute max dynamic shared memory");
 }
 
+const cudaDeviceProp& device_properties(int device) {
+    static std::mutex mu;
+    static cudaDeviceProp props[64];
+    static bool have[64] = {};
+    if (device < 0 || device >= 64) throw std::invalid_argument("device ordinal out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!have[device]) {
+        check(cudaGetDeviceProperties(&props[device], device), "cudaGetDeviceProperties");
+        have[device] = true;
+    }
+    return props[device];
+}
+
 int large_min_order() {
     const char* e = std::getenv("XW_LARGE_MIN_ORDER");
     if (!e || !*e) return XW_MAX_N + 1;
@@ -368,7 +381,7 @@ void prepare_job(const xw_job_spec& s, const xw_params& p, const int8_t* starts,
 void Batch::build(const xw_job_spec* specs, int njobs, const xw_params& p, const int8_t* starts) {
     params = p;
     check(cudaSetDevice(p.device), "cudaSetDevice");
-    check(cudaGetDeviceProperties(&props, p.device), "cudaGetDeviceProperties");
+    props = device_properties(p.device);
     if (njobs < 1) throw std::invalid_argument("batch needs at least one job");
     jobs.resize(njobs);
     rep_seed.resize(njobs);
@@ -693,7 +706,7 @@ void Batch::load(const std::string& path, const xw_params* over) {
     tempering = params.tempering != 0;
     rep_seed.assign(jobs.size(), 0);
     check(cudaSetDevice(params.device), "cudaSetDevice");
-    check(cudaGetDeviceProperties(&props, params.device), "cudaGetDeviceProperties");
+    props = device_properties(params.device);
     derive_layout();
     upload(host);
 }

@@ -109,6 +109,9 @@ uint64_t chunk_wait_limit_ns();
 // maximum.  Every caller sets the same value, so no caller ever lowers the
 // limit another one relies on (the attribute is per kernel and process-wide).
 void raise_smem_limit(const void* fn, int device);
+// The device's properties, queried once per device and kept (the query
+// took from 8 to over 100 ms per call on a loaded B200 host).
+const cudaDeviceProp& device_properties(int device);
 // Record the fastest shape for that class in the tuning cache.
 void record_tuned(int kind, uint32_t slot_bytes, int wpb, int rpw);
 

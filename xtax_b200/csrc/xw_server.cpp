@@ -766,7 +766,7 @@ void Server::engine_loop() {
 void Server::start() {
     check_cuda(cudaSetDevice(cfg.device), "cudaSetDevice");
     cudaDeviceProp props{};
-    check_cuda(cudaGetDeviceProperties(&props, cfg.device), "cudaGetDeviceProperties");
+    props = device_properties(cfg.device);
     sms = props.multiProcessorCount;
     check_cuda(cudaDeviceGetAttribute(&optin_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, cfg.device),
                "cudaDeviceGetAttribute max opt-in shared memory");
