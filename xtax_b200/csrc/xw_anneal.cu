@@ -37,6 +37,8 @@
 
 #include <type_traits>
 
+#include <cooperative_groups.h>
+
 #include "xw_device.cuh"
 #include "xw_kernels.h"
 
@@ -625,15 +627,21 @@ struct Replica {
     int score, conflicts, best_s, best_c, msi, cool;
     int64_t obj_total;
     double T, reheat_T;
+    // the copy that writes the record (a cluster's other CTAs keep an
+    // identical copy in their own shared memory and write nothing)
+    bool owner;
 };
 
 // Loads replica `rid` into the slot: W and the minority lists, the masks,
 // Gram and residuals rebuilt from W and checked against the header.  False
 // when the replica does not run (job done or solved, budget spent, or a
 // failed self-check, which flags the header).  The group's lanes call it.
+// `owner` false: a copy that writes nothing to the record; it also skips
+// the exits on the job's done and solved flags, which other kernels may set
+// while it loads (its owner decides whether the replica runs).
 template <int OPL, bool GEN, int GW>
 __device__ __forceinline__ bool load_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int lane,
-                                             uint64_t chunk_iters, Replica<OPL, GW>& R) {
+                                             uint64_t chunk_iters, Replica<OPL, GW>& R, bool owner = true) {
     constexpr int MW = Replica<OPL, GW>::MW;
     using GT = typename Replica<OPL, GW>::GT;
     const unsigned gm = group_mask<GW>();
@@ -641,8 +649,9 @@ __device__ __forceinline__ bool load_replica(const AnnealArgs& a, uint32_t rid, 
     RepHeader* H = reinterpret_cast<RepHeader*>(rec);
     const uint32_t jid = H->job;
     XwJob* J = a.jobs + jid;
-    if (*(volatile int32_t*)&J->done) return false;
-    if (a.stop_on_solve == 1 && *(volatile int32_t*)&J->solved) return false;
+    R.owner = owner;
+    if (owner && *(volatile int32_t*)&J->done) return false;
+    if (owner && a.stop_on_solve == 1 && *(volatile int32_t*)&J->solved) return false;
 
     // eight rows per lane: int16 Gram and 256-bit row masks (slot_layout)
     const int n = J->n, w = J->w, m = J->m, sparse = J->sparse;
@@ -763,7 +772,7 @@ __device__ __forceinline__ bool load_replica(const AnnealArgs& a, uint32_t rid, 
         R.accepted = 0;
         R.accepted_rows = 0;
         R.two_row_evals = 0;
-        copy16<GW>(rec + J->off_best, sW, nn, lane);
+        if (owner) copy16<GW>(rec + J->off_best, sW, nn, lane);
     }
     R.score = score0;
     R.conflicts = conf0;
@@ -1004,8 +1013,8 @@ __device__ __forceinline__ bool apply_move(Replica<OPL, GW>& R, const Choice& ch
         R.best_s = R.score;
         R.best_c = R.conflicts;
         R.msi = 0;
-        copy16<GW>(R.rec + R.J->off_best, R.sW, R.nn, lane);
-        if (R.best_s == 0 && lane == 0) {
+        if (R.owner) copy16<GW>(R.rec + R.J->off_best, R.sW, R.nn, lane);
+        if (R.best_s == 0 && lane == 0 && R.owner) {
             RepHeader* H = R.H;
             XwJob* J = R.J;
             H->solve_it = R.it;
@@ -1401,59 +1410,85 @@ struct SpecCtl {
     double T;           // the temperature at the round's start
 };
 
+// Per round buffer (two, used in turn): the outcomes of all the round's
+// warps (K per CTA, CL CTAs), and the job's solved flag as the cluster's
+// owner read it.
 struct SpecLayout {
     SlotLayout L;
-    uint32_t off_extra, per_warp, off_out, off_ctl, bytes;
+    uint32_t off_extra, per_warp, off_out, out_stride, off_flag, off_ctl, bytes;
 };
 
 // the latency-mode regions after a slot of `slot_bytes` (the one-warp
-// layout of the replica, or the largest of a launch's replicas)
-__host__ __device__ inline void spec_regions(uint32_t slot_bytes, int K, SpecLayout& S) {
+// layout of the replica, or the largest of a launch's replicas), for K
+// warps per CTA and CL CTAs per replica
+__host__ __device__ inline void spec_regions(uint32_t slot_bytes, int K, int CL, SpecLayout& S) {
     S.per_warp = 32u * 16u + xw_pad16((uint32_t)sizeof(View));
     S.off_extra = xw_pad16(slot_bytes);
     S.off_out = S.off_extra + (uint32_t)(K - 1) * S.per_warp;
-    S.off_ctl = xw_pad16(S.off_out + (uint32_t)K * (uint32_t)sizeof(SpecOut));
+    S.out_stride = xw_pad16((uint32_t)(K * CL) * (uint32_t)sizeof(SpecOut));
+    S.off_flag = S.off_out + 2u * S.out_stride;
+    S.off_ctl = xw_pad16(S.off_flag + 2u * 4u);
     S.bytes = S.off_ctl + (uint32_t)sizeof(SpecCtl);
 }
 
-__host__ __device__ inline SpecLayout spec_layout(int n, int m, int K) {
+__host__ __device__ inline SpecLayout spec_layout(int n, int m, int K, int CL) {
     SpecLayout S;
     S.L = slot_layout(n, m, false);
-    spec_regions(S.L.bytes, K, S);
+    spec_regions(S.L.bytes, K, CL, S);
     return S;
 }
 
-template <bool GEN>
+// The replica loop of a CTA of the latency mode.  With CL > 1 the replica
+// runs on a cluster of CL CTAs (on CL SMs): every CTA loads its own copy,
+// the cluster's warps speculate CL * K iterations, every warp writes its
+// outcome into every CTA's round buffer (distributed shared memory), and
+// after a cluster barrier each CTA's warp 0 makes the same walk and the
+// same commit on its own copy, so the copies stay identical; only rank 0
+// writes the record.  Everything that steers the walk is either the
+// CTAs' identical state or read by rank 0 alone and exchanged (whether
+// the replica runs at all, and the job's solved flag each round), so the
+// CTAs take the same branches and meet at every barrier.
+template <bool GEN, int CL>
 __device__ void run_replica_spec(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int warp, int K, int lane) {
+    namespace cg = cooperative_groups;
+    const int rank = CL > 1 ? (int)cg::this_cluster().block_rank() : 0;
+    const bool owner = rank == 0;
     SpecCtl* ctl = nullptr;
     Replica<1, 32> R;
     bool ok = false;
     // warp 0 loads the replica; the round size goes to the others through
     // shared memory
-    if (warp == 0) ok = load_replica<1, GEN, 32>(a, rid, slot, lane, a.iters, R);
+    if (warp == 0) ok = load_replica<1, GEN, 32>(a, rid, slot, lane, a.iters, R, owner);
     // every warp reads the order to find the layout
     const XwJob* J = a.jobs + reinterpret_cast<const RepHeader*>(a.arena + a.rec_off[rid])->job;
-    const SpecLayout S = spec_layout(J->n, J->m, K);
+    const SpecLayout S = spec_layout(J->n, J->m, K, CL);
     ctl = reinterpret_cast<SpecCtl*>(slot + S.off_ctl);
-    SpecOut* outs = reinterpret_cast<SpecOut*>(slot + S.off_out);
     const int tempering = J->tempering;
     const int mpc = J->moves_per_cool, stuck = J->stuck_threshold;
     const double t_min = J->t_min, cooling = J->cooling, reheat = J->reheat;
+    const int KT = K * CL;
     uint64_t done = 0;
     if (warp == 0) {
         if (ok) build_thresholds<32>(R.sThr, R.T, lane);
-        if (lane == 0) {
-            ctl->it = ok ? R.it : 0;
-            ctl->T = ok ? R.T : 0.0;
+        if (lane == 0 && owner) {
+            SpecCtl c;
+            c.it = ok ? R.it : 0;
+            c.T = ok ? R.T : 0.0;
+            c.pad = 0;
             const bool stop = !ok || R.iters == 0 || (a.stop_on_solve && R.best_s == 0);
-            ctl->count = stop ? 0 : (int32_t)(R.iters < (uint64_t)K ? R.iters : (uint64_t)K);
+            c.count = stop ? 0 : (int32_t)(R.iters < (uint64_t)KT ? R.iters : (uint64_t)KT);
+            *ctl = c;
+            if constexpr (CL > 1) {
+                for (int q = 1; q < CL; ++q) *cg::this_cluster().map_shared_rank(ctl, q) = c;
+            }
         }
     }
-    __syncthreads();
+    if constexpr (CL > 1) cg::this_cluster().sync();
+    else __syncthreads();
     if (ctl->count == 0) {
         // nothing to run: the loaded replica's record still gets its
         // rebuilt state, as the one-warp kernel writes it
-        if (warp == 0 && ok) store_replica<1, 32>(R, lane);
+        if (warp == 0 && ok && owner) store_replica<1, 32>(R, lane);
         return;
     }
     // every warp: the replica's structures (read-only until warp 0 commits)
@@ -1465,6 +1500,7 @@ __device__ void run_replica_spec(const AnnealArgs& a, uint32_t rid, uint8_t* slo
         R.H = reinterpret_cast<RepHeader*>(R.rec);
         R.n = J->n; R.w = J->w; R.m = J->m; R.sparse = J->sparse; R.ld = L.ld;
         R.obj_kind = GEN ? R.H->obj_kind : 0;
+        R.owner = owner;
         R.sW = reinterpret_cast<int8_t*>(slot);
         R.sG = reinterpret_cast<int32_t*>(slot + L.off_g);
         R.sRes = reinterpret_cast<int32_t*>(slot + L.off_res);
@@ -1478,12 +1514,16 @@ __device__ void run_replica_spec(const AnnealArgs& a, uint32_t rid, uint8_t* slo
     Proposer<32> P;
     setup_proposer<1, 32>(R, reinterpret_cast<uint4*>(mine), view, lane, P);
 
+    const int g = rank * K + warp;   // this warp's iteration within the round
 #pragma unroll 1
-    for (;;) {
+    for (int round = 0;; ++round) {
+        const int buf = round & 1;
+        SpecOut* outs = reinterpret_cast<SpecOut*>(slot + S.off_out + (uint32_t)buf * S.out_stride);
+        int32_t* flag = reinterpret_cast<int32_t*>(slot + S.off_flag) + buf;
         const uint64_t it0 = ctl->it;
         const int cnt = ctl->count;
-        if (warp < cnt) {
-            const Choice ch = choose_move<1, GEN, 32>(R, P, it0 + (uint64_t)warp, lane);
+        if (g < cnt) {
+            const Choice ch = choose_move<1, GEN, 32>(R, P, it0 + (uint64_t)g, lane);
             // the Metropolis test at the round's starting temperature: the
             // one warp 0 would make if no cooling or reheat step falls
             // between the round's start and this iteration
@@ -1495,17 +1535,38 @@ __device__ void run_replica_spec(const AnnealArgs& a, uint32_t rid, uint8_t* slo
                                                          : metropolis_accept(ch.bprim, ctl->T, ch.u);
             }
             if (lane == 0) {
-                outs[warp].ch = ch;
-                outs[warp].acc = acc ? 1 : 0;
+                SpecOut o;
+                o.ch = ch;
+                o.acc = acc ? 1 : 0;
+                o.pad = 0;
+                outs[g] = o;
+                if constexpr (CL > 1) {
+                    for (int q = 0; q < CL; ++q)
+                        if (q != rank) cg::this_cluster().map_shared_rank(outs, q)[g] = o;
+                }
             }
         }
-        __syncthreads();
+        if constexpr (CL > 1) {
+            if (owner && warp == 0 && lane == 0) {
+                const int32_t sv = a.stop_on_solve == 1 ? *(volatile int32_t*)&R.J->solved : 0;
+                for (int q = 0; q < CL; ++q) *cg::this_cluster().map_shared_rank(flag, q) = sv;
+            }
+            cg::this_cluster().sync();
+        } else {
+            __syncthreads();
+        }
         if (warp == 0) {
             // Iterations in order until the first accepted move.  Fast path:
             // the rejected calls before it change only counters (moves, msi,
             // cool) unless one of them reaches a cooling or reheat step, so
             // when none can, they are counted in bulk and only the accepted
             // move goes through apply_move.  Otherwise the ordered walk.
+            // The job's solved flag: read here on one CTA, as the owner read
+            // it this round on a cluster.
+            auto solved = [&]() -> bool {
+                if constexpr (CL > 1) return *flag != 0;
+                else return *(volatile int32_t*)&R.J->solved != 0;
+            };
             const bool in = lane < cnt;
             Choice cl = {};
             int al = 0;
@@ -1525,9 +1586,7 @@ __device__ void run_replica_spec(const AnnealArgs& a, uint32_t rid, uint8_t* slo
             bool fast = rejects < room;
             // a check of the job's solved flag (every 64th iteration) that
             // falls in the span and finds it set: take the span in order
-            if (fast && a.stop_on_solve == 1 && (done | 63) < done + (uint64_t)jend &&
-                *(volatile int32_t*)&R.J->solved)
-                fast = false;
+            if (fast && a.stop_on_solve == 1 && (done | 63) < done + (uint64_t)jend && solved()) fast = false;
             int j = 0;
             bool stop = false;
             if (fast) {
@@ -1549,8 +1608,7 @@ __device__ void run_replica_spec(const AnnealArgs& a, uint32_t rid, uint8_t* slo
             } else {
 #pragma unroll 1
                 for (; j < cnt; ++j) {
-                    if (a.stop_on_solve == 1 && ((done + (uint64_t)j) & 63) == 63 &&
-                        *(volatile int32_t*)&R.J->solved) {
+                    if (a.stop_on_solve == 1 && ((done + (uint64_t)j) & 63) == 63 && solved()) {
                         stop = true;
                         break;
                     }
@@ -1576,13 +1634,16 @@ __device__ void run_replica_spec(const AnnealArgs& a, uint32_t rid, uint8_t* slo
                 ctl->it = R.it;
                 ctl->T = R.T;
                 const uint64_t left = R.iters - done;
-                ctl->count = stop || left == 0 ? 0 : (int32_t)(left < (uint64_t)K ? left : (uint64_t)K);
+                ctl->count = stop || left == 0 ? 0 : (int32_t)(left < (uint64_t)KT ? left : (uint64_t)KT);
             }
         }
         __syncthreads();
         if (ctl->count == 0) break;
     }
-    if (warp == 0) store_replica<1, 32>(R, lane);
+    if (warp == 0 && owner) store_replica<1, 32>(R, lane);
+    // the other CTAs' copies stay in their shared memory until every CTA
+    // of the cluster has made its last remote write into this one
+    if constexpr (CL > 1) cg::this_cluster().sync();
 }
 
 // Register budget per thread; it sets how many replica warps an SM holds.
@@ -1637,18 +1698,25 @@ __global__ void __maxnreg__(anneal_maxnreg(OPL, GEN, GW)) anneal_kernel(AnnealAr
 
 // Latency mode: each CTA of K warps owns one replica at a time (orders up
 // to 32), taken from the launch's counter.
-template <bool GEN>
+// The latency mode: one CTA (CL = 1, a persistent loop over the launch's
+// replicas) or one cluster of CL CTAs (one replica per cluster) per replica.
+template <bool GEN, int CL>
 __global__ void __launch_bounds__(512, 1) anneal_spec_kernel(AnnealArgs a, int K) {
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ uint32_t s_item;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
+    if constexpr (CL > 1) {
+        const uint32_t item = blockIdx.x / CL;
+        if (item < a.n_items) run_replica_spec<GEN, CL>(a, a.items[item], smem, warp, K, lane);
+        return;
+    }
     for (;;) {
         if (threadIdx.x == 0) s_item = atomicAdd(a.counter, 1u);
         __syncthreads();
         const uint32_t item = s_item;
         if (item >= a.n_items) break;
-        run_replica_spec<GEN>(a, a.items[item], smem, warp, K, lane);
+        run_replica_spec<GEN, 1>(a, a.items[item], smem, warp, K, lane);
         __syncthreads();
     }
 }
@@ -1810,23 +1878,47 @@ cudaError_t launch_anneal(const AnnealArgs& args, int opl, bool general, int war
     return cudaLaunchKernel(anneal_kernel_fn(opl, general, rpw), grid, block, kargs, smem, stream);
 }
 
-uint32_t anneal_spec_cta_bytes(uint32_t slot_bytes, int K) {
+// warps per replica W: one CTA of W warps up to 16, a cluster of two CTAs
+// of W/2 warps above
+static int spec_cluster(int wpr) { return wpr > 16 ? 2 : 1; }
+
+uint32_t anneal_spec_cta_bytes(uint32_t slot_bytes, int wpr) {
+    const int CL = spec_cluster(wpr);
     SpecLayout S;
-    spec_regions(slot_bytes, K, S);
+    spec_regions(slot_bytes, wpr / CL, CL, S);
     return S.bytes;
 }
 
-const void* anneal_spec_kernel_fn(bool general) {
-    return general ? reinterpret_cast<const void*>(&anneal_spec_kernel<true>)
-                   : reinterpret_cast<const void*>(&anneal_spec_kernel<false>);
+const void* anneal_spec_kernel_fn(bool general, int wpr) {
+    if (spec_cluster(wpr) == 2)
+        return general ? reinterpret_cast<const void*>(&anneal_spec_kernel<true, 2>)
+                       : reinterpret_cast<const void*>(&anneal_spec_kernel<false, 2>);
+    return general ? reinterpret_cast<const void*>(&anneal_spec_kernel<true, 1>)
+                   : reinterpret_cast<const void*>(&anneal_spec_kernel<false, 1>);
 }
 
-cudaError_t launch_anneal_spec(const AnnealArgs& args, bool general, int K, int blocks, cudaStream_t stream) {
-    if (K < 2 || K > 16 || args.chunks != 1) return cudaErrorInvalidValue;
-    const dim3 grid(blocks), block(32 * K);
-    int k = K;
+cudaError_t launch_anneal_spec(const AnnealArgs& args, bool general, int wpr, int blocks, cudaStream_t stream) {
+    if (wpr < 2 || wpr > 32 || (wpr > 16 && (wpr & 1)) || args.chunks != 1) return cudaErrorInvalidValue;
+    const int CL = spec_cluster(wpr);
+    int k = wpr / CL;
     void* kargs[] = {const_cast<AnnealArgs*>(&args), &k};
-    return cudaLaunchKernel(anneal_spec_kernel_fn(general), grid, block, kargs, args.slot_bytes, stream);
+    if (CL == 1)
+        return cudaLaunchKernel(anneal_spec_kernel_fn(general, wpr), dim3(blocks), dim3(32 * k), kargs,
+                                args.slot_bytes, stream);
+    // one cluster of CL CTAs per replica
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(CL * args.n_items);
+    cfg.blockDim = dim3(32 * k);
+    cfg.dynamicSmemBytes = args.slot_bytes;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CL;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelExC(&cfg, anneal_spec_kernel_fn(general, wpr), kargs);
 }
 
 cudaError_t launch_exchange(XwJob* jobs, int njobs, uint8_t* arena, const uint64_t* rec_off, const double* ladder,
