@@ -96,7 +96,8 @@ typedef struct xw_params {
                                      speculate as many iterations at once and keep the first
                                      accepted one (same trajectory, lower latency per move),
                                      18..32 (even) = a cluster of two CTAs on two SMs per
-                                     replica, half the warps on each */
+                                     replica, half the warps on each, 36..64 (multiples of 4)
+                                     = a cluster of four */
     int32_t restart_kicks;        /* elite restarts: 0 = kicks on the host with the reference's
                                      mt19937 streams (xweigh_cuda.cu:2089-2193), after reading
                                      the job's records back; 1 = kicks on the device with a
@@ -304,8 +305,8 @@ typedef struct xw_launch_class {
     int32_t chunks;                /* work items per replica and launch */
     int32_t replicas;
     int32_t general;               /* the general kernel (squared/parity objectives, row swaps) */
-    int32_t warps_per_replica;     /* 1, or 2..32 in the latency mode (one replica per CTA, or
-                                      per cluster of two CTAs above 16) */
+    int32_t warps_per_replica;     /* 1, or 2..64 in the latency mode (one replica per CTA, or
+                                      per cluster of two CTAs above 16, four above 32) */
 } xw_launch_class;
 /* Up to `cap` launch classes of the batch into out; *count receives how
  * many there are. */

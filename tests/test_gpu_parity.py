@@ -226,7 +226,7 @@ def test_orders_of_several_classes_in_one_round_match_oracle():
     batch.close()
 
 
-@pytest.mark.parametrize("wpr", [2, 4, 8, 16, 32])
+@pytest.mark.parametrize("wpr", [2, 4, 8, 16, 32, 64])
 @pytest.mark.parametrize("stop", [0, 2])
 def test_latency_mode_ends_every_replica_as_one_warp(wpr, stop):
     # every warps-per-replica count and both deterministic stop rules (run
@@ -256,17 +256,18 @@ def test_latency_mode_ends_every_replica_as_one_warp(wpr, stop):
     assert out[0] == out[1]
 
 
-def test_latency_cluster_with_the_job_stop_rule():
+@pytest.mark.parametrize("wpr", [32, 64])
+def test_latency_cluster_with_the_job_stop_rule(wpr):
     """Stop rule 1 (every replica of a job stops soon after any solve) on
-    clusters of two CTAs per replica: the job's solved flag, which other
-    replicas set while the launch runs, reaches both CTAs of a cluster as
-    one value, so they stop together; every replica ends without an error,
-    and the solved jobs report a verified solution."""
+    clusters of two and four CTAs per replica: the job's solved flag, which
+    other replicas set while the launch runs, reaches every CTA of a cluster
+    as one value, so they stop together; every replica ends without an
+    error, and the solved jobs report a verified solution."""
     jobs = [{"n": 12, "w": 11, "seed": 900 + k, "replicas": 3} for k in range(8)]
-    p = X.Params(stop_on_solve=1, t_init=3.0, moves_per_launch=2500, warps_per_replica=32,
+    p = X.Params(stop_on_solve=1, t_init=3.0, moves_per_launch=2500, warps_per_replica=wpr,
                  stuck_threshold=900, moves_per_cool=60, max_moves=3 * 20000)
     b = X.Batch(jobs, p)
-    assert all(c["warps_per_replica"] == 32 for c in b.classes())
+    assert all(c["warps_per_replica"] == wpr for c in b.classes())
     b.run(20000)
     b.synchronize()
     for j, jb in enumerate(jobs):

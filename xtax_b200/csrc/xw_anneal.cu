@@ -1567,21 +1567,29 @@ __device__ void run_replica_spec(const AnnealArgs& a, uint32_t rid, uint8_t* slo
                 if constexpr (CL > 1) return *flag != 0;
                 else return *(volatile int32_t*)&R.J->solved != 0;
             };
-            const bool in = lane < cnt;
-            Choice cl = {};
-            int al = 0;
-            if (in) {
-                cl = outs[lane].ch;
-                al = outs[lane].acc;
+            // lane l holds the outcomes of iterations l and 32 + l (up to 64
+            // iterations a round, on a cluster of four)
+            Choice cl0 = {}, cl1 = {};
+            int al0 = 0, al1 = 0;
+            if (lane < cnt) {
+                cl0 = outs[lane].ch;
+                al0 = outs[lane].acc;
             }
-            const unsigned have_m = __ballot_sync(FULL, in && cl.b0 != 0);
-            const unsigned acc_m = __ballot_sync(FULL, in && cl.b0 != 0 && al != 0);
+            if (32 + lane < cnt) {
+                cl1 = outs[32 + lane].ch;
+                al1 = outs[32 + lane].acc;
+            }
+            const uint64_t have_m = (uint64_t)__ballot_sync(FULL, cl0.b0 != 0) |
+                                    ((uint64_t)__ballot_sync(FULL, cl1.b0 != 0) << 32);
+            const uint64_t acc_m = (uint64_t)__ballot_sync(FULL, cl0.b0 != 0 && al0 != 0) |
+                                   ((uint64_t)__ballot_sync(FULL, cl1.b0 != 0 && al1 != 0) << 32);
             // calls (iterations with a candidate) that leave the temperature
             // unchanged: fewer than `room`
             const int room = tempering ? 0x7fffffff : min(mpc - R.cool, stuck - R.msi);
-            const int ja = acc_m ? __ffs(acc_m) - 1 : -1;
+            const int ja = acc_m ? __ffsll((long long)acc_m) - 1 : -1;
             const int jend = ja >= 0 ? ja + 1 : cnt;
-            const int calls = __popc(have_m & (jend >= 32 ? 0xffffffffu : ((1u << jend) - 1u)));
+            const uint64_t span = jend >= 64 ? ~0ull : ((1ull << jend) - 1ull);
+            const int calls = __popcll(have_m & span);
             const int rejects = ja >= 0 ? calls - 1 : calls;
             bool fast = rejects < room;
             // a check of the job's solved flag (every 64th iteration) that
@@ -1590,9 +1598,9 @@ __device__ void run_replica_spec(const AnnealArgs& a, uint32_t rid, uint8_t* slo
             int j = 0;
             bool stop = false;
             if (fast) {
-                const unsigned span = jend >= 32 ? 0xffffffffu : ((1u << jend) - 1u);
-                R.cand_evals += __reduce_add_sync(FULL, (span >> lane) & 1u ? cl.evals : 0u);
-                R.two_row_evals += __reduce_add_sync(FULL, (span >> lane) & 1u ? cl.evals2 : 0u);
+                const bool in0 = (span >> lane) & 1ull, in1 = (span >> (32 + lane)) & 1ull;
+                R.cand_evals += __reduce_add_sync(FULL, (in0 ? cl0.evals : 0u) + (in1 ? cl1.evals : 0u));
+                R.two_row_evals += __reduce_add_sync(FULL, (in0 ? cl0.evals2 : 0u) + (in1 ? cl1.evals2 : 0u));
                 R.moves += (uint64_t)rejects;
                 R.msi += rejects;
                 if (!tempering) R.cool += rejects;
@@ -1879,8 +1887,8 @@ cudaError_t launch_anneal(const AnnealArgs& args, int opl, bool general, int war
 }
 
 // warps per replica W: one CTA of W warps up to 16, a cluster of two CTAs
-// of W/2 warps above
-static int spec_cluster(int wpr) { return wpr > 16 ? 2 : 1; }
+// of W/2 warps up to 32, of four CTAs of W/4 warps up to 64
+static int spec_cluster(int wpr) { return wpr > 32 ? 4 : wpr > 16 ? 2 : 1; }
 
 uint32_t anneal_spec_cta_bytes(uint32_t slot_bytes, int wpr) {
     const int CL = spec_cluster(wpr);
@@ -1890,6 +1898,9 @@ uint32_t anneal_spec_cta_bytes(uint32_t slot_bytes, int wpr) {
 }
 
 const void* anneal_spec_kernel_fn(bool general, int wpr) {
+    if (spec_cluster(wpr) == 4)
+        return general ? reinterpret_cast<const void*>(&anneal_spec_kernel<true, 4>)
+                       : reinterpret_cast<const void*>(&anneal_spec_kernel<false, 4>);
     if (spec_cluster(wpr) == 2)
         return general ? reinterpret_cast<const void*>(&anneal_spec_kernel<true, 2>)
                        : reinterpret_cast<const void*>(&anneal_spec_kernel<false, 2>);
@@ -1898,8 +1909,8 @@ const void* anneal_spec_kernel_fn(bool general, int wpr) {
 }
 
 cudaError_t launch_anneal_spec(const AnnealArgs& args, bool general, int wpr, int blocks, cudaStream_t stream) {
-    if (wpr < 2 || wpr > 32 || (wpr > 16 && (wpr & 1)) || args.chunks != 1) return cudaErrorInvalidValue;
     const int CL = spec_cluster(wpr);
+    if (wpr < 2 || wpr > 64 || wpr % CL != 0 || args.chunks != 1) return cudaErrorInvalidValue;
     int k = wpr / CL;
     void* kargs[] = {const_cast<AnnealArgs*>(&args), &k};
     if (CL == 1)

@@ -208,8 +208,9 @@ std::string validate(int n, int w, const xw_params& p) {
     if (p.start_kind < 0 || p.start_kind > 1) return "CUDA start kind must be 0 or 1";
     if (p.warps_per_block < 0 || p.warps_per_block > 16) return "CUDA warps per block must be in [0, 16]";
     if (p.replicas_per_warp < 0 || p.replicas_per_warp > 2) return "CUDA replicas per warp must be 0, 1 or 2";
-    if (p.warps_per_replica < 0 || p.warps_per_replica > 32 || (p.warps_per_replica > 16 && (p.warps_per_replica & 1)))
-        return "CUDA warps per replica must be in [0, 16], or even up to 32";
+    if (p.warps_per_replica < 0 || p.warps_per_replica > 64 ||
+        (p.warps_per_replica > 16 && p.warps_per_replica % (p.warps_per_replica > 32 ? 4 : 2) != 0))
+        return "CUDA warps per replica must be in [0, 16], even up to 32, or a multiple of 4 up to 64";
     if (p.restart_kicks < 0 || p.restart_kicks > 1) return "CUDA restart kicks must be 0 (host) or 1 (device)";
     if (p.stop_on_solve < 0 || p.stop_on_solve > 2) return "CUDA stop-on-solve mode must be 0, 1 or 2";
     return {};
@@ -760,8 +761,9 @@ void Batch::configure_shape() {
             int wpr = params.warps_per_replica;
             if (wpr == 0 && c.item_count <= (uint32_t)props.multiProcessorCount) {
                 wpr = tuned_warps_per_replica(c.slot_bytes, params.device);
-                // a cluster of two SMs per replica only while every replica
-                // has its two SMs
+                // a cluster of two or four SMs per replica only while every
+                // replica has its SMs
+                if (wpr > 32 && 4 * c.item_count > (uint32_t)props.multiProcessorCount) wpr = 32;
                 if (wpr > 16 && 2 * c.item_count > (uint32_t)props.multiProcessorCount) wpr = 16;
             }
             if (wpr > 1 && configure_latency(k, wpr)) continue;
@@ -802,9 +804,9 @@ bool Batch::configure_latency(size_t k, int wpr) {
         graph_exec = nullptr;
     }
     LaunchClass& c = classes.at(k);
-    if (c.max_n > 32 || wpr < 2 || wpr > 32 || (wpr > 16 && (wpr & 1))) return false;
-    // above 16 warps a replica takes a cluster of two CTAs on two SMs
-    const int cl = wpr > 16 ? 2 : 1;
+    // above 16 warps a replica takes a cluster of two CTAs, above 32 of four
+    const int cl = wpr > 32 ? 4 : wpr > 16 ? 2 : 1;
+    if (c.max_n > 32 || wpr < 2 || wpr > 64 || wpr % cl != 0) return false;
     const void* fn = anneal_spec_kernel_fn(c.general, wpr);
     raise_smem_limit(fn, params.device);
     const uint32_t bytes = anneal_spec_cta_bytes(c.slot_bytes, wpr);
@@ -1630,8 +1632,9 @@ int32_t xw_autotune(const xw_job_spec* jobs, int32_t njobs, const xw_params* pin
             int best_wpr = 1;
             float best_lat = 0.0f;
             if (all[k].max_n <= 32 && all[k].item_count <= (uint32_t)b.props.multiProcessorCount) {
-                for (int wpr : {2, 4, 8, 16, 32}) {
-                    if (wpr > 16 && 2 * all[k].item_count > (uint32_t)b.props.multiProcessorCount) continue;
+                for (int wpr : {2, 4, 8, 16, 32, 64}) {
+                    if (wpr > 16 && (uint32_t)(wpr / 16) * all[k].item_count > (uint32_t)b.props.multiProcessorCount)
+                        continue;
                     if (!b.configure_latency(0, wpr)) continue;
                     const float t = time_trial();
                     if (best_wpr == 1 || t < best_lat) {

@@ -118,11 +118,11 @@ TunedShape tuned_shape(int kind, uint32_t slot_bytes, int device) {
 
 int tuned_warps_per_replica(uint32_t slot_bytes, int device) {
     (void)device;
-    // untuned default: 32 warps, a cluster of two CTAs (W(12,11) single
-    // searches on B200, per search: 0.97 / 1.81 / 2.56 / 3.19 M moves/s at
-    // 4 / 8 / 12 / 16 warps on one SM); the host falls back to 16 where a
-    // class has more replicas than half the SMs
-    int k = 32;
+    // untuned default: 64 warps, a cluster of four CTAs (W(12,11) single
+    // searches on B200, per search: 1.81 / 3.17 M moves/s at 8 / 16 warps
+    // on one SM, 5.02 M at 32 on two); the host falls back to 32 or 16
+    // where a class has more replicas than a quarter or half of the SMs
+    int k = 64;
     {
         std::lock_guard<std::mutex> lock(g_mu);
         load_locked();
@@ -132,7 +132,7 @@ int tuned_warps_per_replica(uint32_t slot_bytes, int device) {
                 break;
             }
     }
-    if (const int v = env_int("XW_WARPS_PER_REPLICA", 1, 32)) k = v;
+    if (const int v = env_int("XW_WARPS_PER_REPLICA", 1, 64)) k = v;
     return k;
 }
 
