@@ -1886,35 +1886,34 @@ cudaError_t launch_anneal(const AnnealArgs& args, int opl, bool general, int war
     return cudaLaunchKernel(anneal_kernel_fn(opl, general, rpw), grid, block, kargs, smem, stream);
 }
 
-// warps per replica W: one CTA of W warps up to 16, a cluster of two CTAs
-// of W/2 warps up to 32, of four CTAs of W/4 warps up to 64
-static int spec_cluster(int wpr) { return wpr > 32 ? 4 : wpr > 16 ? 2 : 1; }
-
-uint32_t anneal_spec_cta_bytes(uint32_t slot_bytes, int wpr) {
-    const int CL = spec_cluster(wpr);
+// wpr warps per replica on `ctas` CTAs (1, 2 or 4; a cluster above 1) of
+// wpr / ctas warps each
+uint32_t anneal_spec_cta_bytes(uint32_t slot_bytes, int wpr, int ctas) {
     SpecLayout S;
-    spec_regions(slot_bytes, wpr / CL, CL, S);
+    spec_regions(slot_bytes, wpr / ctas, ctas, S);
     return S.bytes;
 }
 
-const void* anneal_spec_kernel_fn(bool general, int wpr) {
-    if (spec_cluster(wpr) == 4)
+const void* anneal_spec_kernel_fn(bool general, int ctas) {
+    if (ctas == 4)
         return general ? reinterpret_cast<const void*>(&anneal_spec_kernel<true, 4>)
                        : reinterpret_cast<const void*>(&anneal_spec_kernel<false, 4>);
-    if (spec_cluster(wpr) == 2)
+    if (ctas == 2)
         return general ? reinterpret_cast<const void*>(&anneal_spec_kernel<true, 2>)
                        : reinterpret_cast<const void*>(&anneal_spec_kernel<false, 2>);
     return general ? reinterpret_cast<const void*>(&anneal_spec_kernel<true, 1>)
                    : reinterpret_cast<const void*>(&anneal_spec_kernel<false, 1>);
 }
 
-cudaError_t launch_anneal_spec(const AnnealArgs& args, bool general, int wpr, int blocks, cudaStream_t stream) {
-    const int CL = spec_cluster(wpr);
-    if (wpr < 2 || wpr > 64 || wpr % CL != 0 || args.chunks != 1) return cudaErrorInvalidValue;
+cudaError_t launch_anneal_spec(const AnnealArgs& args, bool general, int wpr, int ctas, int blocks,
+                               cudaStream_t stream) {
+    const int CL = ctas;
+    if ((CL != 1 && CL != 2 && CL != 4) || wpr % CL != 0 || wpr / CL < 2 || wpr / CL > 16 || args.chunks != 1)
+        return cudaErrorInvalidValue;
     int k = wpr / CL;
     void* kargs[] = {const_cast<AnnealArgs*>(&args), &k};
     if (CL == 1)
-        return cudaLaunchKernel(anneal_spec_kernel_fn(general, wpr), dim3(blocks), dim3(32 * k), kargs,
+        return cudaLaunchKernel(anneal_spec_kernel_fn(general, 1), dim3(blocks), dim3(32 * k), kargs,
                                 args.slot_bytes, stream);
     // one cluster of CL CTAs per replica
     cudaLaunchConfig_t cfg = {};
@@ -1929,7 +1928,7 @@ cudaError_t launch_anneal_spec(const AnnealArgs& args, bool general, int wpr, in
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelExC(&cfg, anneal_spec_kernel_fn(general, wpr), kargs);
+    return cudaLaunchKernelExC(&cfg, anneal_spec_kernel_fn(general, CL), kargs);
 }
 
 cudaError_t launch_exchange(XwJob* jobs, int njobs, uint8_t* arena, const uint64_t* rec_off, const double* ladder,

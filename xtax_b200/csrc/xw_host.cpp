@@ -804,12 +804,28 @@ bool Batch::configure_latency(size_t k, int wpr) {
         graph_exec = nullptr;
     }
     LaunchClass& c = classes.at(k);
-    // above 16 warps a replica takes a cluster of two CTAs, above 32 of four
-    const int cl = wpr > 32 ? 4 : wpr > 16 ? 2 : 1;
-    if (c.max_n > 32 || wpr < 2 || wpr > 64 || wpr % cl != 0) return false;
-    const void* fn = anneal_spec_kernel_fn(c.general, wpr);
+    if (c.max_n > 32 || wpr < 2 || wpr > 64) return false;
+    // the warps spread over as many CTAs (a cluster of up to four, one per
+    // SM) as the class's replicas leave SMs for, at 8 to 16 warps per CTA
+    // (C1, W(12,11) per search: 32 warps as four CTAs of 8 5.50 M moves/s,
+    // as two of 16 5.14 M; 8 warps as four CTAs of 2 1.61 M, as one CTA
+    // 1.81 M).  Failing that, the fewest CTAs of 2 to 16 warps that hold
+    // them (their clusters then run in turns).
+    int cl = 0;
+    for (int q : {4, 2, 1}) {
+        if (wpr % q != 0 || wpr / q > 16 || (q > 1 && wpr / q < 8)) continue;
+        if (q > 1 && (uint32_t)q * c.item_count > (uint32_t)props.multiProcessorCount) continue;
+        cl = q;
+        break;
+    }
+    for (int q : {1, 2, 4}) {
+        if (cl != 0) break;
+        if (wpr % q == 0 && wpr / q >= 2 && wpr / q <= 16) cl = q;
+    }
+    if (cl == 0) return false;
+    const void* fn = anneal_spec_kernel_fn(c.general, cl);
     raise_smem_limit(fn, params.device);
-    const uint32_t bytes = anneal_spec_cta_bytes(c.slot_bytes, wpr);
+    const uint32_t bytes = anneal_spec_cta_bytes(c.slot_bytes, wpr, cl);
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * (wpr / cl), bytes) != cudaSuccess) {
         cudaGetLastError();
@@ -817,6 +833,7 @@ bool Batch::configure_latency(size_t k, int wpr) {
     }
     if (per_sm < 1) return false;
     c.wpr = wpr;
+    c.ctas = cl;
     c.spec_bytes = bytes;
     c.rpw = 1;
     c.wpb = wpr / cl;
@@ -835,6 +852,7 @@ bool Batch::configure_class(size_t k, int wpb, int rpw) {
     LaunchClass& c = classes.at(k);
     if (rpw == 2 && c.kind != kTunePairKind) return false;
     c.wpr = 1;
+    c.ctas = 1;
     const void* fn = anneal_kernel_fn(c.opl, c.general, rpw);
     raise_smem_limit(fn, params.device);
     const size_t smem = (size_t)wpb * rpw * c.slot_bytes;
@@ -964,7 +982,7 @@ void Batch::enqueue_rounds(uint64_t iters, bool timed) {
                 ca.slot_bytes = c.spec_bytes;
                 ca.chunks = 1;
                 ca.chunk_done = nullptr;
-                check(launch_anneal_spec(ca, c.general, c.wpr, c.blocks, st), "launch anneal_spec_kernel");
+                check(launch_anneal_spec(ca, c.general, c.wpr, c.ctas, c.blocks, st), "launch anneal_spec_kernel");
             } else {
                 check(launch_anneal(ca, c.opl, c.general, c.wpb, c.blocks, st, c.rpw), "launch anneal_kernel");
             }

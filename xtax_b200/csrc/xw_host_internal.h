@@ -141,9 +141,10 @@ struct Batch {
     // side on their own streams.
     struct LaunchClass {
         int kind = 1, opl = 1, rpw = 1;
-        // warps per replica: 1, or 2..16 for the latency mode (orders up to
-        // 32), whose CTA of `wpr` warps holds one replica (spec_bytes)
-        int wpr = 1;
+        // warps per replica: 1, or 2..64 for the latency mode (orders up to
+        // 32), whose `ctas` CTAs (one, or a cluster of two or four) of
+        // wpr / ctas warps each hold a copy of one replica (spec_bytes)
+        int wpr = 1, ctas = 1;
         uint32_t spec_bytes = 0;
         bool general = false;
         int min_n = 0, max_n = 0;

@@ -53,12 +53,13 @@ cudaError_t launch_anneal(const AnnealArgs& args, int opl, bool general, int war
 // replicas whose one-warp slot (anneal_slot_bytes at one row per lane) is
 // at most slot_bytes; the kernel and its launch (a.slot_bytes: the CTA's
 // dynamic shared memory; a.chunks must be 1).
-// wpr warps per replica: one CTA of wpr warps (2..16), or a cluster of two
-// CTAs of wpr/2 warps (18..32, even) or of four CTAs of wpr/4 warps (33..64,
-// a multiple of 4); a cluster runs one replica, `blocks` unused.
-uint32_t anneal_spec_cta_bytes(uint32_t slot_bytes, int wpr);
-const void* anneal_spec_kernel_fn(bool general, int wpr);
-cudaError_t launch_anneal_spec(const AnnealArgs& args, bool general, int wpr, int blocks, cudaStream_t stream);
+// wpr warps per replica on `ctas` CTAs of wpr / ctas warps (2..16) each:
+// one CTA, or a cluster of two or four (one replica per cluster, `blocks`
+// unused)
+uint32_t anneal_spec_cta_bytes(uint32_t slot_bytes, int wpr, int ctas);
+const void* anneal_spec_kernel_fn(bool general, int ctas);
+cudaError_t launch_anneal_spec(const AnnealArgs& args, bool general, int wpr, int ctas, int blocks,
+                               cudaStream_t stream);
 // Orders above XW_MAX_N (xw_anneal_large.cu), in one of three forms:
 // 0 the Gram matrix and masks in an HBM arena; 1 bit planes in shared
 // memory, no Gram matrix stored (its entries recomputed by popcounts);
