@@ -51,7 +51,9 @@ namespace {
 // shared-memory ring must admit no more CTAs per SM than the TMEM columns
 // do (kCtasPerSm x kAccs x 128 <= 512).  Measured on B200, 65536 matrices,
 // ms at n = 32 / 64 / 96 / 128 (CTAs x stages x accumulators x groups):
-//   2 x 6 x 2 x 2   0.047 / 0.121 / 0.234 / 0.278   (the default)
+//   2 x 6 x 2 x 2   0.047 / 0.121 / 0.234 / 0.278   (the default; 0.045 / 0.110 /
+//                   0.224 / 0.276 with the diagonal entry taken by a select
+//                   tree and the extra block alternating at n = 64)
 //   4 x 3 x 1 x 1   0.049 / 0.133 / 0.256 / 0.307
 //   1 x 8 x 4 x 4   0.070 / 0.141 / 0.311 / 0.346
 //   1 x 8 x 4 x 2   0.070 / 0.168 / 0.305 / 0.412
@@ -202,10 +204,11 @@ __device__ __forceinline__ void rescore_fail(const RescoreParams& p, volatile in
 }
 
 // Per-row statistics of one tile's accumulator rows 32q..32q+31 (this
-// warp's lane quarter); see the epilogue comment below.  Returns the warp's
-// sums and whether every row's diagonal entry is right.
-__device__ __forceinline__ void tile_rows(const RescoreParams& p, uint32_t tacc, int t, int q, int lane, int4& part,
-                                          int& diag_ok, int& mat) {
+// warp's lane quarter); see the epilogue comment below.  rot is the
+// group's count of tiles before this one.  Returns the warp's sums and
+// whether every row's diagonal entry is right.
+__device__ __forceinline__ void tile_rows(const RescoreParams& p, uint32_t tacc, int t, int rot, int q, int lane,
+                                          int4& part, int& diag_ok, int& mat) {
     const int row0 = 32 * q;
     const int b = row0 / p.n;       // matrix of this warp within the tile
     const int i0 = row0 - b * p.n;  // first row of the warp within the matrix
@@ -226,10 +229,18 @@ __device__ __forceinline__ void tile_rows(const RescoreParams& p, uint32_t tacc,
             a_sq += v[j] * v[j] + v[j + 1] * v[j + 1];
         }
         if (c == i0) {
-            int d = v[0];
+            // v[lane] by a five-level select tree on the lane's bits (a
+            // chain of 31 selects measured 4-9% slower per launch)
+            int u[16];
 #pragma unroll
-            for (int j = 1; j < 32; ++j) d = lane == j ? v[j] : d;
-            dg = d;
+            for (int j = 0; j < 16; ++j) u[j] = (lane & 16) ? v[j + 16] : v[j];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) u[j] = (lane & 8) ? u[j + 8] : u[j];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) u[j] = (lane & 4) ? u[j + 4] : u[j];
+#pragma unroll
+            for (int j = 0; j < 2; ++j) u[j] = (lane & 2) ? u[j + 2] : u[j];
+            dg = (lane & 1) ? u[1] : u[0];
         }
         if (p.gram && mat < p.count) {
             int32_t* dst = p.gram + (size_t)mat * p.n * p.n + (size_t)i * p.n + c;
@@ -246,13 +257,19 @@ __device__ __forceinline__ void tile_rows(const RescoreParams& p, uint32_t tacc,
     // G is symmetric: without a Gram output each unordered pair of
     // off-diagonal 32x32 blocks is read once, by the warp of one of its two
     // row blocks (offsets d = 1..nb/2 cyclically), and counted twice; the
-    // diagonal entry (lane j of the warp's diagonal block) is taken out after
+    // diagonal entry (lane j of the warp's diagonal block) is taken out after.
+    // At d = nb/2 the two row blocks rb and rb + d name the same pair: one
+    // of them reads it, the one with rb / d even.  For n = 64 (nb = 2, two
+    // warps per matrix, warp q issuing on scheduler q) the choice
+    // alternates from tile to tile, (rb + rot) / d even, so that schedulers
+    // 0 and 2 do not take the extra block on every tile (measured 5% at
+    // n = 64; at n = 128 alternating measured 4% slower)
     if (p.gram) {
         for (int c = 0; c < p.n; c += 32) block(c, s_abs, s_nz, s_sq);
     } else {
         block(i0, s_abs, s_nz, s_sq);
         for (int d = 1; 2 * d <= nb; ++d) {
-            if (2 * d == nb && rb >= d) continue;
+            if (2 * d == nb && ((nb == 2 ? rb + rot : rb) / d & 1)) continue;
             block(((rb + d) % nb) * 32, o_abs, o_nz, o_sq);
         }
     }
@@ -392,7 +409,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) rescore_tc_kernel(const 
             const int t = (int)blockIdx.x + it * grid;
             int4 part = make_int4(0, 0, 0, 0);
             int diag_ok = 1, mat = 0;
-            if (active) tile_rows(p, tmem + (uint32_t)(a * kAccCols), t, q, lane, part, diag_ok, mat);
+            if (active) tile_rows(p, tmem + (uint32_t)(a * kAccCols), t, it / kGroups, q, lane, part, diag_ok, mat);
             // the accumulator is free for the MMA of a later tile
             asm volatile("tcgen05.fence::before_thread_sync;");
             __syncwarp();
