@@ -846,7 +846,7 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=400, help="requests of the serving stream (0: none)")
     ap.add_argument("--serve-plain", type=int, default=60,
                     help="prefix of the stream also run one request at a time")
-    ap.add_argument("--serve-quantum", type=int, default=1000, help="iterations per replica per server round")
+    ap.add_argument("--serve-quantum", type=int, default=2000, help="iterations per replica per server round")
     ap.add_argument("--serve-reference", type=int, default=60,
                     help="requests of the stream also run by the reference's xweigh_cuda, one process each, "
                          "arriving live")

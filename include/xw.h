@@ -395,7 +395,7 @@ int32_t xw_escape_scan(int32_t n, int32_t w, const int8_t* W_colmajor, int32_t l
 
 typedef struct xw_server_config {
     int32_t device;
-    int32_t quantum_iters;         /* iterations per replica per engine round (default 1000) */
+    int32_t quantum_iters;         /* iterations per replica per engine round (default 2000) */
     int32_t max_requests;          /* resident requests (job slots, default 1024) */
     int32_t max_resident_replicas; /* admission cap on resident replicas (0 = the replica id
                                       space) */
@@ -410,7 +410,7 @@ typedef struct xw_server_config {
                                       requests with the fewest iterations so far, oldest first,
                                       up to max_active_replicas */
     int32_t max_active_replicas;   /* replicas advanced per round under XW_SCHED_LEAST_ATTAINED
-                                      (0 = four waves of the device's resident warps) */
+                                      (0 = eight waves of the device's resident warps) */
     int32_t replicas_per_warp;     /* orders up to 16: 1 or 2 replicas per warp, 0 = tuned */
     int32_t reserved[5];
 } xw_server_config;

@@ -174,7 +174,7 @@ def test_server_config_defaults():
     import ctypes as C
     cfg = X.ServerConfig()
     X.lib().xw_server_config_default(C.byref(cfg))
-    assert (cfg.quantum_iters, cfg.max_requests, cfg.max_replica_ids, cfg.sylvester_shortcut) == (1000, 1024, 262144, 1)
+    assert (cfg.quantum_iters, cfg.max_requests, cfg.max_replica_ids, cfg.sylvester_shortcut) == (2000, 1024, 262144, 1)
     assert cfg.arena_bytes == 1 << 30
 
 

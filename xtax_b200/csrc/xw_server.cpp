@@ -775,15 +775,19 @@ void Server::start() {
             for (int rpw = 1; rpw <= (c == 0 ? 2 : 1); ++rpw)
                 raise_smem_limit(anneal_kernel_fn(opl_of_class(c), general, rpw), cfg.device);
     if (cfg.max_active_replicas <= 0) {
-        // four waves of the resident warps at the order-32 slot: enough work
-        // per round to keep every SM busy through the round's tail
+        // eight waves of the resident warps at the order-32 slot: enough work
+        // per round to keep every SM busy through the round's tails (the C5
+        // stream, 400 requests: 0.567 G moves/s at four waves and 1000
+        // iterations per round, 0.612 G at eight and 2000, with p50/p99
+        // time-to-exact 1.16 s / 23.3 s against 1.44 s / 25.2 s; a stream the
+        // device keeps up with: p50 0.096 s against 0.099 s)
         int per_sm = 0;
         const int wpb = cfg.warps_per_block > 0 ? cfg.warps_per_block : 4;
         const uint32_t slot = anneal_slot_bytes(32, 16, 1);
         check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, anneal_kernel_fn(1, false), 32 * wpb,
                                                                  (size_t)wpb * slot),
                    "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-        cfg.max_active_replicas = std::max(256, 4 * per_sm * wpb * sms);
+        cfg.max_active_replicas = std::max(256, 8 * per_sm * wpb * sms);
     }
     if (cfg.max_resident_replicas <= 0) cfg.max_resident_replicas = cfg.max_replica_ids;
     cfg.max_resident_replicas = std::min(cfg.max_resident_replicas, cfg.max_replica_ids);
@@ -909,7 +913,7 @@ void xw_server_config_default(xw_server_config* c) {
     if (!c) return;
     std::memset(c, 0, sizeof *c);
     c->device = 0;
-    c->quantum_iters = 1000;
+    c->quantum_iters = 2000;
     c->max_requests = 1024;
     c->max_resident_replicas = 0;
     c->max_replica_ids = 262144;
