@@ -1717,15 +1717,15 @@ __global__ void __launch_bounds__(512, 1) anneal_spec_kernel(AnnealArgs a, int K
     if constexpr (CL > 1) {
         const uint32_t item = blockIdx.x / CL;
         if (item < a.n_items) run_replica_spec<GEN, CL>(a, a.items[item], smem, warp, K, lane);
-        return;
-    }
-    for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(a.counter, 1u);
-        __syncthreads();
-        const uint32_t item = s_item;
-        if (item >= a.n_items) break;
-        run_replica_spec<GEN, 1>(a, a.items[item], smem, warp, K, lane);
-        __syncthreads();
+    } else {
+        for (;;) {
+            if (threadIdx.x == 0) s_item = atomicAdd(a.counter, 1u);
+            __syncthreads();
+            const uint32_t item = s_item;
+            if (item >= a.n_items) break;
+            run_replica_spec<GEN, 1>(a, a.items[item], smem, warp, K, lane);
+            __syncthreads();
+        }
     }
 }
 
