@@ -155,6 +155,33 @@ def test_mixed_orders_in_one_launch_match_oracle():
     batch.close()
 
 
+@pytest.mark.parametrize("extra", [None, {"n": 9, "w": 1, "seed": 12, "replicas": 2}],
+                         ids=["one_zero_only", "with_sparse_rows"])
+def test_one_zero_class_and_a_mixed_class_match_oracle(extra):
+    """A class whose jobs all have one zero per row (w = n - 1) runs the
+    kernel with the minority size and side as constants; a class that also
+    holds another shape (W(9,1): one nonzero per row) runs the lean kernel
+    for any shape.  Either way every replica replays on the oracle (a
+    replica given the wrong kernel would carry an error flag instead)."""
+    p = X.Params(stop_on_solve=0, t_init=5.0, moves_per_launch=700, warps_per_replica=1)
+    jobs = [{"n": 20, "w": 19, "seed": 11, "replicas": 3}, {"n": 31, "w": 30, "seed": 13, "replicas": 2}]
+    if extra:
+        jobs.append(extra)
+    batch = X.Batch(jobs, p)
+    assert all(c["warps_per_replica"] == 1 and c["rows_per_lane"] == 1 for c in batch.classes())
+    temps = [[batch.replica(j, r)[0].reheat_temperature for r in range(jb["replicas"])]
+             for j, jb in enumerate(jobs)]
+    batch.run(1400)
+    batch.synchronize()
+    for j, jb in enumerate(jobs):
+        job = oracle_job(jb["n"], jb["w"], jb["seed"], p)
+        for r in range(jb["replicas"]):
+            rep = O.Replica(job, r, start_of(jb["n"], jb["w"], jb["seed"], r, p), temps[j][r], r)
+            rep.run(1400, stop_on_solve=False)
+            compare(batch, j, r, rep)
+    batch.close()
+
+
 SMALL_CASES = [c for c in CASES if c[0] <= 16]
 
 

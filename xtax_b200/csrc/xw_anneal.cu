@@ -1050,7 +1050,10 @@ __device__ __forceinline__ bool apply_move(Replica<OPL, GW>& R, const Choice& ch
 // functions, even inlined, they hold more values live across the loop and
 // spill more under the lean kernel's 96-register budget (measured 6%
 // slower on W(26,25) populations).
-template <int OPL, bool GEN, int GW = 32>
+// ONEZ: every row has one zero (w = n - 1: minority lists of one entry,
+// the dense side), so the minority size and side are constants; a replica
+// of another shape is flagged (XW_ERR_KERNEL) and not annealed.
+template <int OPL, bool GEN, int GW = 32, bool ONEZ = false>
 __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int lane, uint64_t chunk_iters) {
     const unsigned gm = group_mask<GW>();
     uint8_t* rec = a.arena + a.rec_off[rid];
@@ -1059,11 +1062,15 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
     XwJob* J = a.jobs + jid;
     if (*(volatile int32_t*)&J->done) return;
     if (a.stop_on_solve == 1 && *(volatile int32_t*)&J->solved) return;
+    if (ONEZ && (J->m != 1 || J->sparse != 0)) {
+        if (lane == 0) H->err |= XW_ERR_KERNEL;
+        return;
+    }
 
     // eight rows per lane: int16 Gram and 256-bit row masks (slot_layout)
     constexpr int MW = OPL > 4 ? 4 : 2;
     using GT = typename std::conditional<(OPL > 4), int16_t, int32_t>::type;
-    const int n = J->n, w = J->w, m = J->m, sparse = J->sparse;
+    const int n = J->n, w = J->w, m = ONEZ ? 1 : J->m, sparse = ONEZ ? 0 : J->sparse;
     const SlotLayout L = slot_layout(n, m, OPL > 4);
     const int ld = L.ld;
     int8_t* sW = reinterpret_cast<int8_t*>(slot);
@@ -1677,7 +1684,7 @@ constexpr int anneal_maxnreg(int opl, bool general, int gw) {
 // Each lane group (the warp, or each half of it) takes work items from the
 // launch's counter on its own: a replica (all of its launch iterations) or
 // one chunk of them.
-template <int OPL, bool GEN, int GW>
+template <int OPL, bool GEN, int GW, bool ONEZ = false>
 __global__ void __maxnreg__(anneal_maxnreg(OPL, GEN, GW)) anneal_kernel(AnnealArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int lane = threadIdx.x & (GW - 1);
@@ -1691,7 +1698,7 @@ __global__ void __maxnreg__(anneal_maxnreg(OPL, GEN, GW)) anneal_kernel(AnnealAr
         item = __shfl_sync(gm, item, 0, GW);
         if (item >= total) break;
         if (a.chunks == 1) {
-            run_replica<OPL, GEN, GW>(a, a.items[item], slot, lane, a.iters);
+            run_replica<OPL, GEN, GW, ONEZ>(a, a.items[item], slot, lane, a.iters);
             continue;
         }
         const uint32_t c = item / a.n_items;
@@ -1699,7 +1706,7 @@ __global__ void __maxnreg__(anneal_maxnreg(OPL, GEN, GW)) anneal_kernel(AnnealAr
         const uint64_t lo = a.iters * c / a.chunks, hi = a.iters * (c + 1) / a.chunks;
         RepHeader* H = reinterpret_cast<RepHeader*>(a.arena + a.rec_off[rid]);
         const bool ok = chunk_begin(a.chunk_done + rid, c, a.chunk_wait_ns, &H->err, lane, gm);
-        if (ok) run_replica<OPL, GEN, GW>(a, rid, slot, lane, hi - lo);
+        if (ok) run_replica<OPL, GEN, GW, ONEZ>(a, rid, slot, lane, hi - lo);
         chunk_end(a.chunk_done + rid, c, ok, lane, gm);
     }
 }
@@ -1860,7 +1867,9 @@ uint32_t anneal_slot_bytes(int n, int m, int opl) { return slot_layout(n, m, opl
 
 int anneal_opl(int n) { return n <= 32 ? 1 : n <= 64 ? 2 : n <= 128 ? 4 : 8; }
 
-const void* anneal_kernel_fn(int opl, bool general, int rpw) {
+const void* anneal_kernel_fn(int opl, bool general, int rpw, bool one_zero) {
+    if (one_zero && opl == 1 && !general && rpw == 1)
+        return reinterpret_cast<const void*>(&anneal_kernel<1, false, 32, true>);
     if (rpw == 2) {
         return general ? reinterpret_cast<const void*>(&anneal_kernel<1, true, 16>)
                        : reinterpret_cast<const void*>(&anneal_kernel<1, false, 16>);
@@ -1883,7 +1892,7 @@ cudaError_t launch_anneal(const AnnealArgs& args, int opl, bool general, int war
     const size_t smem = (size_t)warps_per_block * rpw * args.slot_bytes;
     const dim3 grid(blocks), block(32 * warps_per_block);
     void* kargs[] = {const_cast<AnnealArgs*>(&args)};
-    return cudaLaunchKernel(anneal_kernel_fn(opl, general, rpw), grid, block, kargs, smem, stream);
+    return cudaLaunchKernel(anneal_kernel_fn(opl, general, rpw, args.one_zero != 0), grid, block, kargs, smem, stream);
 }
 
 // wpr warps per replica on `ctas` CTAs (1, 2 or 4; a cluster above 1) of

@@ -504,6 +504,7 @@ void Batch::derive_layout() {
         c.item_count += 1;
         c.min_n = std::min(c.min_n, J.n);
         c.general = c.general || J.general != 0;
+        c.one_zero = c.one_zero && J.m == 1 && !J.sparse;
         c.slot_bytes = std::max(c.slot_bytes, anneal_slot_bytes(J.n, J.m, c.opl));
     }
     // arena offsets of the large-order replicas (Gram matrices, or planes
@@ -853,7 +854,7 @@ bool Batch::configure_class(size_t k, int wpb, int rpw) {
     if (rpw == 2 && c.kind != kTunePairKind) return false;
     c.wpr = 1;
     c.ctas = 1;
-    const void* fn = anneal_kernel_fn(c.opl, c.general, rpw);
+    const void* fn = anneal_kernel_fn(c.opl, c.general, rpw, c.one_zero);
     raise_smem_limit(fn, params.device);
     const size_t smem = (size_t)wpb * rpw * c.slot_bytes;
     int per_sm = 0;
@@ -927,7 +928,7 @@ void Batch::enqueue_rounds(uint64_t iters, bool timed) {
         a.rec_off = static_cast<const uint64_t*>(d_rec_off);
         a.iters = std::min(left, per);
         a.stop_on_solve = params.stop_on_solve;
-        a.pad = 0;
+        a.one_zero = 0;
         a.chunk_wait_ns = chunk_wait_limit_ns();
         left -= a.iters;
         uint32_t* counters = static_cast<uint32_t*>(d_counters) + (size_t)launches * k;
@@ -975,6 +976,7 @@ void Batch::enqueue_rounds(uint64_t iters, bool timed) {
             ca.n_items = c.item_count;
             ca.slot_bytes = c.slot_bytes;
             ca.counter = counters + l;
+            ca.one_zero = c.one_zero ? 1 : 0;
             ca.chunks = ca.iters >= c.chunks ? c.chunks : 1;
             if (ca.chunks > 1) ca.chunk_done = static_cast<uint32_t*>(d_chunk_done);
             cudaStream_t st = on(l);

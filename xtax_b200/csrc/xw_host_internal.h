@@ -147,6 +147,9 @@ struct Batch {
         int wpr = 1, ctas = 1;
         uint32_t spec_bytes = 0;
         bool general = false;
+        // every job of the class has one zero per row (w = n - 1): the lean
+        // one-row kernel runs its instantiation for that shape
+        bool one_zero = true;
         int min_n = 0, max_n = 0;
         uint32_t slot_bytes = 0;
         uint32_t item_begin = 0, item_count = 0;

@@ -20,7 +20,10 @@ struct AnnealArgs {
     uint32_t* counter;         // persistent work counter, zeroed per launch
     uint64_t iters;            // iterations per replica this launch
     int32_t stop_on_solve;
-    int32_t pad;
+    // 1: every replica of the launch has one zero per row (w = n - 1); the
+    // lean one-row, one-replica-per-warp kernel then runs its instantiation
+    // with the minority size and side as constants (other kernels ignore it)
+    int32_t one_zero;
     uint8_t* gram = nullptr;            // large-order kernel: Gram and mask arena
     const uint64_t* gram_off = nullptr; // byte offset of each replica's Gram there
     // The shared-memory kernel can split each replica's `iters` into `chunks`
@@ -44,7 +47,9 @@ int anneal_opl(int n);
 // `rpw`: replicas per warp, 1, or 2 for orders up to 16 (opl 1; each half
 // of a warp owns a replica and a shared-memory slot of args.slot_bytes, so
 // a CTA holds warps_per_block * rpw slots).
-const void* anneal_kernel_fn(int opl, bool general, int rpw = 1);
+// `one_zero`: the instantiation for launches whose replicas all have one zero
+// per row (AnnealArgs::one_zero); it applies to opl 1, lean, rpw 1 only.
+const void* anneal_kernel_fn(int opl, bool general, int rpw = 1, bool one_zero = false);
 cudaError_t launch_anneal(const AnnealArgs& args, int opl, bool general, int warps_per_block, int blocks,
                           cudaStream_t stream, int rpw = 1);
 // Latency mode (orders up to 32): one replica per CTA of K warps (2..16),

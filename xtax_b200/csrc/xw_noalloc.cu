@@ -286,7 +286,7 @@ extern "C" int32_t xw_anneal_noalloc(int32_t n, int32_t w, const xw_params* p, i
         a.counter = reinterpret_cast<uint32_t*>(scratch + L.off_counters) + k;
         a.iters = std::min(left, per);
         a.stop_on_solve = p->stop_on_solve;
-        a.pad = 0;
+        a.one_zero = 0;
         left -= a.iters;
         e = launch_anneal(a, opl, job_general, wpb, blocks, stream);
         if (e != cudaSuccess) return nfail(XW_ERR_CUDA, std::string("anneal launch failed: ") + cudaGetErrorString(e));

@@ -189,6 +189,7 @@ struct Server {
     std::vector<uint32_t> items_host[kClasses];
     uint32_t class_slot[kClasses] = {};
     bool class_general[kClasses] = {};
+    bool class_one_zero[kClasses] = {};       // every request of the class is W(n, n-1)
     std::map<std::pair<int, uint32_t>, int> per_sm_cache;
     int last_njobs = 0;
 
@@ -408,6 +409,7 @@ void Server::rebuild_items() {
         items_host[c].clear();
         class_slot[c] = 0;
         class_general[c] = false;
+        class_one_zero[c] = true;
     }
     for (int s : order) {
         const ReqPtr& q = slot_req[s];
@@ -415,6 +417,7 @@ void Server::rebuild_items() {
         for (int r = 0; r < q->spec.replicas; ++r) items_host[c].push_back((uint32_t)(q->rep_begin + r));
         class_slot[c] = std::max(class_slot[c], anneal_slot_bytes(q->spec.n, q->job.m, opl_of_class(c)));
         class_general[c] = class_general[c] || q->job.general != 0;
+        class_one_zero[c] = class_one_zero[c] && q->job.m == 1 && !q->job.sparse;
     }
     for (int c = 0; c < kClasses; ++c)
         if (!items_host[c].empty())
@@ -497,7 +500,7 @@ void Server::round(bool& any_tempering) {
         a.counter = d_counters + c;
         a.iters = (uint64_t)cfg.quantum_iters;
         a.stop_on_solve = 2;
-        a.pad = 0;
+        a.one_zero = class_one_zero[c] && cls_rpw[c] == 1 ? 1 : 0;
         a.chunks = cls_chunks[c];
         if (a.chunks > 1) a.chunk_done = d_chunk_done;
         a.chunk_wait_ns = chunk_wait_limit_ns();
@@ -774,6 +777,7 @@ void Server::start() {
         for (bool general : {false, true})
             for (int rpw = 1; rpw <= (c == 0 ? 2 : 1); ++rpw)
                 raise_smem_limit(anneal_kernel_fn(opl_of_class(c), general, rpw), cfg.device);
+    raise_smem_limit(anneal_kernel_fn(1, false, 1, true), cfg.device);
     if (cfg.max_active_replicas <= 0) {
         // eight waves of the resident warps at the order-32 slot: enough work
         // per round to keep every SM busy through the round's tails (the C5
