@@ -1051,9 +1051,10 @@ __device__ __forceinline__ bool apply_move(Replica<OPL, GW>& R, const Choice& ch
 // spill more under the lean kernel's 96-register budget (measured 6%
 // slower on W(26,25) populations).
 // ONEZ: every row has one zero (w = n - 1: minority lists of one entry,
-// the dense side), so the minority size and side are constants; a replica
-// of another shape is flagged (XW_ERR_KERNEL) and not annealed.
-template <int OPL, bool GEN, int GW = 32, bool ONEZ = false>
+// the dense side), so the minority size and side are constants; NFIX > 0:
+// the order is NFIX as well.  A replica of another shape is flagged
+// (XW_ERR_KERNEL) and not annealed.
+template <int OPL, bool GEN, int GW = 32, bool ONEZ = false, int NFIX = 0>
 __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, int lane, uint64_t chunk_iters) {
     const unsigned gm = group_mask<GW>();
     uint8_t* rec = a.arena + a.rec_off[rid];
@@ -1062,7 +1063,7 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
     XwJob* J = a.jobs + jid;
     if (*(volatile int32_t*)&J->done) return;
     if (a.stop_on_solve == 1 && *(volatile int32_t*)&J->solved) return;
-    if (ONEZ && (J->m != 1 || J->sparse != 0)) {
+    if ((ONEZ && (J->m != 1 || J->sparse != 0)) || (NFIX && J->n != NFIX)) {
         if (lane == 0) H->err |= XW_ERR_KERNEL;
         return;
     }
@@ -1070,7 +1071,8 @@ __device__ void run_replica(const AnnealArgs& a, uint32_t rid, uint8_t* slot, in
     // eight rows per lane: int16 Gram and 256-bit row masks (slot_layout)
     constexpr int MW = OPL > 4 ? 4 : 2;
     using GT = typename std::conditional<(OPL > 4), int16_t, int32_t>::type;
-    const int n = J->n, w = J->w, m = ONEZ ? 1 : J->m, sparse = ONEZ ? 0 : J->sparse;
+    // one zero per row: m = n - w = 1, so w = n - 1
+    const int n = NFIX ? NFIX : J->n, w = ONEZ ? n - 1 : J->w, m = ONEZ ? 1 : J->m, sparse = ONEZ ? 0 : J->sparse;
     const SlotLayout L = slot_layout(n, m, OPL > 4);
     const int ld = L.ld;
     int8_t* sW = reinterpret_cast<int8_t*>(slot);
@@ -1684,7 +1686,7 @@ constexpr int anneal_maxnreg(int opl, bool general, int gw) {
 // Each lane group (the warp, or each half of it) takes work items from the
 // launch's counter on its own: a replica (all of its launch iterations) or
 // one chunk of them.
-template <int OPL, bool GEN, int GW, bool ONEZ = false>
+template <int OPL, bool GEN, int GW, bool ONEZ = false, int NFIX = 0>
 __global__ void __maxnreg__(anneal_maxnreg(OPL, GEN, GW)) anneal_kernel(AnnealArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int lane = threadIdx.x & (GW - 1);
@@ -1698,7 +1700,7 @@ __global__ void __maxnreg__(anneal_maxnreg(OPL, GEN, GW)) anneal_kernel(AnnealAr
         item = __shfl_sync(gm, item, 0, GW);
         if (item >= total) break;
         if (a.chunks == 1) {
-            run_replica<OPL, GEN, GW, ONEZ>(a, a.items[item], slot, lane, a.iters);
+            run_replica<OPL, GEN, GW, ONEZ, NFIX>(a, a.items[item], slot, lane, a.iters);
             continue;
         }
         const uint32_t c = item / a.n_items;
@@ -1706,7 +1708,7 @@ __global__ void __maxnreg__(anneal_maxnreg(OPL, GEN, GW)) anneal_kernel(AnnealAr
         const uint64_t lo = a.iters * c / a.chunks, hi = a.iters * (c + 1) / a.chunks;
         RepHeader* H = reinterpret_cast<RepHeader*>(a.arena + a.rec_off[rid]);
         const bool ok = chunk_begin(a.chunk_done + rid, c, a.chunk_wait_ns, &H->err, lane, gm);
-        if (ok) run_replica<OPL, GEN, GW, ONEZ>(a, rid, slot, lane, hi - lo);
+        if (ok) run_replica<OPL, GEN, GW, ONEZ, NFIX>(a, rid, slot, lane, hi - lo);
         chunk_end(a.chunk_done + rid, c, ok, lane, gm);
     }
 }
@@ -1867,9 +1869,37 @@ uint32_t anneal_slot_bytes(int n, int m, int opl) { return slot_layout(n, m, opl
 
 int anneal_opl(int n) { return n <= 32 ? 1 : n <= 64 ? 2 : n <= 128 ? 4 : 8; }
 
-const void* anneal_kernel_fn(int opl, bool general, int rpw, bool one_zero) {
-    if (one_zero && opl == 1 && !general && rpw == 1)
+template <int N>
+const void* one_zero_order_fn() {
+    return reinterpret_cast<const void*>(&anneal_kernel<1, false, 32, true, N>);
+}
+
+// the one-zero kernel compiled for one order: the even orders 6..26 (W(n, n-1)
+// does not exist for odd n), nullptr for the others.  28, 30 and 32 compile
+// with 380 bytes of spills a thread (40 for the kernel of any order) and are
+// left to that kernel.
+const void* one_zero_fixed_fn(int n) {
+    switch (n) {
+    case 6: return one_zero_order_fn<6>();
+    case 8: return one_zero_order_fn<8>();
+    case 10: return one_zero_order_fn<10>();
+    case 12: return one_zero_order_fn<12>();
+    case 14: return one_zero_order_fn<14>();
+    case 16: return one_zero_order_fn<16>();
+    case 18: return one_zero_order_fn<18>();
+    case 20: return one_zero_order_fn<20>();
+    case 22: return one_zero_order_fn<22>();
+    case 24: return one_zero_order_fn<24>();
+    case 26: return one_zero_order_fn<26>();
+    default: return nullptr;
+    }
+}
+
+const void* anneal_kernel_fn(int opl, bool general, int rpw, bool one_zero, int fixed_order) {
+    if (one_zero && opl == 1 && !general && rpw == 1) {
+        if (const void* f = fixed_order > 0 ? one_zero_fixed_fn(fixed_order) : nullptr) return f;
         return reinterpret_cast<const void*>(&anneal_kernel<1, false, 32, true>);
+    }
     if (rpw == 2) {
         return general ? reinterpret_cast<const void*>(&anneal_kernel<1, true, 16>)
                        : reinterpret_cast<const void*>(&anneal_kernel<1, false, 16>);
@@ -1892,7 +1922,8 @@ cudaError_t launch_anneal(const AnnealArgs& args, int opl, bool general, int war
     const size_t smem = (size_t)warps_per_block * rpw * args.slot_bytes;
     const dim3 grid(blocks), block(32 * warps_per_block);
     void* kargs[] = {const_cast<AnnealArgs*>(&args)};
-    return cudaLaunchKernel(anneal_kernel_fn(opl, general, rpw, args.one_zero != 0), grid, block, kargs, smem, stream);
+    return cudaLaunchKernel(anneal_kernel_fn(opl, general, rpw, args.one_zero != 0, args.fixed_order), grid, block,
+                            kargs, smem, stream);
 }
 
 // wpr warps per replica on `ctas` CTAs (1, 2 or 4; a cluster above 1) of

@@ -503,6 +503,7 @@ void Batch::derive_layout() {
         LaunchClass& c = classes.back();
         c.item_count += 1;
         c.min_n = std::min(c.min_n, J.n);
+        c.max_n = std::max(c.max_n, J.n);
         c.general = c.general || J.general != 0;
         c.one_zero = c.one_zero && J.m == 1 && !J.sparse;
         c.slot_bytes = std::max(c.slot_bytes, anneal_slot_bytes(J.n, J.m, c.opl));
@@ -854,7 +855,7 @@ bool Batch::configure_class(size_t k, int wpb, int rpw) {
     if (rpw == 2 && c.kind != kTunePairKind) return false;
     c.wpr = 1;
     c.ctas = 1;
-    const void* fn = anneal_kernel_fn(c.opl, c.general, rpw, c.one_zero);
+    const void* fn = anneal_kernel_fn(c.opl, c.general, rpw, c.one_zero, c.min_n == c.max_n ? c.min_n : 0);
     raise_smem_limit(fn, params.device);
     const size_t smem = (size_t)wpb * rpw * c.slot_bytes;
     int per_sm = 0;
@@ -977,6 +978,7 @@ void Batch::enqueue_rounds(uint64_t iters, bool timed) {
             ca.slot_bytes = c.slot_bytes;
             ca.counter = counters + l;
             ca.one_zero = c.one_zero ? 1 : 0;
+            ca.fixed_order = c.one_zero && c.min_n == c.max_n ? c.min_n : 0;
             ca.chunks = ca.iters >= c.chunks ? c.chunks : 1;
             if (ca.chunks > 1) ca.chunk_done = static_cast<uint32_t*>(d_chunk_done);
             cudaStream_t st = on(l);

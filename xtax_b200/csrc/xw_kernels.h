@@ -34,6 +34,10 @@ struct AnnealArgs {
     uint32_t* chunk_done = nullptr;
     // device-time limit of a chunk's wait for its predecessor, 0 = 30 s
     uint64_t chunk_wait_ns = 0;
+    // with one_zero: the launch's single order, whose instantiation (the even
+    // orders 6..26) then runs with the order as a constant; 0 = any order
+    int32_t fixed_order = 0;
+    int32_t fixed_pad = 0;
 };
 
 // shared-memory bytes one warp needs for a replica of order n, minority m,
@@ -48,8 +52,9 @@ int anneal_opl(int n);
 // of a warp owns a replica and a shared-memory slot of args.slot_bytes, so
 // a CTA holds warps_per_block * rpw slots).
 // `one_zero`: the instantiation for launches whose replicas all have one zero
-// per row (AnnealArgs::one_zero); it applies to opl 1, lean, rpw 1 only.
-const void* anneal_kernel_fn(int opl, bool general, int rpw = 1, bool one_zero = false);
+// per row (AnnealArgs::one_zero); it applies to opl 1, lean, rpw 1 only;
+// `fixed_order` > 0: all of them have that order (AnnealArgs::fixed_order).
+const void* anneal_kernel_fn(int opl, bool general, int rpw = 1, bool one_zero = false, int fixed_order = 0);
 cudaError_t launch_anneal(const AnnealArgs& args, int opl, bool general, int warps_per_block, int blocks,
                           cudaStream_t stream, int rpw = 1);
 // Latency mode (orders up to 32): one replica per CTA of K warps (2..16),
